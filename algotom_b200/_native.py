@@ -1,0 +1,81 @@
+"""ctypes binding of ``libalgotom_b200.so`` (the C ABI in include/algotom_b200.h).
+
+The library is built in-tree (``make -C algotom_b200/csrc`` or
+``__graft_entry__.build()``) into ``algotom_b200/lib``.  There is no fallback:
+if the library is missing or fails to load, every call raises
+:class:`NativeLibraryError`.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
+
+# every symbol include/algotom_b200.h declares
+EXPORTS = ("atb_version", "atb_last_error", "atb_filter_log2m",
+           "atb_filter_rows", "atb_neg_log", "atb_backproject")
+
+F32, F16, BF16 = 0, 1, 2
+PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
+             "wrap": 4, "linear_ramp": 5, "mean": 6, "maximum": 7,
+             "minimum": 8, "median": 9}
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library is missing, failed to load, or a call failed."""
+
+
+_c_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_SIGS = {
+    "atb_version": (ctypes.c_int, []),
+    "atb_last_error": (ctypes.c_char_p, []),
+    "atb_filter_log2m": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "atb_filter_rows": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+        ctypes.c_int, _vp, ctypes.c_int, _c_i64, _c_i64, _vp]),
+    "atb_neg_log": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+        _c_i64, _c_i64, _vp]),
+    "atb_backproject": (ctypes.c_int, [
+        _vp, ctypes.c_int, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+        ctypes.c_float, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library once and attach the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NativeLibraryError(
+            "libalgotom_b200.so not built (expected at %s); run "
+            "`make -C algotom_b200/csrc`" % LIB_PATH)
+    try:
+        lib = ctypes.CDLL(LIB_PATH)
+    except OSError as exc:
+        raise NativeLibraryError("cannot load %s: %s" % (LIB_PATH, exc))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    return load().atb_last_error().decode("utf-8", "replace")
+
+
+def call(name, *args):
+    """Call an ``atb_*`` entry point; raise on a negative return code."""
+    rc = getattr(load(), name)(*args)
+    if rc < 0:
+        raise NativeLibraryError("%s failed (%d): %s" % (name, rc,
+                                                         last_error()))
+    return rc

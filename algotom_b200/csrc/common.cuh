@@ -1,0 +1,40 @@
+// Shared helpers of the algotom_b200 CUDA library (sm_100a only).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/algotom_b200.h"
+
+namespace atb {
+
+// Records a printf-style message as the calling thread's last error and
+// returns `code`.
+int fail(int code, const char *fmt, ...);
+
+// Checks the launch that just happened on this thread; ATB_ECUDA on error.
+int check_launch(const char *what);
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+__device__ __forceinline__ float load_as_float(const float *p) { return __ldg(p); }
+__device__ __forceinline__ float load_as_float(const __half *p) { return __half2float(__ldg(p)); }
+__device__ __forceinline__ float load_as_float(const __nv_bfloat16 *p) {
+  return __bfloat162float(__ldg(p));
+}
+
+__device__ __forceinline__ void store_from_float(float *p, float v) { *p = v; }
+__device__ __forceinline__ void store_from_float(__half *p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ void store_from_float(__nv_bfloat16 *p, float v) {
+  *p = __float2bfloat16_rn(v);
+}
+
+// -log of a transmission value; values <= 0 read as 1 (give 0), as the
+// reference replaces them before taking the logarithm
+// (algotom/rec/reconstruction.py:431-436).  NaN stays NaN.
+__device__ __forceinline__ float neg_log(float v) { return v <= 0.0f ? 0.0f : -logf(v); }
+
+}  // namespace atb

@@ -1,0 +1,385 @@
+"""Drop-in replacement of algotom's FBP / BPF reconstruction functions.
+
+Same names, signatures, defaults, errors and warnings as
+``algotom/rec/reconstruction.py`` (algotom 1.6.0) for the filtered
+back-projection path; the compute runs in the sm_100a kernels of
+``libalgotom_b200.so`` through its C ABI.  There is no CPU path: ``gpu`` and
+``ncore`` are accepted for compatibility and do not change where the work
+runs (``block`` is accepted and ignored; the kernels pick their own tiles).
+
+Inputs may be NumPy arrays (results come back as NumPy arrays with the
+reference's dtypes) or torch tensors (results stay torch tensors on the
+tensor's CUDA device).  A few keyword-only extensions are available:
+``out`` (write the reconstruction into a caller buffer, e.g. pinned host
+memory), ``storage`` ("float32", "float16" or "bfloat16": the element type
+of the filtered sinogram between the two kernels) and ``kahan`` ("chunk",
+the default, or "angle").
+"""
+import math
+import warnings
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from . import windows as win
+from .windows import (make_smoothing_window, make_2d_ramp_window,  # noqa: F401
+                      make_circular_ramp_window)
+
+_STORAGE = {"float32": (torch.float32, nat.F32),
+            "float16": (torch.float16, nat.F16),
+            "bfloat16": (torch.bfloat16, nat.BF16)}
+
+_spec_cache = {}
+_tw_cache = {}
+
+
+# --------------------------------------------------------------------------
+# device plumbing
+# --------------------------------------------------------------------------
+def _device():
+    if not torch.cuda.is_available():
+        raise nat.NativeLibraryError(
+            "algotom_b200 runs on a CUDA device only; none is available")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _stream_ptr(device=None):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _to_device(x, device=None):
+    """float32 CUDA tensor with a contiguous last axis; returns (t, is_np)."""
+    if isinstance(x, torch.Tensor):
+        dev = x.device if x.is_cuda else (device or _device())
+        t = x.to(device=dev, dtype=torch.float32, non_blocking=True)
+        is_np = False
+    else:
+        dev = device or _device()
+        a = np.asarray(x)
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32))
+        t = t.to(dev, non_blocking=t.is_pinned())
+        is_np = True
+    if t.stride(-1) != 1:
+        t = t.contiguous()
+    return t, is_np
+
+
+def _trig(angles, device):
+    """(cos(-a), sin(-a)) in FP64 of the float32-rounded angles."""
+    a = np.float32(np.asarray(angles, dtype=np.float64)).astype(np.float64)
+    if not np.all(np.isfinite(a)):
+        raise ValueError("angles must be finite")
+    tab = np.stack([np.cos(-a), np.sin(-a)], axis=1)
+    return torch.from_numpy(np.ascontiguousarray(tab)).to(device)
+
+
+def _twiddle(log2m, device):
+    key = (log2m, device)
+    t = _tw_cache.get(key)
+    if t is None:
+        tw = win.twiddles(log2m)
+        t = torch.from_numpy(tw.view(np.float32).copy()).to(device)
+        _tw_cache[key] = t
+    return t
+
+
+def _spectrum(ramp_win, filter_name, nrow, ncol, pad, log2m, device):
+    """Device spectrum [1 or nrow, M] for the row filter."""
+    n = ncol + 2 * pad
+    if ramp_win is None or np.shape(ramp_win) != (nrow, n):
+        key = (filter_name, ncol, pad, log2m, device)
+        t = _spec_cache.get(key)
+        if t is None:
+            sp = win.row_filter_spectrum(win.ramp_window_row(n, filter_name),
+                                         ncol, pad, log2m)
+            t = torch.from_numpy(sp.view(np.float32).copy()).to(device)
+            if len(_spec_cache) > 32:
+                _spec_cache.clear()
+            _spec_cache[key] = t
+        return t, 1
+    rw = np.asarray(ramp_win.cpu() if isinstance(ramp_win, torch.Tensor)
+                    else ramp_win)
+    rows = rw[:1] if np.all(rw == rw[:1]) else rw
+    sp = win.row_filter_spectrum(rows, ncol, pad, log2m)
+    return torch.from_numpy(sp.view(np.float32).copy()).to(device), len(rows)
+
+
+def _as3(t):
+    """[nrow, ncol] -> [nrow, 1, ncol] view."""
+    return t.unsqueeze(1) if t.dim() == 2 else t
+
+
+def filter_sinograms(sino3, pad, pad_mode="edge", apply_log=False,
+                     ramp_win=None, filter_name="hann", storage="float32"):
+    """Device ramp filter of a [nrow, nslice, ncol] float32 CUDA tensor.
+
+    Returns a new [nrow, nslice, ncol] tensor of ``storage`` type.
+    """
+    nrow, nslice, ncol = sino3.shape
+    if pad_mode not in nat.PAD_MODES:
+        raise ValueError("pad_mode %r is not supported" % (pad_mode,))
+    log2m = nat.call("atb_filter_log2m", int(ncol), int(pad))
+    dev = sino3.device
+    spec, spec_rows = _spectrum(ramp_win, filter_name, nrow, ncol, pad, log2m,
+                                dev)
+    tdtype, code = _STORAGE[storage]
+    out = torch.empty((nrow, nslice, ncol), dtype=tdtype, device=dev)
+    nat.call("atb_filter_rows", sino3.data_ptr(), sino3.stride(0),
+             sino3.stride(1), nrow, nslice, ncol, int(pad),
+             nat.PAD_MODES[pad_mode], int(bool(apply_log)), spec.data_ptr(),
+             spec_rows, _twiddle(log2m, dev).data_ptr(), log2m,
+             out.data_ptr(), code, out.stride(0), out.stride(1),
+             _stream_ptr(dev))
+    return out
+
+
+def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
+                scale=1.0, out=None, kahan="chunk"):
+    """Device back-projection of [nrow, nslice, ncol] -> [ncol, nslice, ncol].
+
+    ``sino3`` may be float32, float16 or bfloat16 (last axis contiguous).
+    """
+    nrow, nslice, ncol = sino3.shape
+    dev = sino3.device
+    code = {torch.float32: nat.F32, torch.float16: nat.F16,
+            torch.bfloat16: nat.BF16}[sino3.dtype]
+    trig = _trig(angles, dev)
+    if out is None:
+        out = torch.empty((ncol, nslice, ncol), dtype=torch.float32,
+                          device=dev)
+    nat.call("atb_backproject", sino3.data_ptr(), code, sino3.stride(0),
+             sino3.stride(1), nrow, nslice, ncol, trig.data_ptr(),
+             float(np.float32(center)), int(bool(edge_pad)), float(mask_r2),
+             float(scale), out.data_ptr(), out.stride(0), out.stride(1),
+             1 if kahan == "angle" else 0, _stream_ptr(dev))
+    return out
+
+
+def _neg_log(sino3):
+    out = torch.empty_like(sino3)
+    nrow, nslice, ncol = sino3.shape
+    nat.call("atb_neg_log", sino3.data_ptr(), sino3.stride(0),
+             sino3.stride(1), nrow, nslice, ncol, out.data_ptr(),
+             out.stride(0), out.stride(1), _stream_ptr(sino3.device))
+    return out
+
+
+def _check_log_input(sinogram):
+    """Reference pre-step (``reconstruction.py:431-436``): warn on values
+    <= 0 and set them to 1 in the caller's array."""
+    if isinstance(sinogram, torch.Tensor):
+        bad = sinogram <= 0.0
+        if bool(bad.any()):
+            warnings.warn("!!!Applying logarithm is enabled but "
+                          "there are values <= 0.0 in the data!!!")
+            sinogram.masked_fill_(bad, 1.0)
+    else:
+        if np.any(sinogram <= 0.0):
+            warnings.warn("!!!Applying logarithm is enabled but "
+                          "there are values <= 0.0 in the data!!!")
+            sinogram[sinogram <= 0.0] = np.float32(1.0)
+
+
+def _validate(sinogram, center, angles):
+    shape = tuple(sinogram.shape)
+    if len(shape) == 3:
+        nrow, nslice, ncol = shape
+    elif len(shape) == 2:
+        (nrow, ncol), nslice = shape, 1
+    else:
+        raise ValueError("sinogram must be 2-D or 3-D")
+    if center < 0 or center >= ncol:
+        raise ValueError("Center is out of the range [0, {}]".format(ncol - 1))
+    if angles is None:
+        angles = np.deg2rad(np.linspace(0.0, 180.0, nrow))
+    else:
+        if len(angles) != nrow:
+            raise ValueError("!!!Number of angles is not the same as the row "
+                             "number of the sinogram!!!")
+        if isinstance(angles, torch.Tensor):
+            angles = angles.detach().cpu().numpy()
+    return nrow, nslice, ncol, np.asarray(angles, dtype=np.float64)
+
+
+def _mask_r2(ratio, center, ncol):
+    if ratio is None:
+        return -1.0
+    if ratio == 0.0:
+        ratio = min(center, ncol - center) / (0.5 * ncol)
+    radius = ratio * (ncol // 2)
+    return float(radius * radius)
+
+
+def _scale(nrow):
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return float(np.float32(np.pi) / np.float32(nrow - 1))
+
+
+def _finish(rec3, two_d, is_np, out, np_dtype=np.float32):
+    """Shape and hand back a [ncol, nslice, ncol] device result."""
+    res = rec3[:, 0, :] if two_d else rec3
+    if out is not None:
+        dst = out if isinstance(out, torch.Tensor) else torch.from_numpy(out)
+        if tuple(dst.shape) != tuple(res.shape):
+            raise ValueError("out has shape %s, expected %s"
+                             % (tuple(dst.shape), tuple(res.shape)))
+        # pinned host memory (e.g. torch pin_memory) gets a direct DMA
+        dst.copy_(res, non_blocking=dst.is_cuda or dst.is_pinned())
+        if not dst.is_cuda:
+            torch.cuda.current_stream(res.device).synchronize()
+        return out
+    if is_np:
+        return res.cpu().numpy().astype(np_dtype, copy=False)
+    return res
+
+
+# --------------------------------------------------------------------------
+# public drop-in API (algotom.rec.reconstruction names)
+# --------------------------------------------------------------------------
+def apply_ramp_filter(sinogram, ramp_win=None, filter_name=None, pad=None,
+                      pad_mode="edge"):
+    """Ramp filter of a 2-D sinogram; ``reconstruction.py:118-153``.
+
+    NumPy input returns float64 like the reference; tensors stay float32
+    on the device.
+    """
+    t, is_np = _to_device(sinogram)
+    nrow, ncol = t.shape
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    f = filter_sinograms(_as3(t), pad, pad_mode, False, ramp_win, filter_name)
+    f = f[:, 0, :]
+    return f.cpu().numpy().astype(np.float64) if is_np else f
+
+
+def back_projection_gpu(sinogram, angles, center, block=(16, 16),
+                        edge_pad=False):
+    """Back-projection of one sinogram; ``reconstruction.py:193-226``."""
+    t, is_np = _to_device(sinogram)
+    rec = backproject(_as3(t), angles, center, edge_pad=edge_pad)
+    return _finish(rec, True, is_np, None)
+
+
+def back_projection_gpu_chunk(sinograms, angles, center, block=(16, 16),
+                              edge_pad=False):
+    """Back-projection of [nrow, nslice, ncol]; ``reconstruction.py:267-304``."""
+    t, is_np = _to_device(sinograms)
+    rec = backproject(t, angles, center, edge_pad=edge_pad)
+    return _finish(rec, False, is_np, None)
+
+
+def back_projection_cpu(sinogram, angles, center, edge_pad=False):
+    """Name kept from ``reconstruction.py:307-359``; runs on the device."""
+    return back_projection_gpu(sinogram, angles, center, edge_pad=edge_pad)
+
+
+def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
+                       ramp_win=None, filter_name="hann", pad=None,
+                       pad_mode="edge", apply_log=True, gpu=True,
+                       block=(16, 16), ncore=None, *, out=None,
+                       storage="float32", kahan="chunk"):
+    """FBP of a 2-D [nrow, ncol] or 3-D [nrow, nslice, ncol] sinogram.
+
+    Drop-in for ``algotom.rec.reconstruction.fbp_reconstruction``
+    (``reconstruction.py:362-493``): -log (with the in-place <= 0 -> 1
+    replacement and warning), padded ramp-and-window filter, back-projection
+    without edge padding, circle mask (``ratio``; 0.0 picks the largest disc
+    inside the centred field), scale pi/(nrow-1).  Returns float32
+    [ncol, ncol] or [ncol, nslice, ncol].
+    """
+    nrow, nslice, ncol, angles = _validate(sinogram, center, angles)
+    if apply_log:
+        _check_log_input(sinogram)
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    t, is_np = _to_device(sinogram)
+    two_d = t.dim() == 2
+    f = filter_sinograms(_as3(t), pad, pad_mode, apply_log, ramp_win,
+                         filter_name, storage)
+    del t
+    rec = backproject(f, angles, center, edge_pad=False,
+                      mask_r2=_mask_r2(ratio, center, ncol),
+                      scale=_scale(nrow), kahan=kahan)
+    del f
+    return _finish(rec, two_d, is_np, out)
+
+
+def apply_circular_ramp_filter(rec_img, ramp_win=None, filter_name=None,
+                               pad=None, pad_mode="edge"):
+    """2-D circular ramp filter; ``reconstruction.py:527-560``.
+
+    ``real(ifft2(fft2(pad(x)) * ifftshift(W2)))`` cropped.  NumPy input
+    returns float64 like the reference.
+    """
+    t, is_np = _to_device(rec_img)
+    ncol = t.shape[0]
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    r = _circular_filter(t.unsqueeze(0), ramp_win, filter_name, pad,
+                         pad_mode)[0]
+    return r.cpu().numpy().astype(np.float64) if is_np else r
+
+
+def _circular_filter(stack, ramp_win, filter_name, pad, pad_mode):
+    """[nslice, ncol, ncol] float32 -> filtered, same shape (library 2-D FFT)."""
+    nslice, ncol, _ = stack.shape
+    n = ncol + 2 * pad
+    if ramp_win is None or np.shape(ramp_win) != (n, n):
+        ramp_win = make_circular_ramp_window(n, filter_name)
+    h = np.fft.ifftshift(np.asarray(ramp_win.cpu() if isinstance(
+        ramp_win, torch.Tensor) else ramp_win))
+    ht = torch.from_numpy(np.ascontiguousarray(h)).to(stack.device,
+                                                      torch.complex64)
+    mode = {"edge": "replicate", "reflect": "reflect", "wrap": "circular",
+            "constant": "constant"}.get(pad_mode)
+    out = torch.empty_like(stack)
+    for k in range(nslice):
+        x = stack[k]
+        if pad > 0:
+            if mode is None:
+                xp = torch.from_numpy(np.pad(x.cpu().numpy(), pad,
+                                             mode=pad_mode)).to(stack.device)
+            else:
+                xp = torch.nn.functional.pad(x[None, None], (pad,) * 4,
+                                             mode=mode)[0, 0]
+        else:
+            xp = x
+        y = torch.fft.ifft2(torch.fft.fft2(xp.to(torch.float32)) * ht).real
+        out[k] = y[pad:pad + ncol, pad:pad + ncol]
+    return out
+
+
+def bpf_reconstruction(sinogram, center, angles=None, ratio=1.0,
+                       ramp_win=None, filter_name="hann", pad=None,
+                       pad_mode="edge", apply_log=True, gpu=True,
+                       block=(16, 16), ncore=None, *, out=None,
+                       kahan="chunk"):
+    """BPF of a 2-D or 3-D sinogram; ``reconstruction.py:563-684``.
+
+    -log, back-projection of the unfiltered sinogram with edge padding, 2-D
+    circular ramp filter per slice, mask, scale pi/(nrow-1).  2-D NumPy
+    input returns float64 (as the reference does), 3-D float32.
+    """
+    nrow, nslice, ncol, angles = _validate(sinogram, center, angles)
+    if apply_log:
+        _check_log_input(sinogram)
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    t, is_np = _to_device(sinogram)
+    two_d = t.dim() == 2
+    s3 = _neg_log(_as3(t)) if apply_log else _as3(t)
+    bp = backproject(s3, angles, center, edge_pad=True, kahan=kahan)
+    del s3, t
+    stack = bp.permute(1, 0, 2).contiguous()  # [nslice, ncol, ncol]
+    filt = _circular_filter(stack, ramp_win, filter_name, pad, pad_mode)
+    r2 = _mask_r2(ratio, center, ncol)
+    if r2 >= 0:
+        c = ncol // 2
+        idx = torch.arange(ncol, device=filt.device) - c
+        m = ((idx[None, :] ** 2 + idx[:, None] ** 2).to(torch.float64) <= r2)
+        filt = filt * m.to(filt.dtype)
+    filt = filt * _scale(nrow)
+    rec = filt.permute(1, 0, 2)
+    return _finish(rec, two_d, is_np, out,
+                   np.float64 if two_d else np.float32)

@@ -1,0 +1,393 @@
+"""Benchmark: stacked FBP at 2560 detector pixels on B200.
+
+Workload (one "step"): FBP of 256 slices, each a seeded 12-ellipse phantom
+at 2560 x 2560, sinograms float32 [1801 angles over [0, pi), 256, 2560],
+Poisson noise at 5e3 photons then -log, centre 1278.3, hann filter,
+ratio 1.0, pad auto (150).  Metric: pixel-angle updates per second
+(updates per slice = 2560^2 * 1801), plus slices/s and the relative L2 error
+of a sampled slice against the FP64 oracle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one rank per GPU; each rank reconstructs its own
+256 slices (weak scaling, no collective on the data path).  Timing: CUDA
+events on the compute stream around K steps, bracketed by a barrier and a
+device synchronize, max over ranks.  Inputs (4.7 GB per rank) are larger
+than L2.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NSLICE, NROW, NCOL, CENTER = 256, 1801, 2560, 1278.3
+PHOTONS = 5e3
+METRIC = ("FBP pixel·angle updates/s and slices/s at 2560 det, "
+          "rel-L2 err vs FP64 oracle")
+WORKLOAD = ("stacked FBP: 256 slices x 1801 angles x 2560 det, float32, "
+            "centre 1278.3, hann, ratio 1.0, pad 150")
+# algorithmic FP32 work of one update (SURVEY 8(d) counting): position FMA,
+# fraction subtract, tap difference, interpolation FMA, accumulate add;
+# an FMA counts as 2 FLOP
+FLOP_PER_UPDATE = 7.0
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--slices", type=int, default=NSLICE)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def _traffic_per_update():
+    """DRAM bytes per update of the back-projection kernel, from the
+    committed ncu summary (profiles/backproject_*.md), if present."""
+    d = os.path.join(ROOT, "profiles")
+    try:
+        names = sorted(os.listdir(d))
+    except OSError:
+        return None
+    for n in names:
+        if n.startswith("backproject") and n.endswith(".md"):
+            m = re.search(r"dram_bytes_per_update:\s*([0-9.eE+-]+)",
+                          open(os.path.join(d, n)).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+def make_sinograms(nslice, device, seed0=2000):
+    """[NROW, nslice, NCOL] float32 on the device; seed = 2*1000 + slice."""
+    import torch
+    from algotom_b200 import phantom
+    out = torch.empty((NROW, nslice, NCOL), dtype=torch.float32, device=device)
+    ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
+    for k in range(nslice):
+        s, _, _ = phantom.ellipse_sinogram(seed0 + k, NROW, NCOL, CENTER,
+                                           photons=PHOTONS, angles=ang,
+                                           device=device)
+        out[:, k, :] = s
+    return out, ang
+
+
+def cpu_fbp_sample(nslice_max, budget_s, nthreads=None):
+    """Reference-arithmetic CPU FBP (oracle port) on a bounded slice sample."""
+    from algotom_b200 import phantom
+    from oracle import cpu_port
+    ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
+    done, t_total = 0, 0.0
+    nt = nthreads or cpu_port.max_threads()
+    # warm the thread pool / FFT plans on a small case
+    cpu_port.fbp_reconstruction(np.ones((16, 1, 64), np.float32), 31.5,
+                                np.linspace(0, np.pi, 16), nthreads=nt)
+    while done < 1 or (done < nslice_max and t_total < budget_s):
+        s, _, _ = phantom.ellipse_sinogram(2000 + done, NROW, NCOL, CENTER,
+                                           photons=PHOTONS, angles=ang)
+        t0 = time.perf_counter()
+        cpu_port.fbp_reconstruction(s[:, None, :], CENTER, ang, nthreads=nt)
+        t_total += time.perf_counter() - t0
+        done += 1
+    ups = done * NCOL * NCOL * NROW / t_total
+    return ups, done, t_total, nt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    steps = []
+    for i in range(args.warmup + args.steps):
+        ups, done, t, nt = cpu_fbp_sample(1, 0.0)
+        if i >= args.warmup:
+            steps.append(t)
+    t_step = statistics.mean(steps)
+    ups = NCOL * NCOL * NROW / t_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ups,
+        "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded ellipse phantoms)",
+        "config": {"workload": WORKLOAD, "slices": NSLICE, "nrow": NROW,
+                   "ncol": NCOL, "sample": "1 slice per step"},
+        "slices_per_s": 1.0 / t_step,
+        "cpu_baseline": {"value": ups, "unit": "updates/s", "cores": nt,
+                         "kind": "port",
+                         "sample": "1 of 256 slices per step (1801 x 2560): "
+                                   "numpy filter + C back-projection with "
+                                   "the reference's arithmetic"},
+        "e2e": {"value": ups, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from algotom_b200.rec import reconstruction as R
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nslice = args.slices
+    sino, ang = make_sinograms(nslice, dev, seed0=2000 + rank * nslice)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+
+    def step(src, out=None):
+        return R.fbp_reconstruction(src, CENTER, angles=ang, ratio=1.0,
+                                    filter_name="hann", apply_log=False,
+                                    out=out)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing (value)
+    for _ in range(args.warmup):
+        rec = step(sino)
+        del rec
+    clock = ClockSampler(local_rank)
+    barrier()
+    clock.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rec = step(sino)
+        del rec
+    e1.record(stream)
+    barrier()
+    clocks = clock.stop()
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    upd_step = nslice * NCOL * NCOL * NROW
+    value = world * upd_step * args.steps / t_dev
+
+    # ---- per-kernel timing (roofline): filter and back-projection alone
+    from algotom_b200.rec import reconstruction as RR
+    filt = RR.filter_sinograms(sino, 150, "edge", False, None, "hann")
+    mask_r2 = RR._mask_r2(1.0, CENTER, NCOL)
+    scale = RR._scale(NROW)
+    outb = torch.empty((NCOL, nslice, NCOL), dtype=torch.float32, device=dev)
+    for _ in range(2):
+        RR.backproject(filt, ang, CENTER, False, mask_r2, scale, out=outb)
+    nk = max(2, args.steps)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    for _ in range(nk):
+        RR.backproject(filt, ang, CENTER, False, mask_r2, scale, out=outb)
+    ev[1].record(stream)
+    ev[2].record(stream)
+    for _ in range(nk):
+        f2 = RR.filter_sinograms(sino, 150, "edge", False, None, "hann")
+        del f2
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    t_bp = ev[0].elapsed_time(ev[1]) / 1e3 / nk
+    t_filt = ev[2].elapsed_time(ev[3]) / 1e3 / nk
+    del filt, outb
+
+    # ---- end-to-end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.empty((NROW, nslice, NCOL), dtype=torch.float32,
+                              pin_memory=True)
+        host_in.copy_(sino)
+        host_out = torch.empty((NCOL, nslice, NCOL), dtype=torch.float32,
+                               pin_memory=True)
+        hin, hout = host_in.numpy(), host_out.numpy()
+        del sino
+        torch.cuda.empty_cache()
+        step(hin, out=hout)
+        barrier()
+        t0 = time.perf_counter()
+        k_e2e = max(1, min(args.steps, 3))
+        for _ in range(k_e2e):
+            step(hin, out=hout)
+        barrier()
+        t_e2e = max_over_ranks((time.perf_counter() - t0) / k_e2e)
+        e2e = {"value": world * upd_step / t_e2e, "unit": "updates/s",
+               "h2d_bytes_per_step": int(host_in.numel() * 4),
+               "d2h_bytes_per_step": int(host_out.numel() * 4),
+               "ms_per_step": t_e2e * 1e3, "steps": k_e2e}
+        rec_sample = torch.from_numpy(hout[:, 0, :].copy())
+        sino_sample = host_in[:, 0, :].numpy().copy()
+    else:
+        rec_sample = step(sino)[:, 0, :].cpu()
+        sino_sample = sino[:, 0, :].cpu().numpy()
+
+    if rank != 0:
+        return
+
+    # ---- accuracy of slice 0 against the FP64 oracle; CPU baseline
+    err = None
+    cpu = None
+    if not args.no_oracle:
+        from oracle import cpu_port
+        from oracle import fbp_oracle as O
+        f = O.apply_ramp_filter(sino_sample, None, "hann", 150, "edge")
+        ref = cpu_port.back_projection(f.astype(np.float32), ang, CENTER,
+                                       ref_arith=False)
+        ref = ref * O.make_circle_mask(NCOL, 1.0) * (np.pi / (NROW - 1))
+        got = rec_sample.numpy()
+        err = {"rel_l2": O.rel_l2(got, ref),
+               "max_abs": float(np.abs(got - ref).max()),
+               "max_rel_to_peak": float(np.abs(got - ref).max()
+                                        / np.abs(ref).max()),
+               "slices_checked": 1}
+        if world == 1:
+            ups, done, t, nt = cpu_fbp_sample(8, 15.0)
+            cpu = {"value": ups, "unit": "updates/s", "cores": nt,
+                   "kind": "port",
+                   "sample": "%d of 256 slices (1801 x 2560), %.1f s: numpy "
+                             "filter + C back-projection with the "
+                             "reference's arithmetic" % (done, t)}
+
+    peaks, src = _peaks()
+    f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    fp32_peak = 2.0 * 128 * 148 * f_clk / 1e12          # TFLOP/s
+    bp_upd = nslice * NCOL * NCOL * NROW
+    achieved = FLOP_PER_UPDATE * bp_upd / t_bp / 1e12
+    tpu = _traffic_per_update()
+    filt_bytes = NROW * nslice * NCOL * 8.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 12-ellipse phantoms, Poisson 5e3 photons)",
+        "config": {"workload": WORKLOAD, "slices_per_gpu": nslice,
+                   "nrow": NROW, "ncol": NCOL, "center": CENTER,
+                   "storage": "float32", "kahan": "chunk",
+                   "l2": "inputs larger than L2 (4.7 GB sinogram per GPU)"},
+        "slices_per_s": world * nslice * args.steps / t_dev,
+        "accuracy": err,
+        "roofline": {"bound": "fp32", "kernel": "bp_tile_kernel",
+                     "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": (tpu * bp_upd if tpu else None),
+                     "flop_per_update": FLOP_PER_UPDATE,
+                     "ms_per_launch": t_bp * 1e3,
+                     "peak_source": "FP32 FMA pipe, 148 SM x 128 lanes x "
+                                    "sm_max_mhz (%s)" % src},
+        "filter_roofline": {"bound": "hbm", "kernel": "filter_rows_kernel",
+                            "achieved": filt_bytes / t_filt / 1e9,
+                            "peak": float(peaks.get("hbm_gbs", 6650.0)),
+                            "unit": "GB/s",
+                            "frac": filt_bytes / t_filt / 1e9
+                            / float(peaks.get("hbm_gbs", 6650.0)),
+                            "ms_per_launch": t_filt * 1e3},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = _args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,132 @@
+/*
+ * algotom_b200 -- C ABI of the B200 filtered-back-projection library.
+ *
+ * These are the entry points a foreign-function binding of algotom's FBP /
+ * BPF hot path (algotom 1.6.0, algotom/rec/reconstruction.py) calls.  They
+ * take plain device pointers, element strides and sizes; the caller owns
+ * every buffer and the library never frees caller memory.  Every call is
+ * asynchronous on the given stream (cudaStream_t passed as void*, NULL for
+ * the legacy default stream) and re-entrant per stream.
+ *
+ * Return value: 0 on success, a negative ATB_E* code otherwise; the message
+ * of the calling thread's last failure is atb_last_error().  The library
+ * never aborts and never traps the device.
+ *
+ * Layouts follow the reference: a sinogram stack is [nrow angles][nslice]
+ * [ncol detector pixels] and a reconstruction stack is [ncol rows (y)]
+ * [nslice][ncol columns (x)].  Row and slice strides are in elements; the
+ * detector (x) axis is contiguous.
+ */
+#ifndef ALGOTOM_B200_H
+#define ALGOTOM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define ATB_OK 0
+#define ATB_EINVAL (-1)   /* bad argument: size, stride, pointer, enum */
+#define ATB_ECUDA (-2)    /* a CUDA runtime call failed */
+#define ATB_ERANGE (-3)   /* size beyond what this build supports */
+
+/* element types of sinogram storage */
+#define ATB_F32 0
+#define ATB_F16 1
+#define ATB_BF16 2
+
+/* numpy.pad modes along the detector axis (reconstruction.py:146) */
+#define ATB_PAD_EDGE 0
+#define ATB_PAD_CONSTANT 1     /* constant_values = 0 */
+#define ATB_PAD_REFLECT 2
+#define ATB_PAD_SYMMETRIC 3
+#define ATB_PAD_WRAP 4
+#define ATB_PAD_LINEAR_RAMP 5  /* end_values = 0 */
+#define ATB_PAD_MEAN 6
+#define ATB_PAD_MAXIMUM 7
+#define ATB_PAD_MINIMUM 8
+#define ATB_PAD_MEDIAN 9
+
+/* Library version as major*10000 + minor*100 + patch. */
+int atb_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *atb_last_error(void);
+
+/*
+ * Smallest log2 of the FFT length the row filter uses for a detector width
+ * `ncol` and pad `pad`: M = 2^log2m >= (ncol + 2 pad) + ncol - 1, so that the
+ * circular convolution of length ncol + 2 pad is reproduced exactly on the
+ * cropped window.  Returns a negative code if the row does not fit one CTA.
+ */
+int atb_filter_log2m(int ncol, int pad);
+
+/*
+ * Padded ramp-and-window filter of every row of a sinogram stack, with the
+ * optional -log folded in; replaces apply_ramp_filter
+ * (algotom/rec/reconstruction.py:118-153) and the -log pre-step
+ * (reconstruction.py:431-436; values <= 0 read as 1, i.e. give 0).
+ *
+ *   src      float32 [nrow][nslice][ncol] at src_row_stride / src_slice_stride
+ *   pad      detector padding on each side; pad_mode one of ATB_PAD_*
+ *   spec     complex64 [spec_rows][2^log2m]: spectrum of the periodised real
+ *            kernel, already scaled by 2^-log2m.  spec_rows = 1 (one kernel
+ *            for every row) or nrow (one kernel per angle; then two slices of
+ *            one angle share a transform)
+ *   twiddle  complex64 [2^log2m]: exp(-2 pi i t / 2^log2m)
+ *   dst      [nrow][nslice][ncol] of dst_dtype (ATB_F32/F16/BF16) at
+ *            dst_row_stride / dst_slice_stride
+ */
+int atb_filter_rows(const float *src, int64_t src_row_stride,
+                    int64_t src_slice_stride, int nrow, int nslice, int ncol,
+                    int pad, int pad_mode, int apply_log, const void *spec,
+                    int spec_rows, const void *twiddle, int log2m, void *dst,
+                    int dst_dtype, int64_t dst_row_stride,
+                    int64_t dst_slice_stride, void *stream);
+
+/*
+ * Elementwise -log of a float32 sinogram stack, values <= 0 read as 1;
+ * the BPF pre-step (reconstruction.py:632-637).  dst may equal src.
+ */
+int atb_neg_log(const float *src, int64_t src_row_stride,
+                int64_t src_slice_stride, int nrow, int nslice, int ncol,
+                float *dst, int64_t dst_row_stride, int64_t dst_slice_stride,
+                void *stream);
+
+/*
+ * Linear-interpolation back-projection of a stack of sinograms that share
+ * angles and centre; replaces __back_projection_gpu_kernel /
+ * back_projection_gpu (reconstruction.py:156-226),
+ * __back_projection_gpu_chunk_kernel / back_projection_gpu_chunk
+ * (reconstruction.py:229-304) and back_projection_cpu
+ * (reconstruction.py:307-359), fused with the circle mask and the
+ * pi/(nrow-1) scale of fbp_reconstruction (reconstruction.py:488-493).
+ *
+ *   sino     [nrow][nslice][ncol] of sino_dtype at the given strides
+ *   trig     float64 [nrow][2] = (cos(-a), sin(-a)) for the float32-rounded
+ *            angles a
+ *   center   float32-rounded rotation centre, as a double
+ *   edge_pad 0: positions outside [0, ncol-1] add nothing (FBP);
+ *            1: they add the nearest edge sample (BPF)
+ *   mask_r2  < 0: no mask; else pixels with (x-c)^2 + (y-c)^2 > mask_r2,
+ *            c = ncol/2 (integer division), are written as 0
+ *   scale    multiplies every written pixel
+ *   out      float32 [ncol][nslice][ncol] at out_row_stride / out_slice_stride
+ *   flags    bit 0: per-angle compensated (Kahan) accumulation instead of
+ *            the default chunked Kahan (FP32 partials over a chunk of angles,
+ *            compensated across chunks)
+ */
+int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
+                    int64_t sino_slice_stride, int nrow, int nslice, int ncol,
+                    const double *trig, double center, int edge_pad,
+                    double mask_r2, float scale, float *out,
+                    int64_t out_row_stride, int64_t out_slice_stride,
+                    int flags, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALGOTOM_B200_H */

@@ -1,0 +1,164 @@
+/*
+ * C restatement of algotom's CPU back-projector -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Follows back_projection_cpu (algotom/rec/reconstruction.py:307-359): per
+ * angle the reference takes cos/sin of the float32 value -angle in float32
+ * (Numba types math.cos(float32) as float32), forms the detector position
+ * in float64, interpolates with a float32 tap difference and adds the
+ * float64 value into a float32 image.  With ref_arith = 1 this routine does
+ * exactly that, so its output matches the single-threaded reference bit for
+ * bit (built with -ffp-contract=off, as Numba does not contract).  The
+ * reference runs prange over ANGLES and races on the shared image; here the
+ * image rows are handed out to POSIX threads instead, which keeps each
+ * pixel's additions in angle order and makes the result deterministic.
+ *
+ * With ref_arith = 0 it is an FP64 checker: float64 trig of the
+ * float32-rounded angle, float64 tap difference and a float64 accumulator
+ * (out is double*).
+ *
+ * Used as the timed CPU baseline (kind "port") and by the tests as a fast
+ * FP64 oracle at sizes where the NumPy restatement is slow.  Never linked
+ * into, or called by, the product library.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <unistd.h>
+
+typedef struct {
+    const float *sino;
+    long long sino_stride;
+    int nrow, ncol, edge_pad, ref_arith;
+    const double *ct, *st;
+    double cen;
+    void *out;
+    long long out_stride;
+    int next_row;            /* shared row counter, taken under `lock` */
+    pthread_mutex_t lock;
+} bp_job;
+
+/* Image row y of one sinogram: every angle in order, as the reference adds
+ * them into pixel (y, x). */
+static void bp_row(bp_job *j, int y)
+{
+    const int ncol = j->ncol, w1 = ncol - 1;
+    const double ic = 0.5 * (double)w1;
+    const double yc = (double)y - ic;
+    float *of = j->ref_arith ? (float *)j->out + (long long)y * j->out_stride
+                             : 0;
+    double *od = j->ref_arith ? 0
+                              : (double *)j->out + (long long)y * j->out_stride;
+    for (int x = 0; x < ncol; ++x) {
+        if (of) of[x] = 0.0f; else od[x] = 0.0;
+    }
+    for (int i = 0; i < j->nrow; ++i) {
+        const float *row = j->sino + (long long)i * j->sino_stride;
+        const double c = j->ct[i], ys = yc * j->st[i];
+        for (int x = 0; x < ncol; ++x) {
+            double f = ((double)x - ic) * c + ys + j->cen;
+            double val;
+            if (f >= 0.0 && f <= (double)w1) {
+                int d = (int)floor(f);
+                int u = (int)ceil(f);
+                if (u != d) {
+                    float yd = row[d];
+                    /* the reference subtracts the float32 taps in float32 */
+                    double dv = j->ref_arith ? (double)(row[u] - yd)
+                                             : (double)row[u] - (double)yd;
+                    val = (double)yd + dv * (f - (double)d);
+                } else {
+                    val = (double)row[d];
+                }
+            } else if (j->edge_pad) {
+                val = (double)(f < 0.0 ? row[0] : row[w1]);
+            } else {
+                continue;
+            }
+            if (of) of[x] = (float)((double)of[x] + val);
+            else od[x] += val;
+        }
+    }
+}
+
+static void *bp_worker(void *arg)
+{
+    bp_job *j = (bp_job *)arg;
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        int y0 = j->next_row;
+        j->next_row += 4;
+        pthread_mutex_unlock(&j->lock);
+        if (y0 >= j->ncol) break;
+        int y1 = y0 + 4 < j->ncol ? y0 + 4 : j->ncol;
+        for (int y = y0; y < y1; ++y) bp_row(j, y);
+    }
+    return 0;
+}
+
+/* One sinogram [nrow, ncol] (row stride `sino_stride` floats) to an image
+ * [ncol, ncol] whose rows are `out_stride` elements apart. */
+static void bp_one(const float *sino, long long sino_stride, int nrow,
+                   int ncol, const float *angles, float center, int edge_pad,
+                   int ref_arith, void *out, long long out_stride,
+                   int nthreads)
+{
+    bp_job j;
+    double *ct = (double *)malloc(sizeof(double) * (size_t)(nrow + 1));
+    double *st = (double *)malloc(sizeof(double) * (size_t)(nrow + 1));
+    for (int i = 0; i < nrow; ++i) {
+        float th = -angles[i];
+        if (ref_arith) {
+            ct[i] = (double)cosf(th);
+            st[i] = (double)sinf(th);
+        } else {
+            ct[i] = cos((double)th);
+            st[i] = sin((double)th);
+        }
+    }
+    j.sino = sino; j.sino_stride = sino_stride; j.nrow = nrow; j.ncol = ncol;
+    j.edge_pad = edge_pad; j.ref_arith = ref_arith; j.ct = ct; j.st = st;
+    j.cen = (double)center; j.out = out; j.out_stride = out_stride;
+    j.next_row = 0;
+    pthread_mutex_init(&j.lock, 0);
+    if (nthreads > ncol) nthreads = ncol;
+    if (nthreads <= 1) {
+        bp_worker(&j);
+    } else {
+        pthread_t *t = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nthreads);
+        for (int k = 0; k < nthreads; ++k) pthread_create(&t[k], 0, bp_worker, &j);
+        for (int k = 0; k < nthreads; ++k) pthread_join(t[k], 0);
+        free(t);
+    }
+    pthread_mutex_destroy(&j.lock);
+    free(ct);
+    free(st);
+}
+
+/* Stack [nrow, nslice, ncol] -> [ncol, nslice, ncol]; nslice = 1 with a
+ * plain 2-D sinogram.  Returns 0. */
+int oracle_backproject(const float *sino, int nrow, int nslice, int ncol,
+                       const float *angles, float center, int edge_pad,
+                       int ref_arith, void *out, int nthreads)
+{
+    if (nthreads < 1) nthreads = 1;
+    for (int k = 0; k < nslice; ++k) {
+        const float *s = sino + (long long)k * ncol;
+        if (ref_arith) {
+            float *o = (float *)out + (long long)k * ncol;
+            bp_one(s, (long long)nslice * ncol, nrow, ncol, angles, center,
+                   edge_pad, 1, o, (long long)nslice * ncol, nthreads);
+        } else {
+            double *o = (double *)out + (long long)k * ncol;
+            bp_one(s, (long long)nslice * ncol, nrow, ncol, angles, center,
+                   edge_pad, 0, o, (long long)nslice * ncol, nthreads);
+        }
+    }
+    return 0;
+}
+
+int oracle_max_threads(void)
+{
+    long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n > 0 ? (int)n : 1;
+}

@@ -1,0 +1,180 @@
+"""Generate golden input/output vectors by running the reference itself.
+
+Run in a container that has the algotom 1.6.0 source tree (default
+``/root/reference``, or ``$ALGOTOM_REF``) plus numpy/scipy/numba/joblib:
+
+    python tests/golden/make_golden.py
+
+The reference imports ``pywt`` and ``h5py`` at module level
+(``algotom/util/utility.py:58``, ``algotom/io/loadersaver.py:44``); neither is
+used on the FBP/BPF path, so empty stand-in modules are registered first.
+``NUMBA_NUM_THREADS=1`` is forced because the reference's multi-threaded
+``back_projection_cpu`` races on its output (``prange`` over angles with a
+shared ``+=``, ``algotom/rec/reconstruction.py:333,351``); single-threaded it
+is deterministic.
+
+Outputs (``tests/golden/*.npz``) hold the inputs next to the reference's
+outputs so that tests need neither the reference nor this script.
+"""
+import os
+import sys
+import types
+import warnings
+
+os.environ["NUMBA_NUM_THREADS"] = "1"
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
+
+import numpy as np  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("ALGOTOM_REF", "/root/reference")
+
+for _m in ("pywt", "h5py"):
+    sys.modules.setdefault(_m, types.ModuleType(_m))
+sys.path.insert(0, REF)
+sys.path.insert(0, REPO)
+
+import scipy.ndimage as ndi  # noqa: E402
+import algotom.rec.reconstruction as rec  # noqa: E402
+import algotom.util.utility as util  # noqa: E402
+from algotom_b200 import phantom  # noqa: E402
+
+WINDOWS = ["hann", "bartlett", "blackman", "hamming", "nuttall", "parzen",
+           "triang", None]
+PAD_MODES = ["edge", "constant", "reflect", "symmetric", "wrap",
+             "linear_ramp", "mean", "maximum", "minimum", "median"]
+
+
+def _key(*parts):
+    return "__".join(str(p) for p in parts)
+
+
+def make_windows():
+    out = {}
+    for w in (64, 65):
+        for name in WINDOWS:
+            out[_key("smooth", name, w)] = rec.make_smoothing_window(name, w)
+            out[_key("ramp2d", name, w)] = rec.make_2d_ramp_window(2, w, name)
+        for name in ("hann", None):
+            out[_key("circ", name, w)] = rec.make_circular_ramp_window(w, name)
+    for w, ratio in ((65, 1.0), (64, 0.7), (97, 0.93)):
+        out[_key("mask", w, ratio)] = util.make_circle_mask(w, ratio)
+    np.savez_compressed(os.path.join(HERE, "golden_windows.npz"), **out)
+
+
+def make_filter():
+    sino, _, _ = phantom.ellipse_sinogram(11, 32, 96, 47.5, photons=1e4)
+    out = {"sino": sino}
+    for mode in PAD_MODES:
+        out[_key("filt", mode, "hann", "None")] = rec.apply_ramp_filter(
+            sino, None, "hann", None, mode)
+    for name in WINDOWS:
+        out[_key("filt", "edge", name, "None")] = rec.apply_ramp_filter(
+            sino, None, name, None, "edge")
+    for pad in (0, 7, 200):
+        for mode in ("edge", "reflect", "wrap"):
+            out[_key("filt", mode, "hann", pad)] = rec.apply_ramp_filter(
+                sino, None, "hann", pad, mode)
+    # odd width: N = ncol + 2 pad odd, H Hermitian
+    sino_odd, _, _ = phantom.ellipse_sinogram(12, 24, 81, 40.0, photons=1e4)
+    out["sino_odd"] = sino_odd
+    out[_key("filtodd", "edge", "hann", "None")] = rec.apply_ramp_filter(
+        sino_odd, None, "hann", None, "edge")
+    # the reference returns float64; float32 storage keeps the fixture small
+    # and is far below the 1e-6 tolerance these vectors are checked at
+    out = {k: (v.astype(np.float32) if v.dtype == np.float64 else v)
+           for k, v in out.items()}
+    np.savez_compressed(os.path.join(HERE, "golden_filter.npz"), **out)
+
+
+def make_bp():
+    n, nrow = 96, 72
+    sino, ang, _ = phantom.ellipse_sinogram(21, nrow, n, 47.5, photons=1e4)
+    f = rec.apply_ramp_filter(sino, None, "hann", None, "edge")
+    f = np.float32(f)
+    out = {"filtered": f, "angles": ang}
+    for cen in (47.5, 45.3, 52.0):
+        for ep in (False, True):
+            out[_key("bp", cen, int(ep))] = rec.back_projection_cpu(
+                f, np.float32(ang), np.float32(cen), ep)
+    # odd width, 360-degree angles including the endpoint
+    n2, nrow2 = 81, 61
+    ang2 = np.deg2rad(np.linspace(0.0, 360.0, nrow2))
+    s2, _, _ = phantom.ellipse_sinogram(22, nrow2, n2, 40.0, photons=1e4,
+                                        angles=ang2)
+    f2 = np.float32(rec.apply_ramp_filter(s2, None, "hann", None, "edge"))
+    out["filtered_odd"] = f2
+    out["angles_odd"] = ang2
+    for ep in (False, True):
+        out[_key("bpodd", 40.0, int(ep))] = rec.back_projection_cpu(
+            f2, np.float32(ang2), np.float32(40.0), ep)
+    np.savez_compressed(os.path.join(HERE, "golden_bp.npz"), **out)
+
+
+def make_recon():
+    n, nrow = 96, 73
+    sino, ang, _ = phantom.ellipse_sinogram(31, nrow, n, 47.5, photons=1e4)
+    trans = np.exp(-sino).astype(np.float32)  # transmission, for apply_log
+    trans[5, 10] = 0.0
+    trans[9, 3] = -0.5
+    out = {"sino": sino, "trans": trans, "angles": ang}
+    for name, fn in (("fbp", rec.fbp_reconstruction),
+                     ("bpf", rec.bpf_reconstruction)):
+        for ratio in (1.0, 0.0, None):
+            out[_key(name, "2d", ratio)] = fn(sino.copy(), 47.5, angles=ang,
+                                              ratio=ratio, apply_log=False,
+                                              gpu=False)
+        out[_key(name, "2d", "defang")] = fn(sino.copy(), 45.3,
+                                             apply_log=False, gpu=False)
+        out[_key(name, "2d", "nofilter", "reflect")] = fn(
+            sino.copy(), 47.5, angles=ang, filter_name=None, pad=10,
+            pad_mode="reflect", apply_log=False, gpu=False)
+        t = trans.copy()
+        with warnings.catch_warnings(record=True) as caught:
+            warnings.simplefilter("always")
+            out[_key(name, "2d", "log")] = fn(t, 47.5, angles=ang,
+                                              apply_log=True, gpu=False)
+        out[_key(name, "2d", "log", "warned")] = np.array(len(caught) > 0)
+        out[_key(name, "2d", "log", "mutated")] = t
+        s3 = np.stack([sino, 0.5 * sino, sino[:, ::-1].copy()], axis=1)
+        out[_key(name, "3d", 0.0)] = fn(s3.copy(), 47.5, angles=ang,
+                                        ratio=0.0, apply_log=False,
+                                        gpu=False, ncore=1)
+        out[_key(name, "3d1", 1.0)] = fn(s3[:, :1].copy(), 47.5, angles=ang,
+                                         apply_log=False, gpu=False, ncore=1)
+    out["s3"] = np.stack([sino, 0.5 * sino, sino[:, ::-1].copy()], axis=1)
+    dtypes = {k: str(v.dtype) for k, v in out.items()}
+    out = {k: (v.astype(np.float32) if v.dtype == np.float64 and
+               k.startswith(("fbp", "bpf")) else v) for k, v in out.items()}
+    out["dtypes"] = np.array(repr(dtypes))
+    np.savez_compressed(os.path.join(HERE, "golden_recon.npz"), **out)
+
+
+def make_reference_test_fixture():
+    """The reference's own unit-test phantom (test_reconstruction.py:50-65)."""
+    size = 64
+    mat = np.zeros((size + 1, size + 1), dtype=np.float32)
+    mat[20:40, 30:45] = np.float32(1.0)
+    mat = ndi.gaussian_filter(mat, 2.0)
+    sino_360 = np.zeros((73, size + 1), dtype=np.float32)
+    angles = np.linspace(0.0, 360.0, len(sino_360), dtype=np.float32)
+    for i, angle in enumerate(angles):
+        sino_360[i] = np.sum(ndi.rotate(mat, -angle, reshape=False), axis=0)
+    out = {"mat": mat, "sino_360": sino_360, "angles_deg": angles}
+    out["fbp_180"] = rec.fbp_reconstruction(sino_360[:37].copy(), 32,
+                                            apply_log=False, gpu=False)
+    out["bpf_180"] = rec.bpf_reconstruction(sino_360[:37].copy(), 32,
+                                            apply_log=False, gpu=False)
+    np.savez_compressed(os.path.join(HERE, "golden_unittest.npz"), **out)
+
+
+if __name__ == "__main__":
+    make_windows()
+    make_filter()
+    make_bp()
+    make_recon()
+    make_reference_test_fixture()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,77 @@
+"""The C-ABI library: it loads, exports every declared symbol, and rejects
+bad arguments with error codes (no device work is started by these calls)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from algotom_b200 import _native as nat
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "algotom_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(atb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_symbols_are_exported():
+    lib = nat.load()
+    declared = _declared()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(nat.EXPORTS)
+
+
+def test_version_and_no_error():
+    assert nat.load().atb_version() >= 100
+    assert isinstance(nat.last_error(), str)
+
+
+def test_filter_log2m():
+    assert nat.call("atb_filter_log2m", 1024, 150) == 12   # 2347 -> 4096
+    assert nat.call("atb_filter_log2m", 2560, 150) == 13   # 5419 -> 8192
+    assert nat.call("atb_filter_log2m", 96, 14) == 8
+    rc = nat.load().atb_filter_log2m(20000, 150)
+    assert rc == -3 and "2^" in nat.last_error()
+    assert nat.load().atb_filter_log2m(0, 1) == -1
+
+
+def test_bad_arguments_are_rejected():
+    lib = nat.load()
+    # null pointers
+    rc = lib.atb_backproject(None, 0, 0, 0, 10, 1, 10, None, 5.0, 0, -1.0,
+                             1.0, None, 0, 0, 0, None)
+    assert rc == -1 and "null" in nat.last_error()
+    rc = lib.atb_filter_rows(None, 0, 0, 1, 1, 8, 0, 0, 0, None, 1, None, 4,
+                             None, 0, 0, 0, None)
+    assert rc == -1
+    # bad shapes / enums are checked before any device work (dummy
+    # non-null pointers are never dereferenced on these paths)
+    p = ctypes.c_void_p(16)
+    rc = lib.atb_backproject(p, 0, 0, 0, 0, 1, 10, p, 5.0, 0, -1.0, 1.0, p,
+                             0, 0, 0, None)
+    assert rc == -1 and "shape" in nat.last_error()
+    rc = lib.atb_backproject(p, 0, 0, 0, 10, 1, 10, p, 10.0, 0, -1.0, 1.0, p,
+                             0, 0, 0, None)
+    assert rc == -1 and "center" in nat.last_error()
+    rc = lib.atb_backproject(p, 7, 0, 0, 10, 1, 10, p, 5.0, 0, -1.0, 1.0, p,
+                             0, 0, 0, None)
+    assert rc == -1 and "dtype" in nat.last_error()
+    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 42, 0, p, 1, p, 5, p, 0, 0,
+                             0, None)
+    assert rc == -1 and "pad_mode" in nat.last_error()
+    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 1, p, 4, p, 0, 0,
+                             0, None)
+    assert rc == -1 and "2^4" in nat.last_error()
+    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 3, p, 5, p, 0, 0,
+                             0, None)
+    assert rc == -1 and "spec_rows" in nat.last_error()
+
+
+def test_call_raises_with_message():
+    with pytest.raises(nat.NativeLibraryError, match="atb_filter_log2m"):
+        nat.call("atb_filter_log2m", -5, 0)

@@ -1,0 +1,277 @@
+"""Parity of the CUDA path (through the C ABI) with the reference and oracle.
+
+Tolerances: the filter and every FP32 reconstruction must be within 1e-5
+relative L2 of the FP64 oracle (the bar this path is held to); against the
+reference's own float32 outputs (golden vectors) the same bound applies.
+"""
+import numpy as np
+import pytest
+import torch
+
+from algotom_b200 import _native as nat
+from algotom_b200 import phantom
+from algotom_b200.rec import reconstruction as R
+from oracle import cpu_port
+from oracle import fbp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+WINDOWS = ["hann", "bartlett", "blackman", "hamming", "nuttall", "parzen",
+           "triang", None]
+PAD_MODES = ["edge", "constant", "reflect", "symmetric", "wrap",
+             "linear_ramp", "mean", "maximum", "minimum", "median"]
+TOL = 1e-5
+
+
+# ----------------------------------------------------------------- filter
+@pytest.mark.parametrize("mode", PAD_MODES)
+def test_filter_pad_modes(cuda, golden, mode):
+    g = golden("filter")
+    got = R.apply_ramp_filter(g["sino"], None, "hann", None, mode)
+    assert got.dtype == np.float64 and got.shape == g["sino"].shape
+    assert O.rel_l2(got, g["filt__%s__hann__None" % mode]) < 1e-6
+    assert O.rel_l2(got, O.apply_ramp_filter(g["sino"], None, "hann", None,
+                                             mode)) < 1e-6
+
+
+@pytest.mark.parametrize("name", WINDOWS)
+def test_filter_windows(cuda, golden, name):
+    g = golden("filter")
+    got = R.apply_ramp_filter(g["sino"], None, name, None, "edge")
+    assert O.rel_l2(got, g["filt__edge__%s__None" % name]) < 1e-6
+
+
+@pytest.mark.parametrize("pad", [0, 7, 200])
+@pytest.mark.parametrize("mode", ["edge", "reflect", "wrap"])
+def test_filter_pads(cuda, golden, pad, mode):
+    g = golden("filter")
+    got = R.apply_ramp_filter(g["sino"], None, "hann", pad, mode)
+    assert O.rel_l2(got, g["filt__%s__hann__%d" % (mode, pad)]) < 1e-6
+
+
+def test_filter_odd_and_tiny_rows(cuda, golden):
+    g = golden("filter")
+    got = R.apply_ramp_filter(g["sino_odd"], None, "hann", None, "edge")
+    assert O.rel_l2(got, g["filtodd__edge__hann__None"]) < 1e-6
+    rng = np.random.default_rng(0)
+    for ncol, nrow in ((1, 3), (2, 1), (5, 7), (3, 2)):
+        x = rng.standard_normal((nrow, ncol)).astype(np.float32)
+        for mode in ("edge", "reflect", "symmetric", "median"):
+            got = R.apply_ramp_filter(x, None, "hann", 4, mode)
+            ref = O.apply_ramp_filter(x, None, "hann", 4, mode)
+            assert np.abs(got - ref).max() <= 1e-6 * max(1.0, np.abs(ref).max())
+
+
+def test_filter_per_row_window(cuda):
+    """A ramp window that differs per row takes the per-angle path."""
+    sino, _, _ = phantom.ellipse_sinogram(3, 20, 64, 31.5)
+    n = 64 + 2 * 9
+    win = O.make_2d_ramp_window(20, n, "hann")
+    win = win * np.linspace(0.5, 1.5, 20)[:, None]
+    got = R.apply_ramp_filter(sino, win, None, 9)
+    assert O.rel_l2(got, O.apply_ramp_filter(sino, win, None, 9)) < 1e-6
+    # a stack with the same per-row window: two slices per transform
+    s3 = np.stack([sino, 2 * sino, -sino], axis=1)
+    t = torch.from_numpy(s3).cuda()
+    f = R.filter_sinograms(t, 9, "edge", False, win, None)
+    for k in range(3):
+        ref = O.apply_ramp_filter(s3[:, k], win, None, 9)
+        assert O.rel_l2(f[:, k].cpu().numpy(), ref) < 1e-6
+
+
+def test_filter_with_log(cuda):
+    sino, _, _ = phantom.ellipse_sinogram(4, 30, 80, 39.5)
+    trans = np.exp(-sino).astype(np.float32)
+    t = torch.from_numpy(trans[:, None, :]).cuda()
+    f = R.filter_sinograms(t, 12, "edge", True, None, "hann")[:, 0]
+    ref = O.apply_ramp_filter(-np.log(trans.astype(np.float64)), None,
+                              "hann", 12)
+    assert O.rel_l2(f.cpu().numpy(), ref) < 1e-6
+
+
+def test_filter_limits(cuda):
+    x = np.zeros((2, 9000), np.float32)
+    with pytest.raises(nat.NativeLibraryError, match="2\\^"):
+        R.apply_ramp_filter(x, None, "hann", 150)
+    got = R.apply_ramp_filter(np.ones((2, 8000), np.float32), None, "hann",
+                              150)
+    assert np.all(np.isfinite(got))
+
+
+# ---------------------------------------------------------- back-projection
+@pytest.mark.parametrize("cen", [47.5, 45.3, 52.0])
+@pytest.mark.parametrize("ep", [0, 1])
+def test_backprojection_vs_reference(cuda, golden, cen, ep):
+    g = golden("bp")
+    got = R.back_projection_gpu(g["filtered"], g["angles"], cen,
+                                edge_pad=bool(ep))
+    assert got.dtype == np.float32 and got.shape == (96, 96)
+    oracle = O.back_projection(g["filtered"], g["angles"], cen, bool(ep))
+    assert O.rel_l2(got, oracle) < 1e-6
+    assert O.rel_l2(got, g["bp__%s__%d" % (cen, ep)]) < TOL
+
+
+@pytest.mark.parametrize("ep", [0, 1])
+def test_backprojection_odd_360(cuda, golden, ep):
+    g = golden("bp")
+    f, a = g["filtered_odd"], g["angles_odd"]
+    got = R.back_projection_gpu(f, a, 40.0, edge_pad=bool(ep))
+    assert O.rel_l2(got, O.back_projection(f, a, 40.0, bool(ep))) < 1e-6
+    assert O.rel_l2(got, g["bpodd__40.0__%d" % ep]) < TOL
+
+
+@pytest.mark.parametrize("ncol,nrow,cen", [
+    (17, 5, 8.0), (64, 33, 31.5), (65, 64, 0.0), (100, 1, 99.99),
+    (130, 97, 64.2), (257, 31, 128.0), (63, 2, 62.0)])
+@pytest.mark.parametrize("ep", [0, 1])
+def test_backprojection_shapes_and_centres(cuda, ncol, nrow, cen, ep):
+    rng = np.random.default_rng(ncol * 7 + nrow)
+    s = rng.standard_normal((nrow, ncol)).astype(np.float32)
+    ang = np.concatenate([[0.0, np.pi / 2], rng.uniform(-4, 8, nrow)])[:nrow]
+    got = R.back_projection_gpu(s, ang, cen, edge_pad=bool(ep))
+    ref = O.back_projection(s, ang, cen, bool(ep))
+    assert O.rel_l2(got, ref) < 1e-6
+
+
+def test_backprojection_chunk_and_kahan_modes(cuda):
+    rng = np.random.default_rng(11)
+    s3 = rng.standard_normal((45, 3, 70)).astype(np.float32)
+    ang = np.linspace(0, np.pi, 45)
+    got = R.back_projection_gpu_chunk(s3, ang, 34.7)
+    assert got.shape == (70, 3, 70)
+    t = torch.from_numpy(s3).cuda()
+    got2 = R.backproject(t, ang, 34.7, kahan="angle").cpu().numpy()
+    for k in range(3):
+        ref = O.back_projection(s3[:, k], ang, 34.7)
+        assert O.rel_l2(got[:, k], ref) < 1e-6
+        assert O.rel_l2(got2[:, k], ref) < 1e-6
+
+
+def test_backprojection_deterministic(cuda):
+    s, ang, _ = phantom.ellipse_sinogram(8, 181, 300, 149.5)
+    t = torch.from_numpy(s).cuda()
+    a = R.backproject(t[:, None], ang, 149.5)
+    b = R.backproject(t[:, None], ang, 149.5)
+    assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("storage", ["float16", "bfloat16"])
+def test_reduced_storage_reports_error(cuda, storage):
+    """FP16/BF16 filtered storage: FP32 accumulation, bounded error."""
+    s, ang, _ = phantom.ellipse_sinogram(9, 180, 256, 127.5)
+    ref = O.fbp_reconstruction(s, 127.5, angles=ang, apply_log=False)
+    got = R.fbp_reconstruction(s, 127.5, angles=ang, apply_log=False,
+                               storage=storage)
+    err = O.rel_l2(got, ref)
+    assert err < (2e-3 if storage == "float16" else 1.5e-2)
+
+
+# ------------------------------------------------------------ FBP and BPF
+@pytest.mark.parametrize("name", ["fbp", "bpf"])
+def test_recon_2d_vs_reference(cuda, golden, name):
+    g = golden("recon")
+    fn = R.fbp_reconstruction if name == "fbp" else R.bpf_reconstruction
+    dtypes = eval(str(g["dtypes"]))
+    sino, ang = g["sino"], g["angles"]
+    tol = TOL if name == "fbp" else 2e-5
+    for ratio in (1.0, 0.0, None):
+        key = "%s__2d__%s" % (name, ratio)
+        got = fn(sino.copy(), 47.5, angles=ang, ratio=ratio, apply_log=False)
+        assert str(got.dtype) == dtypes[key]
+        assert O.rel_l2(got, g[key]) < tol
+    got = fn(sino.copy(), 45.3, apply_log=False)
+    assert O.rel_l2(got, g["%s__2d__defang" % name]) < tol
+    got = fn(sino.copy(), 47.5, angles=ang, filter_name=None, pad=10,
+             pad_mode="reflect", apply_log=False)
+    ref_o = (O.fbp_reconstruction if name == "fbp" else O.bpf_reconstruction)(
+        sino, 47.5, angles=ang, filter_name=None, pad=10, pad_mode="reflect",
+        apply_log=False)
+    assert O.rel_l2(got, ref_o) < tol
+    t = g["trans"].copy()
+    with pytest.warns(UserWarning, match="values <= 0.0"):
+        got = fn(t, 47.5, angles=ang, apply_log=True)
+    np.testing.assert_array_equal(t, g["%s__2d__log__mutated" % name])
+    assert O.rel_l2(got, g["%s__2d__log" % name]) < tol
+
+
+@pytest.mark.parametrize("name", ["fbp", "bpf"])
+def test_recon_3d_vs_reference(cuda, golden, name):
+    g = golden("recon")
+    fn = R.fbp_reconstruction if name == "fbp" else R.bpf_reconstruction
+    tol = TOL if name == "fbp" else 2e-5
+    got = fn(g["s3"].copy(), 47.5, angles=g["angles"], ratio=0.0,
+             apply_log=False, ncore=1)
+    assert got.shape == (96, 3, 96) and got.dtype == np.float32
+    assert O.rel_l2(got, g["%s__3d__0.0" % name]) < tol
+    got = fn(g["s3"][:, :1].copy(), 47.5, angles=g["angles"], apply_log=False)
+    assert got.shape == (96, 1, 96)
+    assert O.rel_l2(got, g["%s__3d1__1.0" % name]) < tol
+
+
+def test_reference_unittests_ported(cuda, golden):
+    """tests/test_rec/test_reconstruction.py:88-202 of the reference."""
+    g = golden("unittest")
+    mat, s360 = g["mat"], g["sino_360"]
+    s180 = s360[:37]
+    ang_deg = g["angles_deg"]
+    for fn, key in ((R.fbp_reconstruction, "fbp_180"),
+                    (R.bpf_reconstruction, "bpf_180")):
+        rec1 = fn(s180.copy(), 32, apply_log=False, gpu=True)
+        assert np.max(np.abs(mat - rec1)) <= 0.1
+        assert O.rel_l2(rec1, g[key]) < 2e-5
+        rec2 = fn(s360.copy(), 32, angles=np.deg2rad(ang_deg),
+                  apply_log=False, gpu=True)
+        assert np.max(np.abs(mat - rec2)) <= 0.1
+        stack = np.pad(np.expand_dims(s180, 1), ((0, 0), (2, 2), (0, 0)),
+                       mode="edge")
+        rs = fn(stack.copy(), 32, apply_log=False, gpu=True, ratio=0.0,
+                ncore=1)
+        assert np.max(np.abs(mat - rs[:, 0, :])) <= 0.1 and rs.shape[1] == 5
+        rs = fn(stack.copy(), 32, apply_log=False, gpu=True, ratio=1.0,
+                ncore=None)
+        assert np.max(np.abs(mat - rs[:, 0, :])) <= 0.1
+        rs = fn(stack.copy(), 32, apply_log=False, gpu=False,
+                angles=np.deg2rad(ang_deg[:37]), ratio=0.0, ncore=1)
+        assert np.median(np.abs(mat - rs[:, 0, :])) <= 0.2
+        with pytest.warns(Warning):
+            fn(s180.copy(), 32, apply_log=True)
+        with pytest.raises(ValueError):
+            fn(s180, 32, np.deg2rad(ang_deg), apply_log=False)
+        with pytest.raises(ValueError):
+            fn(s180, -1, apply_log=False)
+
+
+def test_torch_inputs_stay_on_device(cuda):
+    s, ang, _ = phantom.ellipse_sinogram(2, 90, 128, 63.5)
+    t = torch.from_numpy(s).cuda()
+    rec = R.fbp_reconstruction(t, 63.5, angles=ang, apply_log=False)
+    assert isinstance(rec, torch.Tensor) and rec.is_cuda
+    ref = O.fbp_reconstruction(s, 63.5, angles=ang, apply_log=False)
+    assert O.rel_l2(rec.cpu().numpy(), ref) < TOL
+
+
+# ------------------------------------------------ full single-slice sizes
+def _fbp_oracle_fast(sino, center, angles, pad=None):
+    """FP64 FBP with the C FP64 back-projector (oracle at full size)."""
+    nrow, ncol = sino.shape
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    f = O.apply_ramp_filter(sino, None, "hann", pad, "edge")
+    rec = cpu_port.back_projection(f.astype(np.float32), angles, center,
+                                   ref_arith=False)
+    # the FP64 back-projector takes float32 taps; the filter error of that
+    # rounding (~6e-8) is far below the tolerance
+    mask = O.make_circle_mask(ncol, 1.0)
+    return rec * mask * (np.pi / (nrow - 1))
+
+
+@pytest.mark.parametrize("ncol,nrow,cen", [(1024, 900, 511.5),
+                                           (2560, 1801, 1278.3)])
+def test_full_size_single_slice(cuda, ncol, nrow, cen):
+    """The benchmark shapes: 1024^2 x 900 and one 2560^2 x 1801 slice."""
+    s, ang, _ = phantom.ellipse_sinogram(1000 + ncol, nrow, ncol, cen,
+                                         photons=1e4)
+    got = R.fbp_reconstruction(s, cen, angles=ang, apply_log=False)
+    ref = _fbp_oracle_fast(s, cen, ang)
+    err = O.rel_l2(got, ref)
+    assert err < TOL, err

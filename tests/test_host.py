@@ -1,0 +1,127 @@
+"""Host-side logic of the drop-in, checked on the CPU.
+
+The product builds its filter constants in FP64 on the host; these tests
+check them against the golden windows and, through a NumPy model of the
+device filter (the same power-of-two embedding and two-rows-per-transform
+packing the kernel uses), against the oracle's filter.
+"""
+import numpy as np
+import pytest
+
+from algotom_b200 import phantom
+from algotom_b200.rec import windows as W
+from oracle import fbp_oracle as O
+
+WINDOWS = ["hann", "bartlett", "blackman", "hamming", "nuttall", "parzen",
+           "triang", None]
+
+
+def test_product_windows_match_reference(golden):
+    g = golden("windows")
+    for w in (64, 65):
+        for name in WINDOWS:
+            np.testing.assert_array_equal(W.make_smoothing_window(name, w),
+                                          g["smooth__%s__%d" % (name, w)])
+            np.testing.assert_allclose(W.make_2d_ramp_window(2, w, name),
+                                       g["ramp2d__%s__%d" % (name, w)],
+                                       rtol=0, atol=1e-15)
+        for name in ("hann", None):
+            np.testing.assert_allclose(W.make_circular_ramp_window(w, name),
+                                       g["circ__%s__%d" % (name, w)],
+                                       rtol=0, atol=1e-14)
+    for w, ratio in ((65, 1.0), (64, 0.7), (97, 0.93)):
+        np.testing.assert_array_equal(W.make_circle_mask(w, ratio),
+                                      g["mask__%d__%s" % (w, ratio)])
+
+
+def _device_filter_model(x2, pad, mode, window_row):
+    """NumPy model of atb_filter_rows for two rows."""
+    ncol = x2.shape[1]
+    log2m = W.next_log2(2 * ncol + 2 * pad - 1)
+    m = 1 << log2m
+    spec = W.row_filter_spectrum(window_row, ncol, pad, log2m)[0]
+    xp = np.pad(x2, ((0, 0), (pad, pad)), mode=mode)
+    z = np.zeros(m, complex)
+    z[:ncol + 2 * pad] = xp[0] + 1j * xp[1]
+    w = np.fft.fft(np.conj(np.fft.fft(z) * spec))
+    return np.stack([w.real[pad:pad + ncol], -w.imag[pad:pad + ncol]])
+
+
+@pytest.mark.parametrize("ncol,pad", [(96, 14), (81, 12), (50, 0), (33, 80)])
+@pytest.mark.parametrize("name", ["hann", None, "parzen"])
+def test_spectrum_embedding_reproduces_filter(ncol, pad, name):
+    rng = np.random.default_rng(ncol + pad)
+    x = rng.standard_normal((2, ncol))
+    got = _device_filter_model(x, pad, "edge",
+                               W.ramp_window_row(ncol + 2 * pad, name))
+    ref = O.apply_ramp_filter(x, None, name, pad, "edge")
+    assert O.rel_l2(got, ref) < 1e-6   # complex64 spectrum
+
+
+def test_spectrum_rejects_short_fft():
+    with pytest.raises(ValueError):
+        W.row_filter_spectrum(W.ramp_window_row(100, "hann"), 80, 10, 7)
+
+
+def test_twiddles():
+    t = W.twiddles(6)
+    np.testing.assert_allclose(t, np.exp(-2j * np.pi * np.arange(64) / 64),
+                               atol=1e-7)
+
+
+def test_phantom_sinogram_is_exact_line_integral():
+    """Exact invariants of the analytic projections of one ellipse: every
+    angle carries the same mass mu/n * pi A B, centred on the projected
+    ellipse centre."""
+    x0, y0, a, b, phi, mu = 5.0, -3.0, 20.0, 9.0, 0.4, 0.7
+    params = np.array([[x0, y0, a, b, phi, mu]])
+    n = 96
+    ang = np.linspace(0.0, np.pi, 7)
+    sino = phantom.analytic_sinogram(params, ang, n, 47.5, size=n)
+    j = np.arange(n)
+    for i, th in enumerate(ang):
+        mass = sino[i].sum()
+        assert mass == pytest.approx(mu / n * np.pi * a * b, rel=1e-2)
+        cen = (sino[i] * j).sum() / mass
+        assert cen == pytest.approx(x0 * np.cos(th) - y0 * np.sin(th) + 47.5,
+                                    abs=0.1)
+    # and the FBP of it reproduces the rasterised ellipse
+    rec = O.fbp_reconstruction(phantom.analytic_sinogram(
+        params, np.linspace(0, np.pi, 360, endpoint=False), n, 47.5),
+        47.5, angles=np.linspace(0, np.pi, 360, endpoint=False),
+        apply_log=False)
+    img = phantom.phantom_image(params, n)
+    inside = img > 0
+    assert np.median(rec[inside]) == pytest.approx(mu / n, rel=0.05)
+
+
+def test_phantom_seeded():
+    a, ang, p = phantom.ellipse_sinogram(5, 30, 64, 31.5)
+    b, _, q = phantom.ellipse_sinogram(5, 30, 64, 31.5)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(p, q)
+    assert a.dtype == np.float32 and a.shape == (30, 64)
+    assert np.all(np.isfinite(a))
+
+
+def test_dropin_validation_before_device():
+    """Argument errors of the reference are raised before any device use."""
+    from algotom_b200.rec import reconstruction as R
+    s = np.ones((10, 20), np.float32)
+    with pytest.raises(ValueError, match="Center"):
+        R.fbp_reconstruction(s, -1, apply_log=False)
+    with pytest.raises(ValueError, match="Center"):
+        R.bpf_reconstruction(s, 20, apply_log=False)
+    with pytest.raises(ValueError, match="Number of angles"):
+        R.fbp_reconstruction(s, 10, angles=np.zeros(7), apply_log=False)
+    with pytest.raises(ValueError):
+        R.fbp_reconstruction(np.ones(5), 1, apply_log=False)
+
+
+def test_dropin_mask_and_scale_helpers():
+    from algotom_b200.rec import reconstruction as R
+    assert R._mask_r2(None, 10, 20) < 0
+    assert R._mask_r2(1.0, 10, 20) == 100.0
+    # ratio 0: largest disc inside the centred field
+    assert R._mask_r2(0.0, 7.0, 20) == pytest.approx((0.7 * 10) ** 2)
+    assert R._scale(181) == pytest.approx(np.pi / 180, rel=1e-7)
