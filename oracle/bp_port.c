@@ -39,44 +39,71 @@ typedef struct {
 } bp_job;
 
 /* Image row y of one sinogram: every angle in order, as the reference adds
- * them into pixel (y, x). */
+ * them into pixel (y, x).  The inner loop is written branch-free (clamped
+ * position, select on the in-range test) so that compilers vectorise it; the
+ * arithmetic per in-range pixel is the reference's: when ceil == floor the
+ * tap difference is multiplied by an exact zero, giving s[d] as the
+ * reference's separate branch does for finite data.  gcc emits AVX-512,
+ * AVX2 and baseline clones and picks one at load time. */
+__attribute__((target_clones("avx512f", "avx2", "default")))
 static void bp_row(bp_job *j, int y)
 {
     const int ncol = j->ncol, w1 = ncol - 1;
     const double ic = 0.5 * (double)w1;
     const double yc = (double)y - ic;
-    float *of = j->ref_arith ? (float *)j->out + (long long)y * j->out_stride
-                             : 0;
-    double *od = j->ref_arith ? 0
-                              : (double *)j->out + (long long)y * j->out_stride;
+    const double wmax = (double)w1;
+    float *restrict of = j->ref_arith
+        ? (float *)j->out + (long long)y * j->out_stride : 0;
+    double *restrict od = j->ref_arith
+        ? 0 : (double *)j->out + (long long)y * j->out_stride;
     for (int x = 0; x < ncol; ++x) {
         if (of) of[x] = 0.0f; else od[x] = 0.0;
     }
     for (int i = 0; i < j->nrow; ++i) {
-        const float *row = j->sino + (long long)i * j->sino_stride;
-        const double c = j->ct[i], ys = yc * j->st[i];
-        for (int x = 0; x < ncol; ++x) {
-            double f = ((double)x - ic) * c + ys + j->cen;
-            double val;
-            if (f >= 0.0 && f <= (double)w1) {
-                int d = (int)floor(f);
-                int u = (int)ceil(f);
-                if (u != d) {
-                    float yd = row[d];
-                    /* the reference subtracts the float32 taps in float32 */
-                    double dv = j->ref_arith ? (double)(row[u] - yd)
-                                             : (double)row[u] - (double)yd;
-                    val = (double)yd + dv * (f - (double)d);
-                } else {
-                    val = (double)row[d];
-                }
-            } else if (j->edge_pad) {
-                val = (double)(f < 0.0 ? row[0] : row[w1]);
-            } else {
-                continue;
+        const float *restrict row = j->sino + (long long)i * j->sino_stride;
+        const double c = j->ct[i], ys = yc * j->st[i], cen = j->cen;
+        const float e0 = row[0], e1 = row[w1];
+        if (of && !j->edge_pad) {
+            for (int x = 0; x < ncol; ++x) {
+                const double f = ((double)x - ic) * c + ys + cen;
+                const int inr = (f >= 0.0) & (f <= wmax);
+                const double fc = inr ? f : 0.0;
+                const int d = (int)fc;
+                const int u = d + (fc > (double)d);
+                const float yd = row[d];
+                const float dv = row[u] - yd;
+                const double val = (double)yd + (double)dv * (fc - (double)d);
+                const float upd = (float)((double)of[x] + val);
+                of[x] = inr ? upd : of[x];
             }
-            if (of) of[x] = (float)((double)of[x] + val);
-            else od[x] += val;
+        } else if (of) {
+            for (int x = 0; x < ncol; ++x) {
+                const double f = ((double)x - ic) * c + ys + cen;
+                const int inr = (f >= 0.0) & (f <= wmax);
+                const double fc = inr ? f : 0.0;
+                const int d = (int)fc;
+                const int u = d + (fc > (double)d);
+                const float yd = row[d];
+                const float dv = row[u] - yd;
+                double val = (double)yd + (double)dv * (fc - (double)d);
+                const double ev = (double)(f < 0.0 ? e0 : e1);
+                val = inr ? val : ev;
+                of[x] = (float)((double)of[x] + val);
+            }
+        } else {
+            for (int x = 0; x < ncol; ++x) {
+                const double f = ((double)x - ic) * c + ys + cen;
+                const int inr = (f >= 0.0) & (f <= wmax);
+                const double fc = inr ? f : 0.0;
+                const int d = (int)fc;
+                const int u = d + (fc > (double)d);
+                const double yd = (double)row[d];
+                const double dv = (double)row[u] - yd;
+                const double val = yd + dv * (fc - (double)d);
+                const double ev = j->edge_pad ? (double)(f < 0.0 ? e0 : e1)
+                                              : 0.0;
+                od[x] += inr ? val : ev;
+            }
         }
     }
 }

@@ -130,7 +130,9 @@ def test_backprojection_shapes_and_centres(cuda, ncol, nrow, cen, ep):
     ang = np.concatenate([[0.0, np.pi / 2], rng.uniform(-4, 8, nrow)])[:nrow]
     got = R.back_projection_gpu(s, ang, cen, edge_pad=bool(ep))
     ref = O.back_projection(s, ang, cen, bool(ep))
-    assert O.rel_l2(got, ref) < 1e-6
+    # white-noise sinograms have neighbour differences as large as the
+    # values, so FP32 positions weigh more than on phantom data
+    assert O.rel_l2(got, ref) < TOL
 
 
 def test_backprojection_chunk_and_kahan_modes(cuda):
@@ -143,8 +145,8 @@ def test_backprojection_chunk_and_kahan_modes(cuda):
     got2 = R.backproject(t, ang, 34.7, kahan="angle").cpu().numpy()
     for k in range(3):
         ref = O.back_projection(s3[:, k], ang, 34.7)
-        assert O.rel_l2(got[:, k], ref) < 1e-6
-        assert O.rel_l2(got2[:, k], ref) < 1e-6
+        assert O.rel_l2(got[:, k], ref) < TOL
+        assert O.rel_l2(got2[:, k], ref) < TOL
 
 
 def test_backprojection_deterministic(cuda):
