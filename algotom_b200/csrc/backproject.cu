@@ -8,53 +8,72 @@
 // 0 <= p <= ncol - 1; outside it adds nothing, or with edge padding the
 // nearest edge sample.
 //
-// Work decomposition.  A CTA of 256 threads owns a 64 x 64 pixel tile of one
-// slice and walks the angles in chunks of kChunk.  For every angle of a chunk
-// the tile only sees detector bins [lo, lo + kWin) (its footprint is at most
-// 63 (|cos| + |sin|) + 2 < 92 bins wide), so the CTA stages just that window
-// into shared memory, as interpolation pairs
+// Work decomposition.  A CTA of 256 threads owns a pixel tile of S slices
+// that share angles and centre, and walks the angles in chunks.  For every
+// angle of a chunk the tile only sees a window of kWin detector bins (its
+// footprint is at most (TX-1)|cos| + (TY-1)|sin| + 2 bins wide), so the CTA
+// stages just that window, per slice, into shared memory as interpolation
+// pairs
 //     (a_j, D_j) = (s[lo+j] - (j-H) D_j, s[lo+j+1] - s[lo+j]),  H = kWin/2
 // so that the value at the window-centred local position q = p - lo - H,
-// bin j = floor(q) + H, is the single FMA a_j + D_j q.  Centring keeps |q|
-// and |j-H| below 48, which bounds the rounding of both terms.  Bins outside the detector hold (0, 0) (or the edge
-// value with D = 0 when edge padding), which reproduces the reference's
-// bounds exactly wherever the interpolant is continuous.  The two detector
-// edges of FBP (no edge padding) are discontinuities: positions just inside
-// count, positions just outside add nothing.  Angles whose tile footprint
-// reaches either edge take a checked path (a CTA-uniform branch) that tests
-// every position against both edges and re-decides, in FP64 with the
-// reference's own expression, any position within 2e-3 bins of an edge --
-// e.g. at 90 degrees whole pixel rows sit 1e-8 bins from position 0, which
-// no FP32 local coordinate can resolve.
+// bin j = floor(q) + H, is the single FMA a_j + D_j q.  With S >= 2 the pairs
+// of two slices sit in one 16-byte word (a_0, a_1, D_0, D_1): one LDS.128,
+// one packed fma.rn.f32x2 and one packed add.rn.f32x2 update two slices,
+// and the position, floor and address work is shared by all S slices.
+//
+// Staging is double-buffered: while a chunk is being accumulated, the raw
+// detector windows of the next chunk stream into shared memory with cp.async
+// (16-byte copies when the rows are 16-byte aligned, 4-byte copies
+// otherwise); a short pass then turns them into pairs.  16-bit storage is
+// read straight from global memory by that pass.
+//
+// Bounds: bins outside the detector hold (0, 0) (or the edge value with
+// D = 0 under edge padding), which reproduces the reference wherever the
+// interpolant is continuous.  The two detector edges of FBP (no edge
+// padding) are discontinuities: angles whose tile footprint reaches either
+// edge take a checked path (a CTA-uniform branch) that tests every position
+// against both edges and re-decides, in FP64 with the reference's own
+// expression, any position within 2e-3 bins of an edge -- at exactly 90
+// degrees whole pixel rows sit 1e-8 bins from position 0, which no FP32 local
+// coordinate can resolve.
 //
 // Positions: the tile-origin position is formed in FP64 per (tile, angle)
-// from FP64 trigonometry of the float32-rounded angle; inside the tile each
-// thread adds its small offset in FP32, so q is accurate to ~1e-5 bins.
-// floor(q) is taken with one round-down add of 1.5 * 2^23, whose bit pattern
-// is the shared-memory index.
+// from FP64 trigonometry of the float32-rounded angle; each thread adds its
+// in-tile offset in FP32, so q is accurate to ~1e-5 bins at any image size.
+// floor(q) is one round-down add of 1.5 * 2^23, whose bit pattern is the
+// shared-memory index.
 //
 // Accumulation: FP32 partial sums over each chunk of angles, added across
-// chunks with Kahan compensation (flag bit 0 switches to per-angle Kahan).
-// Each thread holds 4 x 4 pixels laid out so that one warp instruction
-// covers an 8 x 4 pixel block: its 32 lanes read a compact run of <= 12
-// neighbouring pairs, which shared memory serves without bank conflicts.
+// chunks with Kahan compensation (the single-slice kernel can instead
+// compensate every angle).  One warp instruction covers an 8 x 4 pixel
+// block, whose 32 lanes read a run of about 9 neighbouring bins.
 #include "common.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTile = 64;   // tile edge (pixels)
-constexpr int kChunk = 32;  // angles per staged chunk
-constexpr int kWin = 96;    // staged pairs per angle (>= 63 sqrt(2) + 4)
-constexpr int kHalf = kWin / 2;
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
-constexpr int kPX = 4, kPY = 4;  // pixels per thread along x, y
+constexpr float kEdgeTol = 2e-3f;  // bins; FP32 error of q is < 3e-5
+
+// Tile geometry per slices-per-CTA S.  Warp tile = (8 PX) x (4 PY) pixels,
+// CTA = WX x WY warps (WX * WY = 8).
+template <int S> struct Geo;
+template <> struct Geo<1> {
+  static constexpr int PX = 4, PY = 4, WX = 2, WY = 4, kChunk = 32, kWin = 96;
+};
+template <> struct Geo<2> {
+  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 32, kWin = 80;
+};
+template <> struct Geo<4> {
+  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 16, kWin = 80;
+};
 
 struct BPArgs {
   const void *sino;
   long long srs, sss;
   int nrow, nslice, ncol;
+  int slice_base;  // first slice of this launch
   const double2 *trig;
   double center;
   int edge_pad;
@@ -62,19 +81,17 @@ struct BPArgs {
   float scale;
   float *out;
   long long ors, oss;
-  int per_angle_kahan;
+  int vec16;  // float32 rows 16-byte aligned: stage with 16-byte cp.async
 };
 
 struct __align__(16) AngleParam {
-  float qbase;  // local position of the tile-origin pixel, q = p - lo - kHalf
+  float qbase;  // local position of the tile-origin pixel, q = p - lo - H
   float c, s;   // cos(-a), sin(-a) in FP32 for in-tile offsets
   float qmax;   // local position of detector bin ncol - 1
   float qlo;    // local position of detector bin 0
-  int j0;       // window index of detector bin 0 (= -lo)
+  int j0;       // window index of detector bin 0
   double c64, s64;  // FP64 trigonometry, for the exact edge decision
 };
-
-constexpr float kEdgeTol = 2e-3f;  // bins; FP32 error of q is < 3e-5
 
 __device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
   const float y = __fsub_rn(v, comp);
@@ -83,44 +100,104 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float v) {
   sum = t;
 }
 
-template <typename T, bool kPerAngleKahan>
-__global__ void __launch_bounds__(kThreads, 2) bp_tile_kernel(BPArgs a) {
-  __shared__ float2 pairs[kChunk * kWin];
-  __shared__ AngleParam prm[kChunk];
-  __shared__ int lo_s[kChunk];
-  __shared__ int flag_s[kChunk];  // bit 0: skip angle, bit 1: checked path
+// packed FP32 pairs (Blackwell f32x2 arithmetic)
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+// acc += d * q + a in both lanes
+__device__ __forceinline__ void fma_acc2(unsigned long long &acc, unsigned long long av, unsigned long long dv,
+                                         unsigned long long q) {
+  unsigned long long v;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(v) : "l"(dv), "l"(q), "l"(av));
+  asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc) : "l"(v));
+}
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <typename T, int S>
+struct BPCfg {
+  using G = Geo<S>;
+  static constexpr int PX = G::PX, PY = G::PY, WX = G::WX;
+  static constexpr int TX = 8 * PX * G::WX, TY = 4 * PY * G::WY;
+  static constexpr int kChunk = G::kChunk, kWin = G::kWin, kHalf = kWin / 2;
+  static constexpr int kRaw = ((kWin + 1 + 3 + 3) / 4) * 4;  // raw floats per window, 4-aligned start
+  static constexpr bool kAsync = sizeof(T) == 4;
+  static constexpr int kPairBytes = 8 * S;  // per bin: S (a, D) pairs
+  static constexpr size_t kPairsSmem = (size_t)kChunk * kWin * kPairBytes;
+  static constexpr size_t kRawSmem = kAsync ? 2 * (size_t)kChunk * S * kRaw * 4 : 0;
+  static constexpr size_t kSmem = kPairsSmem + kRawSmem;
+};
+
+template <typename T, int S, bool kPerAngleKahan>
+__global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
+  using K = BPCfg<T, S>;
+  constexpr int PX = K::PX, PY = K::PY, TX = K::TX, TY = K::TY;
+  constexpr int kChunk = K::kChunk, kWin = K::kWin, kHalf = K::kHalf, kRaw = K::kRaw;
+  constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
+
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char *pairs = smem;                                   // [kChunk][kWin][S pairs]
+  float *raw = reinterpret_cast<float *>(smem + K::kPairsSmem);  // [2][kChunk][S][kRaw]
+  __shared__ AngleParam prm[2][kChunk];
+  __shared__ int lo_s[2][kChunk];
+  __shared__ int flag_s[2][kChunk];  // bit 0: skip angle, bit 1: checked path
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
-  const int slice = blockIdx.z;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int slice0 = a.slice_base + blockIdx.z * S;
+  const int nsl = min(S, a.nslice - slice0);  // live slices of this CTA
   const int ncol = a.ncol;
-  const T *sino = reinterpret_cast<const T *>(a.sino) + slice * a.sss;
+  const T *sino = reinterpret_cast<const T *>(a.sino) + slice0 * a.sss;
 
-  // thread -> pixel offsets inside the tile: warp w covers 32 x 16 pixels,
-  // lane (lx, ly) of an 8 x 4 block, replicated 4 x 4 times
-  const int tx = (warp & 1) * 32 + (lane & 7);
-  const int ty = (warp >> 1) * 16 + (lane >> 3);
+  // thread -> pixel offsets inside the tile: warp (wx, wy) covers
+  // (8 PX) x (4 PY) pixels, lane (lx, ly) an 8 x 4 block replicated PX x PY
+  const int tx = (warp % K::WX) * (8 * PX) + (lane & 7);
+  const int ty = (warp / K::WX) * (4 * PY) + (lane >> 3);
 
-  float acc[kPY][kPX], sum[kPY][kPX], comp[kPY][kPX];
+  // accumulators: FP32 chunk partials (packed two slices per word when
+  // S >= 2) and the compensated running totals
+  float accf[PY][PX];
+  unsigned long long acc2[PY][PX][NP];
+  float sum[PY][PX][S], comp[PY][PX][S];
 #pragma unroll
-  for (int b = 0; b < kPY; ++b)
+  for (int b = 0; b < PY; ++b)
 #pragma unroll
-    for (int c = 0; c < kPX; ++c) { acc[b][c] = 0.f; sum[b][c] = 0.f; comp[b][c] = 0.f; }
+    for (int c = 0; c < PX; ++c) {
+      accf[b][c] = 0.f;
+#pragma unroll
+      for (int g = 0; g < NP; ++g) acc2[b][c][g] = 0ull;
+#pragma unroll
+      for (int k = 0; k < S; ++k) { sum[b][c][k] = 0.f; comp[b][c][k] = 0.f; }
+    }
 
   const double ic = 0.5 * (double)(ncol - 1);
-  const double ext = (double)(kTile - 1);
+  const int nchunk = (a.nrow + kChunk - 1) / kChunk;
 
-  for (int i0 = 0; i0 < a.nrow; i0 += kChunk) {
-    // (1) per-angle window and local-position parameters, FP64
+  // per-angle window and local-position parameters of chunk k, FP64
+  auto params = [&](int k, int buf) {
     if (tid < kChunk) {
-      const int i = i0 + tid;
+      const int i = k * kChunk + tid;
       int flag = 1, lo = 0;
       AngleParam p = {0.f, 0.f, 0.f, 0.f, 0.f, 0, 0.0, 0.0};
       if (i < a.nrow) {
         const double2 cs = a.trig[i];
         const double P0 = ((double)x0 - ic) * cs.x + ((double)y0 - ic) * cs.y + a.center;
-        const double ec = ext * cs.x, es = ext * cs.y;
+        const double ec = (double)(TX - 1) * cs.x, es = (double)(TY - 1) * cs.y;
         // non-finite trig (rejected by the host) is skipped, never indexed
         if (isfinite(P0) && isfinite(ec) && isfinite(es)) {
           const double pmin = P0 + fmin(0.0, ec) + fmin(0.0, es);
@@ -141,73 +218,127 @@ __global__ void __launch_bounds__(kThreads, 2) bp_tile_kernel(BPArgs a) {
           }
         }
       }
-      prm[tid] = p;
-      lo_s[tid] = lo;
-      flag_s[tid] = flag;
+      prm[buf][tid] = p;
+      lo_s[buf][tid] = lo;
+      flag_s[buf][tid] = flag;
     }
-    __syncthreads();
+  };
 
-    // (2) stage interpolation pairs of every angle of the chunk
-    for (int e = tid; e < kChunk * kWin; e += kThreads) {
-      const int ai = e / kWin, j = e - ai * kWin;
-      const int i = i0 + ai;
-      float2 pr = make_float2(0.f, 0.f);
-      if (i < a.nrow && !(flag_s[ai] & 1)) {
-        const T *row = sino + i * a.srs;
-        const int d = lo_s[ai] + j;
-        float v, dv;
-        if (a.edge_pad) {
-          const int d0 = min(max(d, 0), ncol - 1), d1 = min(max(d + 1, 0), ncol - 1);
-          v = atb::load_as_float(row + d0);
-          dv = atb::load_as_float(row + d1) - v;
-        } else if (d < 0 || d > ncol - 1) {
-          v = 0.f; dv = 0.f;
-        } else if (d == ncol - 1) {
-          v = atb::load_as_float(row + d); dv = 0.f;
-        } else {
-          v = atb::load_as_float(row + d);
-          dv = atb::load_as_float(row + d + 1) - v;
-        }
-        pr = make_float2(fmaf(-(float)(j - kHalf), dv, v), dv);
-      }
-      pairs[e] = pr;
-    }
-    __syncthreads();
-
-    // (3) accumulate
-    const int nang = min(kChunk, a.nrow - i0);
-    for (int ai = 0; ai < nang; ++ai) {
-      const int flag = flag_s[ai];
-      if (flag & 1) continue;
-      const AngleParam p = prm[ai];
-      const float qt = fmaf((float)tx, p.c, fmaf((float)ty, p.s, p.qbase));
-      const float c8 = 8.f * p.c, s4 = 4.f * p.s;
-      const float2 *w = pairs + ai * kWin + kHalf;  // indexed by floor(q)
-      if (!(flag & 2)) {
-#pragma unroll
-        for (int b = 0; b < kPY; ++b) {
-          const float qr = fmaf((float)b, s4, qt);
-#pragma unroll
-          for (int c = 0; c < kPX; ++c) {
-            const float q = fmaf((float)c, c8, qr);
-            const int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
-            const float2 pr = w[j];
-            const float v = fmaf(pr.y, q, pr.x);
-            if (kPerAngleKahan) kahan_add(sum[b][c], comp[b][c], v);
-            else acc[b][c] += v;
-          }
+  // raw windows of chunk k into raw[buf] (float32 storage only); elements
+  // outside the detector row are never copied
+  auto issue_raw = [&](int k, int buf) {
+    if constexpr (K::kAsync) {
+      float *rb = raw + (size_t)buf * kChunk * S * kRaw;
+      const float *sf = reinterpret_cast<const float *>(sino);
+      if (a.vec16) {
+        constexpr int kVec = kRaw / 4;
+        for (int e = tid; e < kChunk * S * kVec; e += kThreads) {
+          const int v = e % kVec, ks = (e / kVec) % S, ai = e / (kVec * S);
+          const int i = k * kChunk + ai;
+          if (i >= a.nrow || ks >= nsl || (flag_s[buf][ai] & 1)) continue;
+          const int d = ((lo_s[buf][ai] >> 2) << 2) + 4 * v;
+          if (d < 0 || d >= ncol) continue;  // ncol % 4 == 0: a vector is inside or outside
+          cp_async16(rb + ((size_t)ai * S + ks) * kRaw + 4 * v, sf + i * a.srs + ks * a.sss + d);
         }
       } else {
-        // checked path: the footprint reaches a detector edge
+        for (int e = tid; e < kChunk * S * kRaw; e += kThreads) {
+          const int v = e % kRaw, ks = (e / kRaw) % S, ai = e / (kRaw * S);
+          const int i = k * kChunk + ai;
+          if (i >= a.nrow || ks >= nsl || (flag_s[buf][ai] & 1)) continue;
+          const int d = ((lo_s[buf][ai] >> 2) << 2) + v;
+          if (d < 0 || d >= ncol) continue;
+          cp_async4(rb + ((size_t)ai * S + ks) * kRaw + v, sf + i * a.srs + ks * a.sss + d);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  // detector sample d (0 <= d < ncol) of (angle i, slice ks)
+  auto tap = [&](int buf, int ai, int ks, int i, int d) -> float {
+    if constexpr (K::kAsync) {
+      const int r = d - ((lo_s[buf][ai] >> 2) << 2);
+      if (r >= 0 && r < kRaw) return raw[(((size_t)buf * kChunk + ai) * S + ks) * kRaw + r];
+    }
+    return atb::load_as_float(sino + i * a.srs + ks * a.sss + d);
+  };
+
+  // chunk k's windows -> interpolation pairs
+  auto make_pairs = [&](int k, int buf) {
+    for (int e = tid; e < kChunk * kWin; e += kThreads) {
+      const int ai = e / kWin, j = e - ai * kWin;
+      const int i = k * kChunk + ai;
+      float av[S], dv[S];
 #pragma unroll
-        for (int b = 0; b < kPY; ++b) {
-          const float qr = fmaf((float)b, s4, qt);
+      for (int ks = 0; ks < S; ++ks) { av[ks] = 0.f; dv[ks] = 0.f; }
+      if (i < a.nrow && !(flag_s[buf][ai] & 1)) {
+        const int d = lo_s[buf][ai] + j;
 #pragma unroll
-          for (int c = 0; c < kPX; ++c) {
-            const float q = fmaf((float)c, c8, qr);
-            int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
+        for (int ks = 0; ks < S; ++ks) {
+          if (ks >= nsl) continue;
+          float v, w;
+          if (a.edge_pad) {
+            const int d0 = min(max(d, 0), ncol - 1), d1 = min(max(d + 1, 0), ncol - 1);
+            v = tap(buf, ai, ks, i, d0);
+            w = d1 == d0 ? 0.f : tap(buf, ai, ks, i, d1) - v;
+          } else if (d < 0 || d > ncol - 1) {
+            v = 0.f; w = 0.f;
+          } else if (d == ncol - 1) {
+            v = tap(buf, ai, ks, i, d); w = 0.f;
+          } else {
+            v = tap(buf, ai, ks, i, d);
+            w = tap(buf, ai, ks, i, d + 1) - v;
+          }
+          av[ks] = fmaf(-(float)(j - kHalf), w, v);
+          dv[ks] = w;
+        }
+      }
+      unsigned char *dst = pairs + (size_t)e * K::kPairBytes;
+      if constexpr (S == 1) {
+        *reinterpret_cast<float2 *>(dst) = make_float2(av[0], dv[0]);
+      } else {
+#pragma unroll
+        for (int g = 0; g < S / 2; ++g)
+          reinterpret_cast<float4 *>(dst)[g] = make_float4(av[2 * g], av[2 * g + 1], dv[2 * g], dv[2 * g + 1]);
+      }
+    }
+  };
+
+  params(0, 0);
+  __syncthreads();
+  issue_raw(0, 0);
+
+  for (int k = 0; k < nchunk; ++k) {
+    const int buf = k & 1, nbuf = buf ^ 1;
+    cp_async_wait_all();
+    __syncthreads();  // raw(k) landed; pairs(k-1) and params(k-1) no longer read
+    if (k + 1 < nchunk) params(k + 1, nbuf);
+    make_pairs(k, buf);
+    __syncthreads();  // pairs(k) and params(k+1) visible
+    if (k + 1 < nchunk) issue_raw(k + 1, nbuf);
+
+    // accumulate chunk k
+    const int nang = min(kChunk, a.nrow - k * kChunk);
+    for (int ai = 0; ai < nang; ++ai) {
+      const int flag = flag_s[buf][ai];
+      if (flag & 1) continue;
+      const AngleParam p = prm[buf][ai];
+      const float qt = fmaf((float)tx, p.c, fmaf((float)ty, p.s, p.qbase));
+      const float c8 = 8.f * p.c, s4 = 4.f * p.s;
+      // this angle's pairs, indexed by floor(q) (window centre at 0)
+      const unsigned char *w = pairs + ((size_t)ai * kWin + kHalf) * K::kPairBytes;
+      const bool checked = flag & 2;
+#pragma unroll
+      for (int b = 0; b < PY; ++b) {
+        const float qr = fmaf((float)b, s4, qt);
+#pragma unroll
+        for (int c = 0; c < PX; ++c) {
+          const float q = fmaf((float)c, c8, qr);
+          int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
+          bool inr = true;
+          if (checked) {
             const float dl = q - p.qlo, dr = q - p.qmax;
-            bool inr = (dl >= 0.f) && (dr <= 0.f);
+            inr = (dl >= 0.f) && (dr <= 0.f);
             if (fabsf(dl) < kEdgeTol || fabsf(dr) < kEdgeTol) {
               // same expression and rounding order as the reference's
               // (x - ic) cos + (y - ic) sin + center, in FP64
@@ -217,49 +348,102 @@ __global__ void __launch_bounds__(kThreads, 2) bp_tile_kernel(BPArgs a) {
               inr = (pe >= 0.0) && (pe <= (double)(ncol - 1));
               j = max(j, p.j0 - kHalf);
             }
-            const float2 pr = w[j];
+          }
+          if constexpr (S == 1) {
+            const float2 pr = reinterpret_cast<const float2 *>(w)[j];
             const float v = inr ? fmaf(pr.y, q, pr.x) : 0.f;
-            if (kPerAngleKahan) kahan_add(sum[b][c], comp[b][c], v);
-            else acc[b][c] += v;
+            if (kPerAngleKahan) kahan_add(sum[b][c][0], comp[b][c][0], v);
+            else accf[b][c] += v;
+          } else {
+            const unsigned long long Q = pack2(q, q);
+            const float4 *w4 = reinterpret_cast<const float4 *>(w) + (size_t)j * (S / 2);
+#pragma unroll
+            for (int g = 0; g < S / 2; ++g) {
+              float4 pr = w4[g];
+              if (checked && !inr) pr = make_float4(0.f, 0.f, 0.f, 0.f);
+              fma_acc2(acc2[b][c][g], pack2(pr.x, pr.y), pack2(pr.z, pr.w), Q);
+            }
           }
         }
       }
     }
+    // fold this chunk's partials into the compensated totals
     if (!kPerAngleKahan) {
 #pragma unroll
-      for (int b = 0; b < kPY; ++b)
+      for (int b = 0; b < PY; ++b)
 #pragma unroll
-        for (int c = 0; c < kPX; ++c) { kahan_add(sum[b][c], comp[b][c], acc[b][c]); acc[b][c] = 0.f; }
+        for (int c = 0; c < PX; ++c) {
+          if constexpr (S == 1) {
+            kahan_add(sum[b][c][0], comp[b][c][0], accf[b][c]);
+            accf[b][c] = 0.f;
+          } else {
+#pragma unroll
+            for (int g = 0; g < S / 2; ++g) {
+              float lo, hi;
+              unpack2(acc2[b][c][g], lo, hi);
+              kahan_add(sum[b][c][2 * g], comp[b][c][2 * g], lo);
+              kahan_add(sum[b][c][2 * g + 1], comp[b][c][2 * g + 1], hi);
+              acc2[b][c][g] = 0ull;
+            }
+          }
+        }
     }
-    __syncthreads();
   }
 
-  // (4) epilogue: compensated total, circle mask, scale, store
+  // epilogue: compensated total, circle mask, scale, store
   const int cm = ncol / 2;
 #pragma unroll
-  for (int b = 0; b < kPY; ++b) {
+  for (int b = 0; b < PY; ++b) {
     const int y = y0 + ty + 4 * b;
 #pragma unroll
-    for (int c = 0; c < kPX; ++c) {
+    for (int c = 0; c < PX; ++c) {
       const int x = x0 + tx + 8 * c;
       if (x < ncol && y < ncol) {
-        float v = __fsub_rn(sum[b][c], comp[b][c]) * a.scale;
+        bool keep = true;
         if (a.mask_r2 >= 0.0) {
           const long long dx = x - cm, dy = y - cm;
-          if ((double)(dx * dx + dy * dy) > a.mask_r2) v = 0.f;
+          keep = (double)(dx * dx + dy * dy) <= a.mask_r2;
         }
-        a.out[y * a.ors + slice * a.oss + x] = v;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+          if (k < nsl) {
+            const float v = keep ? __fsub_rn(sum[b][c][k], comp[b][c][k]) * a.scale : 0.f;
+            a.out[y * a.ors + (slice0 + k) * a.oss + x] = v;
+          }
+        }
       }
     }
   }
 }
 
-template <typename T>
-int launch_bp(const BPArgs &a, cudaStream_t st) {
-  dim3 grid((a.ncol + kTile - 1) / kTile, (a.ncol + kTile - 1) / kTile, a.nslice);
-  if (a.per_angle_kahan) bp_tile_kernel<T, true><<<grid, kThreads, 0, st>>>(a);
-  else bp_tile_kernel<T, false><<<grid, kThreads, 0, st>>>(a);
+template <typename T, int S, bool kPerAngleKahan>
+int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
+  using K = BPCfg<T, S>;
+  auto fn = bp_kernel<T, S, kPerAngleKahan>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::kSmem);
+  if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_backproject: %s", cudaGetErrorString(e));
+  dim3 grid((a.ncol + K::TX - 1) / K::TX, (a.ncol + K::TY - 1) / K::TY, (nslices + S - 1) / S);
+  fn<<<grid, kThreads, K::kSmem, st>>>(a);
   return atb::check_launch("atb_backproject");
+}
+
+template <typename T>
+int dispatch(BPArgs a, int per_angle_kahan, cudaStream_t st) {
+  if (per_angle_kahan) return launch_bp<T, 1, true>(a, a.nslice, st);
+  // four slices per CTA for the bulk of a stack, then the remainder
+  const int n4 = (a.nslice / 4) * 4;
+  int rc = ATB_OK;
+  if (n4 > 0) rc = launch_bp<T, 4, false>(a, n4, st);
+  if (rc != ATB_OK) return rc;
+  const int rem = a.nslice - n4;
+  if (rem == 0) return ATB_OK;
+  a.slice_base = n4;
+  if (rem >= 2) {
+    rc = launch_bp<T, 2, false>(a, 2, st);
+    if (rc != ATB_OK || rem == 2) return rc;
+    a.slice_base = n4 + 2;
+  }
+  return launch_bp<T, 1, false>(a, 1, st);
 }
 
 }  // namespace
@@ -271,22 +455,24 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
   if (!sino || !trig || !out) return atb::fail(ATB_EINVAL, "atb_backproject: null pointer");
   if (nrow < 1 || nslice < 1 || ncol < 1)
     return atb::fail(ATB_EINVAL, "atb_backproject: bad shape nrow=%d nslice=%d ncol=%d", nrow, nslice, ncol);
-  if (nslice > 65535) return atb::fail(ATB_ERANGE, "atb_backproject: nslice=%d > 65535", nslice);
+  if (nslice > 4 * 65535) return atb::fail(ATB_ERANGE, "atb_backproject: nslice=%d too large", nslice);
   if (ncol > (1 << 20)) return atb::fail(ATB_ERANGE, "atb_backproject: ncol=%d too large", ncol);
   if (!(center >= 0.0) || center >= (double)ncol)
     return atb::fail(ATB_EINVAL, "atb_backproject: center %g outside [0, %d)", center, ncol);
   BPArgs a;
   a.sino = sino; a.srs = sino_row_stride; a.sss = sino_slice_stride;
-  a.nrow = nrow; a.nslice = nslice; a.ncol = ncol;
+  a.nrow = nrow; a.nslice = nslice; a.ncol = ncol; a.slice_base = 0;
   a.trig = reinterpret_cast<const double2 *>(trig);
   a.center = center; a.edge_pad = edge_pad ? 1 : 0; a.mask_r2 = mask_r2; a.scale = scale;
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride;
-  a.per_angle_kahan = flags & 1;
+  a.vec16 = sino_dtype == ATB_F32 && (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % 4 == 0 &&
+            sino_slice_stride % 4 == 0 && ncol % 4 == 0;
   cudaStream_t st = atb::as_stream(stream);
+  const int pak = flags & 1;
   switch (sino_dtype) {
-    case ATB_F32: return launch_bp<float>(a, st);
-    case ATB_F16: return launch_bp<__half>(a, st);
-    case ATB_BF16: return launch_bp<__nv_bfloat16>(a, st);
+    case ATB_F32: return dispatch<float>(a, pak, st);
+    case ATB_F16: return dispatch<__half>(a, pak, st);
+    case ATB_BF16: return dispatch<__nv_bfloat16>(a, pak, st);
     default: return atb::fail(ATB_EINVAL, "atb_backproject: unknown sino_dtype %d", sino_dtype);
   }
 }
