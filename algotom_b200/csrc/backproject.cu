@@ -17,9 +17,11 @@
 //     (a_j, D_j) = (s[lo+j] - (j-H) D_j, s[lo+j+1] - s[lo+j]),  H = kWin/2
 // so that the value at the window-centred local position q = p - lo - H,
 // bin j = floor(q) + H, is the single FMA a_j + D_j q.  With S >= 2 the pairs
-// of two slices sit in one 16-byte word (a_0, a_1, D_0, D_1): one LDS.128,
-// one packed fma.rn.f32x2 and one packed add.rn.f32x2 update two slices,
-// and the position, floor and address work is shared by all S slices.
+// of two slices sit in one 16-byte word (a_0, a_1, D_0, D_1), one plane per
+// slice pair so that neighbouring bins are 16 bytes apart (conflict-free
+// quarter-warp LDS.128): one LDS.128, one packed fma.rn.f32x2 and one packed
+// add.rn.f32x2 update two slices, and the position, floor and address work
+// is shared by all S slices.
 //
 // Staging is double-buffered: while a chunk is being accumulated, the raw
 // detector windows of the next chunk stream into shared memory with cp.async
@@ -47,6 +49,8 @@
 // chunks with Kahan compensation (the single-slice kernel can instead
 // compensate every angle).  One warp instruction covers an 8 x 4 pixel
 // block, whose 32 lanes read a run of about 9 neighbouring bins.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace {
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
   constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
 
   extern __shared__ __align__(16) unsigned char smem[];
-  unsigned char *pairs = smem;                                   // [kChunk][kWin][S pairs]
+  unsigned char *pairs = smem;  // S == 1: [kChunk][kWin] float2; else [kChunk][S/2][kWin] float4
   float *raw = reinterpret_cast<float *>(smem + K::kPairsSmem);  // [2][kChunk][S][kRaw]
   __shared__ AngleParam prm[2][kChunk];
   __shared__ int lo_s[2][kChunk];
@@ -293,13 +297,13 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
           dv[ks] = w;
         }
       }
-      unsigned char *dst = pairs + (size_t)e * K::kPairBytes;
       if constexpr (S == 1) {
-        *reinterpret_cast<float2 *>(dst) = make_float2(av[0], dv[0]);
+        reinterpret_cast<float2 *>(pairs)[e] = make_float2(av[0], dv[0]);
       } else {
+        float4 *p4 = reinterpret_cast<float4 *>(pairs) + (size_t)ai * (S / 2) * kWin + j;
 #pragma unroll
         for (int g = 0; g < S / 2; ++g)
-          reinterpret_cast<float4 *>(dst)[g] = make_float4(av[2 * g], av[2 * g + 1], dv[2 * g], dv[2 * g + 1]);
+          p4[g * kWin] = make_float4(av[2 * g], av[2 * g + 1], dv[2 * g], dv[2 * g + 1]);
       }
     }
   };
@@ -327,45 +331,54 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
       const float c8 = 8.f * p.c, s4 = 4.f * p.s;
       // this angle's pairs, indexed by floor(q) (window centre at 0)
       const unsigned char *w = pairs + ((size_t)ai * kWin + kHalf) * K::kPairBytes;
-      const bool checked = flag & 2;
+      if constexpr (S > 1) w = pairs + ((size_t)ai * (S / 2) * kWin + kHalf) * 16;
+      auto body = [&](auto checked_tag) {
+        constexpr bool kChecked = decltype(checked_tag)::value;
 #pragma unroll
-      for (int b = 0; b < PY; ++b) {
-        const float qr = fmaf((float)b, s4, qt);
+        for (int b = 0; b < PY; ++b) {
+          const float qr = fmaf((float)b, s4, qt);
 #pragma unroll
-        for (int c = 0; c < PX; ++c) {
-          const float q = fmaf((float)c, c8, qr);
-          int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
-          bool inr = true;
-          if (checked) {
-            const float dl = q - p.qlo, dr = q - p.qmax;
-            inr = (dl >= 0.f) && (dr <= 0.f);
-            if (fabsf(dl) < kEdgeTol || fabsf(dr) < kEdgeTol) {
-              // same expression and rounding order as the reference's
-              // (x - ic) cos + (y - ic) sin + center, in FP64
-              const double xc = (double)(x0 + tx + 8 * c) - ic;
-              const double yc = (double)(y0 + ty + 4 * b) - ic;
-              const double pe = __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)), a.center);
-              inr = (pe >= 0.0) && (pe <= (double)(ncol - 1));
-              j = max(j, p.j0 - kHalf);
+          for (int c = 0; c < PX; ++c) {
+            const float q = fmaf((float)c, c8, qr);
+            int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
+            bool inr = true;
+            if constexpr (kChecked) {
+              const float dl = q - p.qlo, dr = q - p.qmax;
+              inr = (dl >= 0.f) && (dr <= 0.f);
+              if (fabsf(dl) < kEdgeTol || fabsf(dr) < kEdgeTol) {
+                // same expression and rounding order as the reference's
+                // (x - ic) cos + (y - ic) sin + center, in FP64
+                const double xc = (double)(x0 + tx + 8 * c) - ic;
+                const double yc = (double)(y0 + ty + 4 * b) - ic;
+                const double pe =
+                    __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)), a.center);
+                inr = (pe >= 0.0) && (pe <= (double)(ncol - 1));
+                j = max(j, p.j0 - kHalf);
+              }
             }
-          }
-          if constexpr (S == 1) {
-            const float2 pr = reinterpret_cast<const float2 *>(w)[j];
-            const float v = inr ? fmaf(pr.y, q, pr.x) : 0.f;
-            if (kPerAngleKahan) kahan_add(sum[b][c][0], comp[b][c][0], v);
-            else accf[b][c] += v;
-          } else {
-            const unsigned long long Q = pack2(q, q);
-            const float4 *w4 = reinterpret_cast<const float4 *>(w) + (size_t)j * (S / 2);
+            if constexpr (S == 1) {
+              const float2 pr = reinterpret_cast<const float2 *>(w)[j];
+              float v = fmaf(pr.y, q, pr.x);
+              if constexpr (kChecked) v = inr ? v : 0.f;
+              if (kPerAngleKahan) kahan_add(sum[b][c][0], comp[b][c][0], v);
+              else accf[b][c] += v;
+            } else {
+              const unsigned long long Q = pack2(q, q);
+              const float4 *w4 = reinterpret_cast<const float4 *>(w) + j;
 #pragma unroll
-            for (int g = 0; g < S / 2; ++g) {
-              float4 pr = w4[g];
-              if (checked && !inr) pr = make_float4(0.f, 0.f, 0.f, 0.f);
-              fma_acc2(acc2[b][c][g], pack2(pr.x, pr.y), pack2(pr.z, pr.w), Q);
+              for (int g = 0; g < S / 2; ++g) {
+                float4 pr = w4[g * kWin];
+                if constexpr (kChecked) {
+                  if (!inr) pr = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                fma_acc2(acc2[b][c][g], pack2(pr.x, pr.y), pack2(pr.z, pr.w), Q);
+              }
             }
           }
         }
-      }
+      };
+      if (flag & 2) body(std::true_type{});
+      else body(std::false_type{});
     }
     // fold this chunk's partials into the compensated totals
     if (!kPerAngleKahan) {
