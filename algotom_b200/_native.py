@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 
 # every symbol include/algotom_b200.h declares
 EXPORTS = ("atb_version", "atb_last_error", "atb_filter_log2m",
-           "atb_filter_rows", "atb_neg_log", "atb_backproject")
+           "atb_filter_rows", "atb_neg_log", "atb_backproject",
+           "atb_radon_adjoint")
 
 F32, F16, BF16 = 0, 1, 2
 PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
@@ -42,6 +43,9 @@ _SIGS = {
         _vp, ctypes.c_int, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
         ctypes.c_float, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
+    "atb_radon_adjoint": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+        ctypes.c_double, _vp, _c_i64, _c_i64, _vp]),
 }
 
 _lib = None

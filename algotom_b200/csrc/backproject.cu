@@ -86,6 +86,7 @@ struct BPArgs {
   float *out;
   long long ors, oss;
   int vec16;  // float32 rows 16-byte aligned: stage with 16-byte cp.async
+  int slope;  // back-project the interpolant's slope D_j instead of its value
 };
 
 struct __align__(16) AngleParam {
@@ -159,6 +160,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
   __shared__ AngleParam prm[2][kChunk];
   __shared__ int lo_s[2][kChunk];
   __shared__ int flag_s[2][kChunk];  // bit 0: skip angle, bit 1: checked path
+  __shared__ float edge_s[2][kChunk][S][2];  // s[0], s[ncol-1] (edge padding)
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -228,79 +230,112 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
     }
   };
 
-  // raw windows of chunk k into raw[buf] (float32 storage only); elements
-  // outside the detector row are never copied
+  // Staging work is split by angle: kTPA threads per angle of the chunk,
+  // each taking every kTPA-th bin of that angle's window.
+  constexpr int kTPA = kThreads / kChunk;
+  constexpr int kJPT = kWin / kTPA;
+  static_assert(kThreads % kChunk == 0 && kWin % kTPA == 0, "staging split");
+  const int s_ai = tid / kTPA, s_jl = tid % kTPA;
+  const int ncol1 = ncol - 1;
+  const long long srs = a.srs, sss = a.sss;
+  const bool edge_pad = a.edge_pad, slope = a.slope, vec16 = a.vec16;
+
+  // raw windows (and, for edge padding, the two edge samples) of chunk k
+  // into raw[buf]; float32 storage only.  Elements outside the detector row
+  // are never copied.
   auto issue_raw = [&](int k, int buf) {
     if constexpr (K::kAsync) {
-      float *rb = raw + (size_t)buf * kChunk * S * kRaw;
-      const float *sf = reinterpret_cast<const float *>(sino);
-      if (a.vec16) {
-        constexpr int kVec = kRaw / 4;
-        for (int e = tid; e < kChunk * S * kVec; e += kThreads) {
-          const int v = e % kVec, ks = (e / kVec) % S, ai = e / (kVec * S);
-          const int i = k * kChunk + ai;
-          if (i >= a.nrow || ks >= nsl || (flag_s[buf][ai] & 1)) continue;
-          const int d = ((lo_s[buf][ai] >> 2) << 2) + 4 * v;
-          if (d < 0 || d >= ncol) continue;  // ncol % 4 == 0: a vector is inside or outside
-          cp_async16(rb + ((size_t)ai * S + ks) * kRaw + 4 * v, sf + i * a.srs + ks * a.sss + d);
+      const int i = k * kChunk + s_ai;
+      if (i < a.nrow && !(flag_s[buf][s_ai] & 1)) {
+        const int base = (lo_s[buf][s_ai] >> 2) << 2;
+        const float *src = reinterpret_cast<const float *>(sino) + i * srs;
+        float *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
+        if (vec16) {
+          constexpr int kVec = kRaw / 4;
+          for (int idx = s_jl; idx < S * kVec; idx += kTPA) {
+            const int ks = idx / kVec, v = idx - ks * kVec;
+            const int d = base + 4 * v;
+            if (ks < nsl && d >= 0 && d < ncol)  // ncol % 4 == 0: a vector is in or out
+              cp_async16(rb + ks * kRaw + 4 * v, src + ks * sss + d);
+          }
+        } else {
+          for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
+            const int ks = idx / kRaw, v = idx - ks * kRaw;
+            const int d = base + v;
+            if (ks < nsl && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
+          }
         }
-      } else {
-        for (int e = tid; e < kChunk * S * kRaw; e += kThreads) {
-          const int v = e % kRaw, ks = (e / kRaw) % S, ai = e / (kRaw * S);
-          const int i = k * kChunk + ai;
-          if (i >= a.nrow || ks >= nsl || (flag_s[buf][ai] & 1)) continue;
-          const int d = ((lo_s[buf][ai] >> 2) << 2) + v;
-          if (d < 0 || d >= ncol) continue;
-          cp_async4(rb + ((size_t)ai * S + ks) * kRaw + v, sf + i * a.srs + ks * a.sss + d);
+        if (edge_pad && s_jl < nsl) {
+          cp_async4(&edge_s[buf][s_ai][s_jl][0], src + s_jl * sss);
+          cp_async4(&edge_s[buf][s_ai][s_jl][1], src + s_jl * sss + ncol1);
         }
       }
     }
     cp_async_commit();
   };
 
-  // detector sample d (0 <= d < ncol) of (angle i, slice ks)
-  auto tap = [&](int buf, int ai, int ks, int i, int d) -> float {
-    if constexpr (K::kAsync) {
-      const int r = d - ((lo_s[buf][ai] >> 2) << 2);
-      if (r >= 0 && r < kRaw) return raw[(((size_t)buf * kChunk + ai) * S + ks) * kRaw + r];
-    }
-    return atb::load_as_float(sino + i * a.srs + ks * a.sss + d);
-  };
-
-  // chunk k's windows -> interpolation pairs
+  // chunk k's windows -> interpolation pairs (skipped angles are left as
+  // they are: the accumulation never reads them)
   auto make_pairs = [&](int k, int buf) {
-    for (int e = tid; e < kChunk * kWin; e += kThreads) {
-      const int ai = e / kWin, j = e - ai * kWin;
-      const int i = k * kChunk + ai;
+    const int i = k * kChunk + s_ai;
+    if (i >= a.nrow || (flag_s[buf][s_ai] & 1)) return;
+    const int lo = lo_s[buf][s_ai];
+    const int base = (lo >> 2) << 2;
+    // every d and d+1 of the window inside [0, ncol-1] with d <= ncol-2
+    const bool interior = lo >= 0 && lo + kWin <= ncol1;
+    const float *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
+    const T *row = sino + i * srs;
+    // detector sample x (0 <= x <= ncol-1) of slice ks
+    auto val = [&](int ks, int x) -> float {
+      if constexpr (K::kAsync) {
+        const int r = x - base;
+        if (r >= 0 && r < kRaw) return rb[ks * kRaw + r];
+        return edge_s[buf][s_ai][ks][x == 0 ? 0 : 1];  // clamped edge sample
+      } else {
+        return atb::load_as_float(row + ks * sss + x);
+      }
+    };
+#pragma unroll 2
+    for (int t = 0; t < kJPT; ++t) {
+      const int j = s_jl + kTPA * t;
+      const int d = lo + j;
+      const float jc = (float)(j - kHalf);
       float av[S], dv[S];
 #pragma unroll
-      for (int ks = 0; ks < S; ++ks) { av[ks] = 0.f; dv[ks] = 0.f; }
-      if (i < a.nrow && !(flag_s[buf][ai] & 1)) {
-        const int d = lo_s[buf][ai] + j;
-#pragma unroll
-        for (int ks = 0; ks < S; ++ks) {
-          if (ks >= nsl) continue;
-          float v, w;
-          if (a.edge_pad) {
-            const int d0 = min(max(d, 0), ncol - 1), d1 = min(max(d + 1, 0), ncol - 1);
-            v = tap(buf, ai, ks, i, d0);
-            w = d1 == d0 ? 0.f : tap(buf, ai, ks, i, d1) - v;
-          } else if (d < 0 || d > ncol - 1) {
-            v = 0.f; w = 0.f;
-          } else if (d == ncol - 1) {
-            v = tap(buf, ai, ks, i, d); w = 0.f;
-          } else {
-            v = tap(buf, ai, ks, i, d);
-            w = tap(buf, ai, ks, i, d + 1) - v;
+      for (int ks = 0; ks < S; ++ks) {
+        float v = 0.f, w = 0.f;
+        if (ks < nsl) {
+          if (interior) {
+            if constexpr (K::kAsync) {
+              v = rb[ks * kRaw + d - base];
+              w = rb[ks * kRaw + d + 1 - base] - v;
+            } else {
+              v = atb::load_as_float(row + ks * sss + d);
+              w = atb::load_as_float(row + ks * sss + d + 1) - v;
+            }
+          } else if (edge_pad) {
+            const int d0 = min(max(d, 0), ncol1), d1 = min(max(d + 1, 0), ncol1);
+            v = val(ks, d0);
+            w = d1 == d0 ? 0.f : val(ks, d1) - v;
+          } else if (d >= 0 && d < ncol1) {
+            v = val(ks, d);
+            w = val(ks, d + 1) - v;
+          } else if (d == ncol1) {
+            v = val(ks, d);  // last bin: its value only at p = ncol-1
           }
-          av[ks] = fmaf(-(float)(j - kHalf), w, v);
+        }
+        if (slope) {  // derivative of the interpolant with respect to p
+          av[ks] = w;
+          dv[ks] = 0.f;
+        } else {
+          av[ks] = fmaf(-jc, w, v);
           dv[ks] = w;
         }
       }
       if constexpr (S == 1) {
-        reinterpret_cast<float2 *>(pairs)[e] = make_float2(av[0], dv[0]);
+        reinterpret_cast<float2 *>(pairs)[s_ai * kWin + j] = make_float2(av[0], dv[0]);
       } else {
-        float4 *p4 = reinterpret_cast<float4 *>(pairs) + (size_t)ai * (S / 2) * kWin + j;
+        float4 *p4 = reinterpret_cast<float4 *>(pairs) + (size_t)s_ai * (S / 2) * kWin + j;
 #pragma unroll
         for (int g = 0; g < S / 2; ++g)
           p4[g * kWin] = make_float4(av[2 * g], av[2 * g + 1], dv[2 * g], dv[2 * g + 1]);
@@ -478,6 +513,7 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
   a.trig = reinterpret_cast<const double2 *>(trig);
   a.center = center; a.edge_pad = edge_pad ? 1 : 0; a.mask_r2 = mask_r2; a.scale = scale;
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride;
+  a.slope = (flags >> 1) & 1;
   a.vec16 = sino_dtype == ATB_F32 && (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % 4 == 0 &&
             sino_slice_stride % 4 == 0 && ncol % 4 == 0;
   cudaStream_t st = atb::as_stream(stream);

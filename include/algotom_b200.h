@@ -116,7 +116,11 @@ int atb_neg_log(const float *src, int64_t src_row_stride,
  *   out      float32 [ncol][nslice][ncol] at out_row_stride / out_slice_stride
  *   flags    bit 0: per-angle compensated (Kahan) accumulation instead of
  *            the default chunked Kahan (FP32 partials over a chunk of angles,
- *            compensated across chunks)
+ *            compensated across chunks);
+ *            bit 1: back-project the slope of the interpolant,
+ *            s[d+1] - s[d] at d = floor(p), instead of its value: the
+ *            derivative of the back-projection with respect to the centre
+ *            (no counterpart in the reference; used by the autograd path)
  */
 int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int64_t sino_slice_stride, int nrow, int nslice, int ncol,
@@ -124,6 +128,25 @@ int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     double mask_r2, float scale, float *out,
                     int64_t out_row_stride, int64_t out_slice_stride,
                     int flags, void *stream);
+
+/*
+ * Forward (Radon) projection that is the exact adjoint of atb_backproject
+ * without edge padding: out[i][k][d] = sum over pixels of
+ * img[y][k][x] * hat(p_i(y, x) - d) over positions inside [0, ncol-1].
+ * The transpose of the reference back-projector
+ * (algotom/rec/reconstruction.py:156-190, 307-359), which has no adjoint of
+ * its own; it gives the gradient of a back-projection with respect to its
+ * sinogram, and is the projector of model-based reconstruction.
+ *
+ *   img   float32 [ncol][nslice][ncol] at img_row_stride / img_slice_stride
+ *   trig, center as for atb_backproject
+ *   out   float32 [nrow][nslice][ncol] at out_row_stride / out_slice_stride
+ */
+int atb_radon_adjoint(const float *img, int64_t img_row_stride,
+                      int64_t img_slice_stride, int nrow, int nslice,
+                      int ncol, const double *trig, double center, float *out,
+                      int64_t out_row_stride, int64_t out_slice_stride,
+                      void *stream);
 
 #ifdef __cplusplus
 }
