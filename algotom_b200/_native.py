@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 # every symbol include/algotom_b200.h declares
 EXPORTS = ("atb_version", "atb_last_error", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
-           "atb_radon_adjoint")
+           "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch")
 
 F32, F16, BF16 = 0, 1, 2
 PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
@@ -24,6 +24,16 @@ PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
 
 class NativeLibraryError(RuntimeError):
     """The CUDA library is missing, failed to load, or a call failed."""
+
+
+class BpItem(ctypes.Structure):
+    """``atb_bp_item`` of include/algotom_b200.h."""
+    _fields_ = [("sino", ctypes.c_void_p), ("sino_row_stride", ctypes.c_int64),
+                ("trig", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("out_row_stride", ctypes.c_int64), ("center", ctypes.c_double),
+                ("mask_r2", ctypes.c_double), ("scale", ctypes.c_float),
+                ("nrow", ctypes.c_int), ("ncol", ctypes.c_int),
+                ("edge_pad", ctypes.c_int)]
 
 
 _c_i64 = ctypes.c_int64
@@ -46,6 +56,9 @@ _SIGS = {
     "atb_radon_adjoint": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
         ctypes.c_double, _vp, _c_i64, _c_i64, _vp]),
+    "atb_bp_batch_plan": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "atb_backproject_batch": (ctypes.c_int, [
+        _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
 }
 
 _lib = None

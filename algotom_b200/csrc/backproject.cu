@@ -147,14 +147,15 @@ struct BPCfg {
   static constexpr size_t kSmem = kPairsSmem + kRawSmem;
 };
 
+// One CTA's work: the TX x TY pixel tile (bx, by) of the slice group bz.
+// Every thread of the CTA must call it (it synchronises).
 template <typename T, int S, bool kPerAngleKahan>
-__global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
+__device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz, unsigned char *smem) {
   using K = BPCfg<T, S>;
   constexpr int PX = K::PX, PY = K::PY, TX = K::TX, TY = K::TY;
   constexpr int kChunk = K::kChunk, kWin = K::kWin, kHalf = K::kHalf, kRaw = K::kRaw;
   constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
 
-  extern __shared__ __align__(16) unsigned char smem[];
   unsigned char *pairs = smem;  // S == 1: [kChunk][kWin] float2; else [kChunk][S/2][kWin] float4
   float *raw = reinterpret_cast<float *>(smem + K::kPairsSmem);  // [2][kChunk][S][kRaw]
   __shared__ AngleParam prm[2][kChunk];
@@ -164,8 +165,8 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int slice0 = a.slice_base + blockIdx.z * S;
+  const int x0 = bx * TX, y0 = by * TY;
+  const int slice0 = a.slice_base + bz * S;
   const int nsl = min(S, a.nslice - slice0);  // live slices of this CTA
   const int ncol = a.ncol;
   const T *sino = reinterpret_cast<const T *>(a.sino) + slice0 * a.sss;
@@ -218,7 +219,10 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
           p.c64 = cs.x;
           p.s64 = cs.y;
           flag = 0;
-          if (!a.edge_pad) {
+          if (a.slope) {
+            // slope mode is continuous (edges smoothed over one bin)
+            if (pmin > (double)ncol + 1e-2 || pmax < -1.0 - 1e-2) flag = 1;
+          } else if (!a.edge_pad) {
             if (pmin > (double)(ncol - 1) + 1e-2 || pmax < -1e-2) flag = 1;
             else if (pmin < 1e-2 || pmax > (double)(ncol - 1) - 1e-2) flag = 2;
           }
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
             if (ks < nsl && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
           }
         }
-        if (edge_pad && s_jl < nsl) {
+        if ((edge_pad || slope) && s_jl < nsl) {
           cp_async4(&edge_s[buf][s_ai][s_jl][0], src + s_jl * sss);
           cp_async4(&edge_s[buf][s_ai][s_jl][1], src + s_jl * sss + ncol1);
         }
@@ -282,7 +286,8 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
     const int lo = lo_s[buf][s_ai];
     const int base = (lo >> 2) << 2;
     // every d and d+1 of the window inside [0, ncol-1] with d <= ncol-2
-    const bool interior = lo >= 0 && lo + kWin <= ncol1;
+    // (slope mode: also clear of the smoothed edges at bins 0 and ncol-2)
+    const bool interior = slope ? (lo >= 1 && lo + kWin <= ncol1 - 1) : (lo >= 0 && lo + kWin <= ncol1);
     const float *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
     const T *row = sino + i * srs;
     // detector sample x (0 <= x <= ncol-1) of slice ks
@@ -313,6 +318,25 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
               v = atb::load_as_float(row + ks * sss + d);
               w = atb::load_as_float(row + ks * sss + d + 1) - v;
             }
+          } else if (slope) {
+            // derivative in p of the back-projected interpolant with its two
+            // edge steps (+s[0] at p = 0, -s[ncol-1] at p = ncol-1) smoothed
+            // over one bin: on bin d, value A + B f with f = p - d; stored
+            // below as (A, B) in the (value, difference) slots
+            float A = 0.f, B = 0.f;
+            if (d >= 0 && d < ncol1) A = val(ks, d + 1) - val(ks, d);
+            if (d == -1 || d == 0) {
+              const float e0 = val(ks, 0);
+              if (d == -1) B += e0;
+              else { A += e0; B -= e0; }
+            }
+            if (d == ncol1 - 1 || d == ncol1) {
+              const float e1 = val(ks, ncol1);
+              if (d == ncol1 - 1) B -= e1;
+              else { A -= e1; B += e1; }
+            }
+            v = A;
+            w = B;
           } else if (edge_pad) {
             const int d0 = min(max(d, 0), ncol1), d1 = min(max(d + 1, 0), ncol1);
             v = val(ks, d0);
@@ -324,10 +348,10 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
             v = val(ks, d);  // last bin: its value only at p = ncol-1
           }
         }
-        if (slope) {  // derivative of the interpolant with respect to p
+        if (slope && interior) {  // slope of the interpolant, constant per bin
           av[ks] = w;
           dv[ks] = 0.f;
-        } else {
+        } else {  // value v + w f on bin d, f = p - d = q - (j - H)
           av[ks] = fmaf(-jc, w, v);
           dv[ks] = w;
         }
@@ -465,11 +489,58 @@ __global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
 }
 
 template <typename T, int S, bool kPerAngleKahan>
+__global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  bp_tile<T, S, kPerAngleKahan>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+}
+
+// Persistent back-projection of a batch of single-slice items of uneven
+// shapes: every CTA pulls work units (item, tile) from counter[0] until the
+// list is exhausted; the last CTA to leave resets counter[0] and counter[1]
+// to zero, so the next launch (or graph replay) starts from a clean state.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2)
+    bp_batch_kernel(const atb_bp_item *items, const int *units, int nunits, int *counter) {
+  using K = BPCfg<T, 1>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int unit_s;
+  for (;;) {
+    __syncthreads();  // the previous unit is done with unit_s
+    if (threadIdx.x == 0) unit_s = atomicAdd(counter, 1);
+    __syncthreads();
+    const int u = unit_s;
+    if (u >= nunits) break;
+    const unsigned code = (unsigned)units[u];
+    const atb_bp_item it = items[code >> 16];
+    const int tile = (int)(code & 0xffffu);
+    BPArgs a;
+    a.sino = it.sino; a.srs = it.sino_row_stride; a.sss = 0;
+    a.nrow = it.nrow; a.nslice = 1; a.ncol = it.ncol; a.slice_base = 0;
+    a.trig = reinterpret_cast<const double2 *>(it.trig);
+    a.center = it.center; a.edge_pad = it.edge_pad; a.mask_r2 = it.mask_r2; a.scale = it.scale;
+    a.out = it.out; a.ors = it.out_row_stride; a.oss = 0;
+    a.slope = 0;
+    a.vec16 = sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(it.sino) % 16) == 0 &&
+              it.sino_row_stride % 4 == 0 && it.ncol % 4 == 0;
+    const int tiles_x = (it.ncol + K::TX - 1) / K::TX;
+    bp_tile<T, 1, false>(a, tile % tiles_x, tile / tiles_x, 0, smem);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(counter + 1, 1) == (int)gridDim.x - 1) {
+      atomicExch(counter, 0);
+      atomicExch(counter + 1, 0);
+      __threadfence();
+    }
+  }
+}
+
+template <typename T, int S, bool kPerAngleKahan>
 int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
   using K = BPCfg<T, S>;
   auto fn = bp_kernel<T, S, kPerAngleKahan>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::kSmem);
-  if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_backproject: %s", cudaGetErrorString(e));
+  const int rc = atb::ensure_smem(fn, K::kSmem, "atb_backproject");
+  if (rc != ATB_OK) return rc;
   dim3 grid((a.ncol + K::TX - 1) / K::TX, (a.ncol + K::TY - 1) / K::TY, (nslices + S - 1) / S);
   fn<<<grid, kThreads, K::kSmem, st>>>(a);
   return atb::check_launch("atb_backproject");
@@ -524,4 +595,65 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
     case ATB_BF16: return dispatch<__nv_bfloat16>(a, pak, st);
     default: return atb::fail(ATB_EINVAL, "atb_backproject: unknown sino_dtype %d", sino_dtype);
   }
+}
+
+namespace {
+int sm_count() {
+  static int cache[64] = {0};
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev]) return cache[dev];
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  cache[dev] = n;
+  return n;
+}
+constexpr int kBatchTile = 64;  // tile edge of the single-slice geometry
+}  // namespace
+
+extern "C" int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units, int capacity) {
+  if (!items || nitems < 1) return atb::fail(ATB_EINVAL, "atb_bp_batch_plan: no items");
+  if (nitems > 65536) return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: nitems=%d > 65536", nitems);
+  long long total = 0;
+  for (int b = 0; b < nitems; ++b) {
+    const atb_bp_item &it = items[b];
+    if (it.nrow < 1 || it.ncol < 1) return atb::fail(ATB_EINVAL, "atb_bp_batch_plan: item %d bad shape", b);
+    const long long t = (long long)((it.ncol + kBatchTile - 1) / kBatchTile) * ((it.ncol + kBatchTile - 1) / kBatchTile);
+    if (t > 65536) return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: item %d has ncol=%d > 16384", b, it.ncol);
+    total += t;
+  }
+  if (!units) return (int)total;  // size query
+  if (total > capacity) return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: %lld units > capacity %d", total, capacity);
+  // longest-processing-time order: items by angle count, largest first
+  // (every unit of an item costs nrow angle passes over one tile)
+  int *order = new int[nitems];
+  for (int b = 0; b < nitems; ++b) order[b] = b;
+  for (int x = 1; x < nitems; ++x) {  // stable insertion sort, nitems is small
+    const int v = order[x];
+    int y = x - 1;
+    while (y >= 0 && items[order[y]].nrow < items[v].nrow) { order[y + 1] = order[y]; --y; }
+    order[y + 1] = v;
+  }
+  int n = 0;
+  for (int q = 0; q < nitems; ++q) {
+    const int b = order[q];
+    const int tx = (items[b].ncol + kBatchTile - 1) / kBatchTile;
+    for (int t = 0; t < tx * tx; ++t) units[n++] = (int)(((unsigned)b << 16) | (unsigned)t);
+  }
+  delete[] order;
+  return n;
+}
+
+extern "C" int atb_backproject_batch(const atb_bp_item *items, int nitems, const int *units, int nunits,
+                                     int *counter, int max_ctas, void *stream) {
+  if (!items || !units || !counter) return atb::fail(ATB_EINVAL, "atb_backproject_batch: null pointer");
+  if (nitems < 1 || nunits < 1) return atb::fail(ATB_EINVAL, "atb_backproject_batch: empty batch");
+  using K = BPCfg<float, 1>;
+  static_assert(K::TX == kBatchTile && K::TY == kBatchTile, "batch tiles are square");
+  const int rc = atb::ensure_smem(bp_batch_kernel<float>, K::kSmem, "atb_backproject_batch");
+  if (rc != ATB_OK) return rc;
+  int grid = 2 * sm_count();
+  if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
+  if (grid > nunits) grid = nunits;
+  bp_batch_kernel<float><<<grid, kThreads, K::kSmem, atb::as_stream(stream)>>>(items, units, nunits, counter);
+  return atb::check_launch("atb_backproject_batch");
 }

@@ -20,6 +20,15 @@ int check_launch(const char *what);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Raises a kernel's dynamic shared-memory limit once per (kernel, device),
+// so that launches made while a stream is being captured into a CUDA graph
+// issue no configuration calls.  Thread-safe.  Returns 0 or ATB_ECUDA.
+int ensure_smem_raw(const void *fn, size_t bytes, const char *what);
+template <typename F>
+int ensure_smem(F *fn, size_t bytes, const char *what) {
+  return ensure_smem_raw(reinterpret_cast<const void *>(fn), bytes, what);
+}
+
 __device__ __forceinline__ float load_as_float(const float *p) { return __ldg(p); }
 __device__ __forceinline__ float load_as_float(const __half *p) { return __half2float(__ldg(p)); }
 __device__ __forceinline__ float load_as_float(const __nv_bfloat16 *p) {

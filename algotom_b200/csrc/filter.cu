@@ -377,9 +377,8 @@ __global__ void neg_log_kernel(const float *__restrict__ src, long long srs, lon
 template <typename OutT, int T>
 int launch_filter_t(const FilterArgs &a, long long npairs, cudaStream_t st) {
   const size_t smem = sizeof(float2) * (size_t)((1 << a.log2m) + ((1 << a.log2m) >> 4));
-  cudaError_t e = cudaFuncSetAttribute(filter_rows_kernel<OutT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_filter_rows: %s", cudaGetErrorString(e));
+  const int rc = atb::ensure_smem(filter_rows_kernel<OutT, T>, smem, "atb_filter_rows");
+  if (rc != ATB_OK) return rc;
   filter_rows_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(a);
   return atb::check_launch("atb_filter_rows");
 }

@@ -1,0 +1,165 @@
+"""Batched FBP of sinograms of uneven width, angle count and centre.
+
+The reference reconstructs one slice (or one chunk of slices sharing a
+geometry) per call (``algotom/rec/reconstruction.py:362-493``).  Here a whole
+list of single-slice problems -- each with its own width, angles and centre --
+is filtered (one ``atb_filter_rows`` launch per item) and back-projected in
+ONE persistent launch (``atb_backproject_batch``): a device counter hands out
+(item, 64 x 64 tile) work units, largest angle counts first.  The whole
+sequence can be captured once into a CUDA graph and replayed; the persistent
+kernel returns its counter to zero, so replays need no reset.
+
+Every item uses the reference's FBP semantics: filter (window, pad, pad
+mode), back-projection without edge padding, circle mask and pi/(nrow-1)
+scale.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from . import reconstruction as R
+
+
+class BatchedFBP:
+    """A fixed batch geometry with device buffers, runnable and capturable.
+
+    Parameters
+    ----------
+    shapes : list of (nrow, ncol)
+    centers : list of float (rounded to float32 like the reference)
+    angles : list of 1-D arrays (radians), one per item
+    filter_name, pad, pad_mode, ratio : as ``fbp_reconstruction``
+    """
+
+    def __init__(self, shapes, centers, angles, filter_name="hann", pad=None,
+                 pad_mode="edge", ratio=1.0, device=None):
+        self.dev = torch.device(device) if device is not None else R._device()
+        self.n = len(shapes)
+        if not (len(centers) == len(angles) == self.n) or self.n == 0:
+            raise ValueError("shapes, centers and angles must have one entry "
+                             "per item")
+        self.filter_name, self.pad_mode = filter_name, pad_mode
+        self.inputs, self.filtered, self.outputs = [], [], []
+        self._trig, self._spec, self._pad, self._log2m = [], [], [], []
+        self._tw = []
+        items = (nat.BpItem * self.n)()
+        for b, ((nrow, ncol), cen, ang) in enumerate(zip(shapes, centers,
+                                                         angles)):
+            nrow, ncol = int(nrow), int(ncol)
+            if len(ang) != nrow:
+                raise ValueError("item %d: %d angles for %d rows"
+                                 % (b, len(ang), nrow))
+            if cen < 0 or cen >= ncol:
+                raise ValueError("item %d: Center is out of the range "
+                                 "[0, %d]" % (b, ncol - 1))
+            p = min(int(0.15 * ncol), 150) if pad is None else int(pad)
+            log2m = nat.call("atb_filter_log2m", ncol, p)
+            spec, _ = R._spectrum(None, filter_name, nrow, ncol, p, log2m,
+                                  self.dev)
+            x = torch.zeros((nrow, ncol), dtype=torch.float32,
+                            device=self.dev)
+            f = torch.empty_like(x)
+            o = torch.empty((ncol, ncol), dtype=torch.float32,
+                            device=self.dev)
+            trig = R._trig(ang, self.dev)
+            self.inputs.append(x)
+            self.filtered.append(f)
+            self.outputs.append(o)
+            self._trig.append(trig)
+            self._spec.append(spec)
+            self._pad.append(p)
+            self._log2m.append(log2m)
+            self._tw.append(R._twiddle(log2m, self.dev))
+            it = items[b]
+            it.sino, it.sino_row_stride = f.data_ptr(), f.stride(0)
+            it.trig = trig.data_ptr()
+            it.out, it.out_row_stride = o.data_ptr(), o.stride(0)
+            it.center = float(np.float32(cen))
+            it.mask_r2 = R._mask_r2(ratio, float(cen), ncol)
+            it.scale = R._scale(nrow)
+            it.nrow, it.ncol, it.edge_pad = nrow, ncol, 0
+        self.items_host = items
+        nunits = nat.call("atb_bp_batch_plan", ctypes.addressof(items),
+                          self.n, None, 0)
+        units = (ctypes.c_int * nunits)()
+        nat.call("atb_bp_batch_plan", ctypes.addressof(items), self.n,
+                 ctypes.addressof(units), nunits)
+        self.nunits = nunits
+        raw = bytes(items)
+        self.items_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8
+                                          ).to(self.dev)
+        self.units_dev = torch.frombuffer(bytearray(bytes(units)),
+                                          dtype=torch.int32).to(self.dev)
+        self.counter = torch.zeros(2, dtype=torch.int32, device=self.dev)
+        self.graph = None
+        self.updates = int(sum(r * c * c for r, c in shapes))
+
+    def launch(self, max_ctas=0):
+        """Filter every item, then one persistent back-projection launch."""
+        st = R._stream_ptr(self.dev)
+        for b in range(self.n):
+            x, f = self.inputs[b], self.filtered[b]
+            nrow, ncol = x.shape
+            nat.call("atb_filter_rows", x.data_ptr(), x.stride(0), 0, nrow, 1,
+                     ncol, self._pad[b], nat.PAD_MODES[self.pad_mode], 0,
+                     self._spec[b].data_ptr(), 1, self._tw[b].data_ptr(),
+                     self._log2m[b], f.data_ptr(), nat.F32, f.stride(0), 0,
+                     st)
+        nat.call("atb_backproject_batch", self.items_dev.data_ptr(), self.n,
+                 self.units_dev.data_ptr(), self.nunits,
+                 self.counter.data_ptr(), int(max_ctas), st)
+
+    def capture(self):
+        """Capture :meth:`launch` into a CUDA graph (after one warm launch)."""
+        self.launch()
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        self.graph = g
+        return g
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def __call__(self, sinograms):
+        """Copy the sinograms in, run (graph if captured), return outputs."""
+        for x, s in zip(self.inputs, sinograms):
+            x.copy_(torch.as_tensor(s), non_blocking=True)
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self.launch()
+        return self.outputs
+
+
+def uneven_batch_geometry(seed=3000, n_items=64, wmin=512, wmax=4096,
+                          amin=361, amax=3601, half_acq_every=8):
+    """Seeded geometry of the uneven batch workload.
+
+    Widths log-uniform in [wmin, wmax], angle counts uniform in
+    [amin, amax] over [0, pi), centres jittered +/-3 px around the middle.
+    Every ``half_acq_every``-th item stands for a 360-degree half-acquisition
+    scan after its conversion to 180 degrees: the stitched sinogram is
+    1.6 x the width (rotation axis 0.3 of the width off the detector
+    centre, i.e. at 0.8 of the width from the left edge, mirrored), with
+    the angle count of the 180-degree half.  Returns a list of dicts with
+    nrow, ncol, center, angles, half_acquisition.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(n_items):
+        w = int(round(np.exp(rng.uniform(np.log(wmin), np.log(wmax)))))
+        nrow = int(rng.integers(amin, amax + 1))
+        half = half_acq_every and (b % half_acq_every == half_acq_every - 1)
+        if half:
+            w = int(round(1.6 * w))
+        cen = (w - 1) / 2.0 + rng.uniform(-3.0, 3.0)
+        ang = np.linspace(0.0, np.pi, nrow, endpoint=False)
+        out.append(dict(nrow=nrow, ncol=w, center=cen, angles=ang,
+                        half_acquisition=bool(half)))
+    return out

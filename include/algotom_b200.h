@@ -117,10 +117,13 @@ int atb_neg_log(const float *src, int64_t src_row_stride,
  *   flags    bit 0: per-angle compensated (Kahan) accumulation instead of
  *            the default chunked Kahan (FP32 partials over a chunk of angles,
  *            compensated across chunks);
- *            bit 1: back-project the slope of the interpolant,
- *            s[d+1] - s[d] at d = floor(p), instead of its value: the
- *            derivative of the back-projection with respect to the centre
- *            (no counterpart in the reference; used by the autograd path)
+ *            bit 1: back-project the derivative of the interpolant with
+ *            respect to p instead of its value: s[d+1] - s[d] at
+ *            d = floor(p), plus the two detector-edge steps (+s[0] at
+ *            p = 0, -s[ncol-1] at p = ncol-1) smoothed over one bin; this
+ *            is the derivative of the back-projection with respect to the
+ *            centre (no counterpart in the reference; used by the autograd
+ *            path; edge_pad must be 0)
  */
 int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int64_t sino_slice_stride, int nrow, int nslice, int ncol,
@@ -147,6 +150,55 @@ int atb_radon_adjoint(const float *img, int64_t img_row_stride,
                       int ncol, const double *trig, double center, float *out,
                       int64_t out_row_stride, int64_t out_slice_stride,
                       void *stream);
+
+/*
+ * One single-slice back-projection of a batch (device pointers inside).
+ * Field meanings as in atb_backproject; the sinogram is float32.
+ */
+typedef struct {
+  const float *sino;        /* [nrow][ncol] */
+  int64_t sino_row_stride;
+  const double *trig;       /* [nrow][2] */
+  float *out;               /* [ncol][ncol] */
+  int64_t out_row_stride;
+  double center;
+  double mask_r2;
+  float scale;
+  int nrow;
+  int ncol;
+  int edge_pad;
+} atb_bp_item;
+
+/*
+ * Host-side work list of a batch for atb_backproject_batch: one entry per
+ * (item, 64 x 64 pixel tile), item index << 16 | tile, items ordered by
+ * angle count, largest first (longest-processing-time order).  With
+ * units == NULL returns the number of entries; otherwise fills up to
+ * `capacity` and returns the count.  ncol <= 16384, nitems <= 65536.
+ * No counterpart in the reference, which loops over slices on the host
+ * (reconstruction.py:482-487).
+ */
+int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units,
+                      int capacity);
+
+/*
+ * Back-projection of a batch of single-slice sinograms of uneven width,
+ * angle count and centre in one persistent launch: each CTA pulls work
+ * units from `counter` until `units` is exhausted.  Batched counterpart of
+ * __back_projection_gpu_kernel (reconstruction.py:156-190), one launch for
+ * what the reference does with one launch per call.
+ *
+ *   items    device array [nitems] of atb_bp_item
+ *   units    device array [nunits] from atb_bp_batch_plan
+ *   counter  device scratch, two int32, zero before the first call; the
+ *            kernel returns it to zero, so a CUDA graph can replay the launch
+ *   max_ctas 0: two CTAs per SM; otherwise at most this many CTAs
+ *
+ * Calls that share `counter` must not overlap on the device.
+ */
+int atb_backproject_batch(const atb_bp_item *items, int nitems,
+                          const int *units, int nunits, int *counter,
+                          int max_ctas, void *stream);
 
 #ifdef __cplusplus
 }

@@ -75,3 +75,25 @@ def test_bad_arguments_are_rejected():
 def test_call_raises_with_message():
     with pytest.raises(nat.NativeLibraryError, match="atb_filter_log2m"):
         nat.call("atb_filter_log2m", -5, 0)
+
+
+def test_batch_plan_orders_by_cost():
+    """The host-side work list: one unit per 64x64 tile, largest angle
+    counts first, item index in the high 16 bits."""
+    items = (nat.BpItem * 3)()
+    for it, (nrow, ncol) in zip(items, [(100, 64), (300, 130), (200, 65)]):
+        it.nrow, it.ncol = nrow, ncol
+    n = nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3, None, 0)
+    assert n == 1 + 9 + 4
+    units = (ctypes.c_int * n)()
+    assert nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3,
+                    ctypes.addressof(units), n) == n
+    got = [(u >> 16, u & 0xffff) for u in units]
+    assert got == [(1, t) for t in range(9)] + [(2, t) for t in range(4)] + \
+        [(0, 0)]
+    lib = nat.load()
+    assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3,
+                                 ctypes.addressof(units), 5) == -3
+    items[0].ncol = 20000
+    assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3, None, 0) == -3
+    assert "16384" in nat.last_error()

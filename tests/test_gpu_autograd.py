@@ -48,12 +48,44 @@ def test_adjoint_identity_device_pair(cuda, ncol, nrow, cen):
     assert abs(lhs - rhs) <= 2e-6 * float(bs.double().norm() * g.double().norm())
 
 
+BLOBS = [(20.0, -10.0, 12.0, 1.0), (-30.0, 25.0, 8.0, 0.7),
+         (5.0, 40.0, 15.0, 0.5)]
+
+
+def _blob_sino(ang, n, center):
+    """Exact projections of Gaussian blobs (x0, y0, sigma, amplitude)."""
+    u = np.arange(n)[None, :] - center
+    s = np.zeros((len(ang), n))
+    for x0, y0, sg, amp in BLOBS:
+        u0 = x0 * np.cos(ang) - y0 * np.sin(ang)
+        s += amp * np.sqrt(2 * np.pi) * sg * np.exp(-(u - u0[:, None]) ** 2
+                                                    / (2 * sg * sg))
+    return s
+
+
+def _blob_image(n):
+    ic = 0.5 * (n - 1)
+    yy, xx = np.mgrid[0:n, 0:n] - ic
+    img = np.zeros((n, n))
+    for x0, y0, sg, amp in BLOBS:
+        img += amp * np.exp(-((xx - x0) ** 2 + (yy - y0) ** 2) / (2 * sg * sg))
+    return img
+
+
+def _smooth_weight(n, seed=1):
+    import scipy.ndimage as ndi
+    return ndi.gaussian_filter(np.random.default_rng(seed).standard_normal(
+        (n, n)), 8) * 50
+
+
 def test_center_gradient_backprojection_fd(cuda):
-    """dL/dc of L = <B_c s, w> against central differences, step 1e-3."""
-    s, ang, _ = phantom.ellipse_sinogram(5, 60, 256, 127.7, photons=None)
-    st = torch.from_numpy(s).cuda()
-    w = torch.from_numpy(np.random.default_rng(1).standard_normal(
-        (256, 256)).astype(np.float32)).cuda()
+    """dL/dc of L = <B_c s, w> against central differences, step 1e-3,
+    for a smooth object and weight (the back-projection of a linear
+    interpolant has slope kinks wherever a position crosses a bin; smooth
+    inputs keep their sum inside the step below 1e-3 of the derivative)."""
+    n, ang = 256, np.linspace(0, np.pi, 60, endpoint=False)
+    st = torch.from_numpy(_blob_sino(ang, n, 127.7).astype(np.float32)).cuda()
+    w = torch.from_numpy(_smooth_weight(n).astype(np.float32)).cuda()
     c = torch.tensor(127.7, dtype=torch.float64, requires_grad=True)
     loss = (AG.back_projection(st, c, ang).double() * w.double()).sum()
     (gc,) = torch.autograd.grad(loss, [c])
@@ -61,19 +93,16 @@ def test_center_gradient_backprojection_fd(cuda):
     lp = _dot(AG.back_projection(st, 127.7 + h, ang), w)
     lm = _dot(AG.back_projection(st, 127.7 - h, ang), w)
     fd = (lp - lm) / (2 * h)
-    assert abs(float(gc) - fd) <= 1e-3 * max(abs(fd), 1e-12), (float(gc), fd)
+    assert abs(float(gc) - fd) <= 1e-3 * abs(fd), (float(gc), fd)
 
 
 def test_center_gradient_projection_fd(cuda):
     """dL/dc of L = ||A_c x - b||^2 / 2 against central differences."""
-    n = 192
-    params = phantom.ellipse_params(3, n)
-    x = torch.from_numpy(phantom.phantom_image(params, n).astype(np.float32)
-                         ).cuda()
+    n = 256
     ang = np.linspace(0, np.pi, 60, endpoint=False)
-    b = torch.from_numpy(phantom.analytic_sinogram(params, ang, n, 96.3)
-                         .astype(np.float32)).cuda()
-    c = torch.tensor(95.4, dtype=torch.float64, requires_grad=True)
+    x = torch.from_numpy(_blob_image(n).astype(np.float32)).cuda()
+    b = torch.from_numpy(_blob_sino(ang, n, 128.6).astype(np.float32)).cuda()
+    c = torch.tensor(127.4, dtype=torch.float64, requires_grad=True)
     r = AG.forward_projection(x, c, ang) - b
     loss = 0.5 * (r.double() ** 2).sum()
     (gc,) = torch.autograd.grad(loss, [c])
@@ -82,8 +111,46 @@ def test_center_gradient_projection_fd(cuda):
         rr = AG.forward_projection(x, cv, ang).double() - b.double()
         return float(0.5 * (rr ** 2).sum())
     h = 1e-3
-    fd = (L(95.4 + h) - L(95.4 - h)) / (2 * h)
+    fd = (L(127.4 + h) - L(127.4 - h)) / (2 * h)
     assert abs(float(gc) - fd) <= 1e-3 * abs(fd), (float(gc), fd)
+
+
+def _slope_model(s, ang, c):
+    """NumPy model of the slope mode: per bin d (f = p - d) the derivative
+    of the interpolant, plus +s[0] and -s[n-1] edge steps smoothed by a
+    one-bin hat."""
+    nrow, n = s.shape
+    ic = 0.5 * (n - 1)
+    xc = np.arange(n) - ic
+    out = np.zeros((n, n))
+    for i in range(nrow):
+        p = xc[None, :] * np.cos(-ang[i]) + xc[:, None] * np.sin(-ang[i]) + c
+        d = np.floor(p).astype(int)
+        f = p - d
+        row = s[i]
+        A = np.where((d >= 0) & (d < n - 1),
+                     row[np.clip(d + 1, 0, n - 1)] - row[np.clip(d, 0, n - 1)],
+                     0.0)
+        B = np.zeros_like(p)
+        A += np.where(d == 0, row[0], 0)
+        B += np.where(d == -1, row[0], 0) - np.where(d == 0, row[0], 0)
+        B -= np.where(d == n - 2, row[n - 1], 0)
+        A -= np.where(d == n - 1, row[n - 1], 0)
+        B += np.where(d == n - 1, row[n - 1], 0)
+        out += A + B * f
+    return out
+
+
+@pytest.mark.parametrize("n,cen", [(96, 47.3), (130, 60.9)])
+def test_slope_mode_matches_model(cuda, n, cen):
+    """Slope mode with non-zero detector edges (the smoothed edge steps)."""
+    rng = np.random.default_rng(n)
+    s = rng.uniform(0.5, 1.5, (40, n))
+    ang = rng.uniform(0, np.pi, 40)
+    got = AG._bp(torch.from_numpy(s.astype(np.float32)).cuda()[:, None],
+                 AG._trig(ang, torch.device("cuda")), cen, slope=True)
+    ref = _slope_model(s.astype(np.float32).astype(np.float64), ang, cen)
+    assert O.rel_l2(got[:, 0].cpu().numpy(), ref) < 1e-5
 
 
 def test_sinogram_gradient_is_adjoint(cuda):
@@ -100,12 +167,11 @@ def test_sinogram_gradient_is_adjoint(cuda):
 
 
 def test_iterative_reconstruction_with_center_refinement(cuda):
-    """Sparse-view least squares + TV descent recovers the image and moves
-    the centre toward the truth."""
+    """Sparse-view least squares + TV descent on the device recovers the
+    image and moves the centre toward the truth."""
     n, nrow, c_true = 256, 60, 127.7
-    params = phantom.ellipse_params(11, n)
     ang = np.linspace(0, np.pi, nrow, endpoint=False)
-    b = phantom.analytic_sinogram(params, ang, n, c_true)
+    b = _blob_sino(ang, n, c_true)
     b = b + np.random.default_rng(0).normal(0, 0.01 * b.max(), b.shape)
     bt = torch.from_numpy(b.astype(np.float32)).cuda()
     x, c, hist = AG.iterative_reconstruction(bt, ang, 125.5, n_iter=150,
