@@ -153,48 +153,86 @@ def total_variation(img, eps=1e-8):
     return torch.sqrt(dx[:-1, :] ** 2 + dy[:, :-1] ** 2 + eps).sum()
 
 
+def fbp_differentiable(sino, center, angles, filter_name="hann", pad=None):
+    """FBP (no mask) whose output is differentiable in the centre.
+
+    The ramp filter does not depend on the centre, so it runs once without
+    autograd (``atb_filter_rows``); the back-projection carries the centre
+    gradient.  ``sino``: float32 CUDA [nrow, ncol].
+    """
+    nrow, ncol = sino.shape
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    f = R.filter_sinograms(sino.detach()[:, None, :], pad, "edge", False,
+                           None, filter_name)[:, 0, :]
+    return back_projection(f, center, angles) * (np.pi / (nrow - 1))
+
+
+def estimate_center(sino, angles, center, n_steps=30, step=1.0,
+                    filter_name="hann"):
+    """Refine the rotation centre by minimising the reprojection error
+    ||A_c FBP_c(b) - b||^2 with the exact total derivative in c (through
+    both the back-projection and the projector).  Sign search: move by
+    ``step`` against the gradient, halve the step whenever its sign flips.
+    Returns (centre, history of (centre, loss)).
+    """
+    ang = np.asarray(angles, np.float64)
+    c_val, last, hist = float(center), 0.0, []
+    for _ in range(n_steps):
+        c = torch.tensor(c_val, dtype=torch.float64, requires_grad=True)
+        x = fbp_differentiable(sino, c, ang, filter_name)
+        r = forward_projection(x, c, ang) - sino
+        loss = (r.double() ** 2).sum()
+        (gc,) = torch.autograd.grad(loss, [c])
+        hist.append((c_val, float(loss.detach())))
+        g = float(gc)
+        if g == 0.0:
+            break
+        sgn = 1.0 if g > 0 else -1.0
+        if last and sgn != last:
+            step *= 0.5
+        c_val -= sgn * step
+        last = sgn
+    return c_val, hist
+
+
 def iterative_reconstruction(sino, angles, center, n_iter=200, tv_weight=1e-3,
-                             step=None, center_step=0.5, refine_center=True,
-                             center_warmup=20, x0=None):
+                             step=None, refine_center=True, center_steps=30,
+                             x0=None):
     """Gradient descent on ||A x - b||^2 / 2 + tv_weight TV(x), A = B^T.
 
-    With ``refine_center`` the centre is refined jointly from the gradient of
-    the same loss through the projector's centre dependence: after
-    ``center_warmup`` image steps (the centre gradient is uninformative while
-    x is still near zero), every iteration moves the centre by
-    ``center_step`` pixels against the sign of dL/dc and halves that step
-    whenever the sign flips.  ``sino``: float32 CUDA [nrow, ncol].  Returns
-    (image, centre, loss history).  ``step`` defaults to 1 / ||A||^2,
-    estimated by power iteration.
+    With ``refine_center`` the centre is first refined from ``center`` with
+    :func:`estimate_center` (gradient of the reprojection error through the
+    differentiable FBP and projector; with the image free, a joint descent
+    lets the image absorb a centre error).  The image descent starts from
+    zero (or ``x0``) with step 1 / ||A||^2 (power iteration).
+    ``sino``: float32 CUDA [nrow, ncol].  Returns (image, centre, loss
+    history of the image descent).
     """
     dev = sino.device
     nrow, ncol = sino.shape
     ang = np.asarray(angles, np.float64)
-    c = torch.tensor(float(center), dtype=torch.float64, requires_grad=True)
+    c = float(center)
+    if refine_center:
+        c, _ = estimate_center(sino, ang, c, n_steps=center_steps)
     x = (torch.zeros((ncol, ncol), dtype=torch.float32, device=dev)
          if x0 is None else x0.clone()).requires_grad_(True)
+    trig = _trig(ang, dev)
     if step is None:
-        trig = _trig(ang, dev)
         v = torch.rand((ncol, ncol), device=dev)
         for _ in range(20):
-            v = _from3_img(_bp(_radon(_as3_img(v), trig, float(center), nrow),
-                               trig, float(center)), True)
+            v = _from3_img(_bp(_radon(_as3_img(v), trig, c, nrow), trig, c),
+                           True)
             v = v / v.norm()
-        Av = _radon(_as3_img(v), trig, float(center), nrow)
+        Av = _radon(_as3_img(v), trig, c, nrow)
         step = 1.0 / max(float((Av.double() ** 2).sum()), 1e-12)
+    ct = torch.tensor(c, dtype=torch.float64)
     hist = []
-    cstep, last_sign = float(center_step), 0.0
-    for it in range(n_iter):
-        r = forward_projection(x, c, ang) - sino
+    for _ in range(n_iter):
+        r = forward_projection(x, ct, ang) - sino
         loss = 0.5 * (r * r).sum() + tv_weight * total_variation(x)
-        gx, gc = torch.autograd.grad(loss, [x, c])
+        (gx,) = torch.autograd.grad(loss, [x])
         with torch.no_grad():
             x -= step * gx
-            if refine_center and it >= center_warmup and float(gc) != 0.0:
-                sgn = 1.0 if float(gc) > 0 else -1.0
-                if last_sign and sgn != last_sign:
-                    cstep *= 0.5
-                c -= sgn * cstep
-                last_sign = sgn
-        hist.append(float(loss))
-    return x.detach(), float(c.detach()), hist
+        hist.append(float(loss.detach()))
+    return x.detach(), c, hist

@@ -35,10 +35,14 @@ METRIC = ("FBP pixel·angle updates/s and slices/s at 2560 det, "
           "rel-L2 err vs FP64 oracle")
 WORKLOAD = ("stacked FBP: 256 slices x 1801 angles x 2560 det, float32, "
             "centre 1278.3, hann, ratio 1.0, pad 150")
-# algorithmic FP32 work of one update (SURVEY 8(d) counting): position FMA,
-# fraction subtract, tap difference, interpolation FMA, accumulate add;
-# an FMA counts as 2 FLOP
+# algorithmic FP32 work of one update: position FMA, fraction subtract, tap
+# difference, interpolation FMA, accumulate add; an FMA counts as 2 FLOP
 FLOP_PER_UPDATE = 7.0
+# on-chip bytes one update must read: the two FP32 taps of its bin (held as
+# one 8-byte interpolation pair in shared memory)
+SMEM_BYTES_PER_UPDATE = 8.0
+SMEM_BYTES_PER_CLK_PER_SM = 128.0
+N_SM = 148
 
 
 def _args():
@@ -326,9 +330,11 @@ def run_ours(args, rank, world, local_rank):
 
     peaks, src = _peaks()
     f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
-    fp32_peak = 2.0 * 128 * 148 * f_clk / 1e12          # TFLOP/s
+    fp32_peak = 2.0 * 128 * N_SM * f_clk / 1e12          # TFLOP/s
+    smem_peak = SMEM_BYTES_PER_CLK_PER_SM * N_SM * f_clk / 1e9  # GB/s
     bp_upd = nslice * NCOL * NCOL * NROW
     achieved = FLOP_PER_UPDATE * bp_upd / t_bp / 1e12
+    smem_achieved = SMEM_BYTES_PER_UPDATE * bp_upd / t_bp / 1e9
     tpu = _traffic_per_update()
     filt_bytes = NROW * nslice * NCOL * 8.0
     line = {
@@ -343,14 +349,22 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (4.7 GB sinogram per GPU)"},
         "slices_per_s": world * nslice * args.steps / t_dev,
         "accuracy": err,
-        "roofline": {"bound": "fp32", "kernel": "bp_tile_kernel",
-                     "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+        "roofline": {"bound": "smem", "kernel": "bp_kernel",
+                     "achieved": smem_achieved, "peak": smem_peak,
+                     "unit": "GB/s", "frac": smem_achieved / smem_peak,
                      "traffic": (tpu * bp_upd if tpu else None),
-                     "flop_per_update": FLOP_PER_UPDATE,
+                     "bytes_per_update": SMEM_BYTES_PER_UPDATE,
+                     "updates_per_s": bp_upd / t_bp,
                      "ms_per_launch": t_bp * 1e3,
-                     "peak_source": "FP32 FMA pipe, 148 SM x 128 lanes x "
-                                    "sm_max_mhz (%s)" % src},
+                     "peak_source": "shared-memory delivery, 128 B/clk x 148 "
+                                    "SM x sm_max_mhz (%s); traffic = DRAM "
+                                    "bytes per launch" % src},
+        "fp32_roofline": {"bound": "fp32", "achieved": achieved,
+                          "peak": fp32_peak, "unit": "TFLOP/s",
+                          "frac": achieved / fp32_peak,
+                          "flop_per_update": FLOP_PER_UPDATE,
+                          "peak_source": "FP32 FMA pipe, 148 SM x 128 lanes "
+                                         "x 2 x sm_max_mhz (%s)" % src},
         "filter_roofline": {"bound": "hbm", "kernel": "filter_rows_kernel",
                             "achieved": filt_bytes / t_filt / 1e9,
                             "peak": float(peaks.get("hbm_gbs", 6650.0)),

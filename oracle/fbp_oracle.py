@@ -115,7 +115,8 @@ def filter_kernel_spatial(width, filter_name=None):
 # --------------------------------------------------------------------------
 # Back-projection
 # --------------------------------------------------------------------------
-def back_projection(sinogram, angles, center, edge_pad=False):
+def back_projection(sinogram, angles, center, edge_pad=False,
+                    round_inputs=True):
     """FP64 linear-interpolation back-projection of one sinogram.
 
     Restates ``back_projection_cpu`` (``reconstruction.py:307-359``) and the
@@ -125,12 +126,17 @@ def back_projection(sinogram, angles, center, edge_pad=False):
     ``s[d] + (s[u]-s[d]) (p-d)`` with ``d = floor(p)``, ``u = ceil(p)`` (just
     ``s[d]`` when ``u == d``); otherwise it adds ``s[0]`` (``p < 0``) or
     ``s[ncol-1]`` when ``edge_pad``, else nothing.  Angles and centre are
-    rounded to float32 first, as the reference does before every call.
+    rounded to float32 first, as the reference does before every call
+    (``round_inputs=False`` keeps them exact, for derivative checks).
     """
     sino = np.asarray(sinogram, dtype=np.float64)
     nrow, ncol = sino.shape
-    ang = np.float32(np.asarray(angles)).astype(np.float64)
-    cen = float(np.float32(center))
+    if round_inputs:
+        ang = np.float32(np.asarray(angles)).astype(np.float64)
+        cen = float(np.float32(center))
+    else:
+        ang = np.asarray(angles, dtype=np.float64)
+        cen = float(center)
     ic = 0.5 * (ncol - 1)
     xc = np.arange(ncol, dtype=np.float64) - ic
     out = np.zeros((ncol, ncol))
@@ -149,6 +155,34 @@ def back_projection(sinogram, angles, center, edge_pad=False):
             val = np.where(p < 0.0, row[0], val)
             val = np.where(p > ncol - 1, row[ncol - 1], val)
         out += val
+    return out
+
+
+def forward_projection(image, angles, center):
+    """FP64 adjoint of :func:`back_projection` (no edge padding).
+
+    Scatters each pixel with position ``p`` in ``[0, ncol-1]`` onto bins
+    ``floor(p)`` and ``floor(p)+1`` with weights ``1-f`` and ``f`` -- the
+    transpose of the reference back-projector's interpolation
+    (``reconstruction.py:307-359``).  Angles and centre are used as given
+    (no float32 rounding), as for a differentiable model.
+    """
+    img = np.asarray(image, dtype=np.float64)
+    ncol = img.shape[0]
+    ang = np.asarray(angles, dtype=np.float64)
+    ic = 0.5 * (ncol - 1)
+    xc = np.arange(ncol, dtype=np.float64) - ic
+    out = np.zeros((len(ang), ncol))
+    for i, a in enumerate(ang):
+        p = xc[None, :] * math.cos(-a) + xc[:, None] * math.sin(-a) + center
+        ok = (p >= 0.0) & (p <= ncol - 1)
+        pc = p[ok]
+        v = img[ok]
+        d = np.floor(pc).astype(np.int64)
+        f = pc - d
+        np.add.at(out[i], d, (1.0 - f) * v)
+        hi = d + 1 <= ncol - 1
+        np.add.at(out[i], d[hi] + 1, (f * v)[hi])
     return out
 
 

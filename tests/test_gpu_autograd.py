@@ -79,36 +79,42 @@ def _smooth_weight(n, seed=1):
 
 
 def test_center_gradient_backprojection_fd(cuda):
-    """dL/dc of L = <B_c s, w> against central differences, step 1e-3,
-    for a smooth object and weight (the back-projection of a linear
-    interpolant has slope kinks wherever a position crosses a bin; smooth
-    inputs keep their sum inside the step below 1e-3 of the derivative)."""
+    """dL/dc of L = <B_c s, w> against FP64 central differences (step 1e-3)
+    of the reference back-projector, for a smooth object and weight (the
+    back-projection of a linear interpolant has slope kinks wherever a
+    position crosses a bin; smooth inputs keep their effect inside the step
+    well below 1e-3 of the derivative)."""
     n, ang = 256, np.linspace(0, np.pi, 60, endpoint=False)
-    st = torch.from_numpy(_blob_sino(ang, n, 127.7).astype(np.float32)).cuda()
-    w = torch.from_numpy(_smooth_weight(n).astype(np.float32)).cuda()
+    s = _blob_sino(ang, n, 127.7).astype(np.float32)
+    w = _smooth_weight(n).astype(np.float32)
     c = torch.tensor(127.7, dtype=torch.float64, requires_grad=True)
-    loss = (AG.back_projection(st, c, ang).double() * w.double()).sum()
+    loss = (AG.back_projection(torch.from_numpy(s).cuda(), c, ang).double()
+            * torch.from_numpy(w).cuda().double()).sum()
     (gc,) = torch.autograd.grad(loss, [c])
+
+    def L(cv):
+        return float((O.back_projection(s, ang, cv, round_inputs=False)
+                      * w).sum())
     h = 1e-3
-    lp = _dot(AG.back_projection(st, 127.7 + h, ang), w)
-    lm = _dot(AG.back_projection(st, 127.7 - h, ang), w)
-    fd = (lp - lm) / (2 * h)
+    fd = (L(127.7 + h) - L(127.7 - h)) / (2 * h)
     assert abs(float(gc) - fd) <= 1e-3 * abs(fd), (float(gc), fd)
 
 
 def test_center_gradient_projection_fd(cuda):
-    """dL/dc of L = ||A_c x - b||^2 / 2 against central differences."""
+    """dL/dc of L = ||A_c x - b||^2 / 2 against FP64 central differences of
+    the adjoint of the reference back-projector."""
     n = 256
     ang = np.linspace(0, np.pi, 60, endpoint=False)
-    x = torch.from_numpy(_blob_image(n).astype(np.float32)).cuda()
-    b = torch.from_numpy(_blob_sino(ang, n, 128.6).astype(np.float32)).cuda()
+    x = _blob_image(n).astype(np.float32)
+    b = _blob_sino(ang, n, 128.6).astype(np.float32)
     c = torch.tensor(127.4, dtype=torch.float64, requires_grad=True)
-    r = AG.forward_projection(x, c, ang) - b
+    r = AG.forward_projection(torch.from_numpy(x).cuda(), c, ang) - \
+        torch.from_numpy(b).cuda()
     loss = 0.5 * (r.double() ** 2).sum()
     (gc,) = torch.autograd.grad(loss, [c])
 
     def L(cv):
-        rr = AG.forward_projection(x, cv, ang).double() - b.double()
+        rr = O.forward_projection(x, ang, cv) - b
         return float(0.5 * (rr ** 2).sum())
     h = 1e-3
     fd = (L(127.4 + h) - L(127.4 - h)) / (2 * h)
@@ -144,9 +150,13 @@ def _slope_model(s, ang, c):
 @pytest.mark.parametrize("n,cen", [(96, 47.3), (130, 60.9)])
 def test_slope_mode_matches_model(cuda, n, cen):
     """Slope mode with non-zero detector edges (the smoothed edge steps)."""
+    # smooth rows with non-zero edges: the slope is piecewise constant in p,
+    # so FP32 and FP64 positions may pick neighbouring bins; smooth data
+    # keeps those neighbours' slopes close
     rng = np.random.default_rng(n)
-    s = rng.uniform(0.5, 1.5, (40, n))
     ang = rng.uniform(0, np.pi, 40)
+    u = np.arange(n)[None, :]
+    s = 1.0 + 0.5 * np.sin(0.05 * u + rng.uniform(0, 6, (40, 1)))
     got = AG._bp(torch.from_numpy(s.astype(np.float32)).cuda()[:, None],
                  AG._trig(ang, torch.device("cuda")), cen, slope=True)
     ref = _slope_model(s.astype(np.float32).astype(np.float64), ang, cen)
@@ -167,8 +177,9 @@ def test_sinogram_gradient_is_adjoint(cuda):
 
 
 def test_iterative_reconstruction_with_center_refinement(cuda):
-    """Sparse-view least squares + TV descent on the device recovers the
-    image and moves the centre toward the truth."""
+    """Sparse-view least squares + TV descent on the device after centre
+    refinement through the differentiable FBP: the centre lands near the
+    truth and the data misfit drops."""
     n, nrow, c_true = 256, 60, 127.7
     ang = np.linspace(0, np.pi, nrow, endpoint=False)
     b = _blob_sino(ang, n, c_true)
@@ -177,4 +188,6 @@ def test_iterative_reconstruction_with_center_refinement(cuda):
     x, c, hist = AG.iterative_reconstruction(bt, ang, 125.5, n_iter=150,
                                              tv_weight=1e-3)
     assert hist[-1] < 0.05 * hist[0]
-    assert abs(c - c_true) < 0.25 * abs(125.5 - c_true), c
+    assert abs(c - c_true) < 0.25, c
+    truth = _blob_image(n)
+    assert O.rel_l2(x.cpu().numpy(), truth) < 0.25
