@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 # every symbol include/algotom_b200.h declares
 EXPORTS = ("atb_version", "atb_last_error", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
-           "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch")
+           "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
+           "atb_backproject_batch_noalloc")
 
 F32, F16, BF16 = 0, 1, 2
 PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
@@ -59,6 +60,8 @@ _SIGS = {
     "atb_bp_batch_plan": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
     "atb_backproject_batch": (ctypes.c_int, [
         _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
+    "atb_backproject_batch_noalloc": (ctypes.c_int, [
+        _vp, ctypes.c_int, ctypes.c_int, _vp]),
 }
 
 _lib = None

@@ -49,6 +49,7 @@
 // chunks with Kahan compensation (the single-slice kernel can instead
 // compensate every angle).  One warp instruction covers an 8 x 4 pixel
 // block, whose 32 lanes read a run of about 9 neighbouring bins.
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -656,4 +657,117 @@ extern "C" int atb_backproject_batch(const atb_bp_item *items, int nitems, const
   if (grid > nunits) grid = nunits;
   bp_batch_kernel<float><<<grid, kThreads, K::kSmem, atb::as_stream(stream)>>>(items, units, nunits, counter);
   return atb::check_launch("atb_backproject_batch");
+}
+
+// ---------------------------------------------------------------------------
+// Batched back-projection for callers that cannot allocate device memory.
+//
+// Some callers hold device buffers for their inputs and outputs but may not
+// call cudaMalloc themselves: a plugin inside an application whose memory
+// pool must account for every device byte, a latency-bound loop that cannot
+// afford cudaMalloc's implicit synchronisation, or a foreign-language caller
+// that is handed device pointers but has no CUDA runtime to allocate with.
+// atb_backproject_batch needs three small device scratch buffers from its
+// caller (item table, work list, counter).  The entry point below keeps them
+// instead in one file-scope __device__ array of fixed size, which every GPU
+// that loads this library holds until the process exits.
+namespace {
+
+constexpr int kNoAllocMaxItems = 4096;
+constexpr int kNoAllocMaxUnits = 1 << 20;
+constexpr size_t kNoAllocItemsOffset = 256;  // the counter pair sits first
+constexpr size_t kNoAllocUnitsOffset =
+    kNoAllocItemsOffset + ((sizeof(atb_bp_item) * kNoAllocMaxItems + 255) / 256) * 256;
+constexpr size_t kNoAllocBytes = kNoAllocUnitsOffset + sizeof(int) * (size_t)kNoAllocMaxUnits;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// host-side staging of the item table and work list (static: no heap use);
+// guarded by g_noalloc_mu together with the per-device scratch addresses
+atb_bp_item g_noalloc_items[kNoAllocMaxItems];
+int g_noalloc_order[kNoAllocMaxItems];
+int g_noalloc_units[kNoAllocMaxUnits];
+unsigned char *g_noalloc_dev[64] = {nullptr};
+std::mutex g_noalloc_mu;
+
+}  // namespace
+
+extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems, int max_ctas, void *stream) {
+  if (!items) return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: null item table");
+  if (nitems < 1) return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: empty batch");
+  if (nitems > kNoAllocMaxItems)
+    return atb::fail(ATB_ERANGE, "atb_backproject_batch_noalloc: nitems=%d exceeds the fixed limit of %d items",
+                     nitems, kNoAllocMaxItems);
+  long long nunits = 0;
+  for (int b = 0; b < nitems; ++b) {
+    const atb_bp_item &it = items[b];
+    if (!it.sino || !it.trig || !it.out || it.nrow < 1 || it.ncol < 1)
+      return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: item %d is incomplete", b);
+    if (it.ncol > 16384)
+      return atb::fail(ATB_ERANGE, "atb_backproject_batch_noalloc: item %d has ncol=%d > 16384", b, it.ncol);
+    if (!(it.center >= 0.0) || it.center >= (double)it.ncol)
+      return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: item %d centre outside [0, ncol)", b);
+    const long long t = (it.ncol + kBatchTile - 1) / kBatchTile;
+    nunits += t * t;
+  }
+  if (nunits > kNoAllocMaxUnits)
+    return atb::fail(ATB_ERANGE,
+                     "atb_backproject_batch_noalloc: %lld tiles of 64 x 64 exceed the fixed limit of %d",
+                     nunits, kNoAllocMaxUnits);
+
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64)
+    return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: no usable current device");
+  if (!g_noalloc_dev[dev]) {  // first call on this device: host address of the scratch array
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: cudaGetSymbolAddress: %s",
+                       cudaGetErrorString(e));
+    g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+  }
+  unsigned char *base = g_noalloc_dev[dev];
+  int *counter = reinterpret_cast<int *>(base);
+  atb_bp_item *items_dev = reinterpret_cast<atb_bp_item *>(base + kNoAllocItemsOffset);
+  int *units_dev = reinterpret_cast<int *>(base + kNoAllocUnitsOffset);
+
+  // work list in longest-processing-time order, as atb_bp_batch_plan
+  for (int b = 0; b < nitems; ++b) {
+    g_noalloc_items[b] = items[b];
+    g_noalloc_order[b] = b;
+  }
+  for (int x = 1; x < nitems; ++x) {
+    const int v = g_noalloc_order[x];
+    int y = x - 1;
+    while (y >= 0 && items[g_noalloc_order[y]].nrow < items[v].nrow) {
+      g_noalloc_order[y + 1] = g_noalloc_order[y];
+      --y;
+    }
+    g_noalloc_order[y + 1] = v;
+  }
+  int n = 0;
+  for (int q = 0; q < nitems; ++q) {
+    const int b = g_noalloc_order[q];
+    const int tx = (items[b].ncol + kBatchTile - 1) / kBatchTile;
+    for (int t = 0; t < tx * tx; ++t) g_noalloc_units[n++] = (int)(((unsigned)b << 16) | (unsigned)t);
+  }
+
+  cudaStream_t st = atb::as_stream(stream);
+  // the array keeps the previous call's contents: the counter must start at 0
+  if ((e = cudaMemsetAsync(counter, 0, 2 * sizeof(int), st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(items_dev, g_noalloc_items, sizeof(atb_bp_item) * (size_t)nitems,
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(units_dev, g_noalloc_units, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess)
+    return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: %s", cudaGetErrorString(e));
+  using K = BPCfg<float, 1>;
+  const int rc = atb::ensure_smem(bp_batch_kernel<float>, K::kSmem, "atb_backproject_batch_noalloc");
+  if (rc != ATB_OK) return rc;
+  int grid = 2 * sm_count();
+  if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
+  if (grid > n) grid = n;
+  bp_batch_kernel<float><<<grid, kThreads, K::kSmem, st>>>(items_dev, units_dev, n, counter);
+  return atb::check_launch("atb_backproject_batch_noalloc");
 }

@@ -200,6 +200,33 @@ int atb_backproject_batch(const atb_bp_item *items, int nitems,
                           const int *units, int nunits, int *counter,
                           int max_ctas, void *stream);
 
+/*
+ * atb_backproject_batch for callers that cannot allocate device memory.
+ * No counterpart in the reference (it is an addition of this library).
+ *
+ * For a caller that owns device buffers for its sinograms, angle tables and
+ * outputs but may not call cudaMalloc -- a plugin whose host application
+ * accounts for every device byte, a loop that cannot afford cudaMalloc's
+ * implicit synchronisation, a foreign-language caller with no CUDA runtime
+ * of its own.  Takes the item table in HOST memory (device pointers inside)
+ * and keeps the work list, item table and counter in a fixed __device__
+ * array of this library (about 4.4 MB, held by every GPU that loads the
+ * library until the process exits).  It allocates nothing.
+ *
+ *   items     host array [nitems], nitems <= 4096; ncol <= 16384 per item
+ *   max_ctas  as atb_backproject_batch
+ *
+ * Limits: at most 4096 items and 1048576 tiles of 64 x 64 pixels in total;
+ * larger batches are rejected with ATB_ERANGE before any device work.
+ * The first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  Every call reuses the same array and overwrites the previous
+ * call's table: calls that overlap on the device (on different streams, or
+ * from different host threads without ordering) race on it.
+ */
+int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems,
+                                  int max_ctas, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,89 @@
+"""The allocation-free batch entry point against the allocating one.
+
+atb_backproject_batch_noalloc serves callers that hold device buffers for
+their data but may not call cudaMalloc (e.g. a plugin whose host application
+owns the device memory budget).  It keeps its scratch in a fixed device
+array of the library.  This test drives it through the C ABI, twice in a
+row (the second call must not see the first call's leftovers), and compares
+its output with atb_backproject_batch, which takes caller-allocated scratch.
+The file name keeps it last in collection order.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from algotom_b200 import _native as nat
+from algotom_b200 import phantom
+from algotom_b200.rec import batch as B
+from algotom_b200.rec import reconstruction as R
+from oracle import fbp_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5  # relative L2, the bar every FP32 reconstruction is held to
+
+
+def _batch():
+    geo = [(90, 64, 31.5), (181, 130, 66.0), (37, 97, 47.2), (240, 200, 98.9),
+           (61, 33, 16.0), (120, 257, 130.1)]
+    sinos, angs, shapes, cens = [], [], [], []
+    for k, (nrow, ncol, cen) in enumerate(geo):
+        s, a, _ = phantom.ellipse_sinogram(900 + k, nrow, ncol, cen,
+                                           photons=1e4)
+        sinos.append(s)
+        angs.append(a)
+        shapes.append((nrow, ncol))
+        cens.append(cen)
+    return sinos, angs, shapes, cens
+
+
+def test_noalloc_matches_allocating_entry_point_twice(cuda):
+    sinos, angs, shapes, cens = _batch()
+    bf = B.BatchedFBP(shapes, cens, angs)
+    for x, s in zip(bf.inputs, sinos):
+        x.copy_(torch.from_numpy(s))
+    bf.launch()  # filter + atb_backproject_batch (caller-provided scratch)
+    torch.cuda.synchronize()
+    reference = [o.clone() for o in bf.outputs]
+
+    stream = R._stream_ptr(cuda)
+    for call in range(2):
+        for o in bf.outputs:
+            o.fill_(float("nan"))
+        rc = nat.load().atb_backproject_batch_noalloc(
+            ctypes.addressof(bf.items_host), bf.n, 0, stream)
+        assert rc == 0, nat.last_error()
+        torch.cuda.synchronize()
+        for ref, got, s, a, c in zip(reference, bf.outputs, sinos, angs,
+                                     cens):
+            assert torch.isfinite(got).all()
+            err = O.rel_l2(got.cpu().numpy(), ref.cpu().numpy())
+            assert err < TOL, (call, err)
+        # and against the FP64 oracle, for one item per call
+        k = call
+        oracle = O.fbp_reconstruction(sinos[k], cens[k], angles=angs[k],
+                                      apply_log=False)
+        assert O.rel_l2(bf.outputs[k].cpu().numpy(), oracle) < TOL
+
+
+def test_noalloc_rejects_oversized_batches(cuda):
+    items = (nat.BpItem * 4097)()
+    lib = nat.load()
+    rc = lib.atb_backproject_batch_noalloc(ctypes.addressof(items), 4097, 0,
+                                           None)
+    assert rc == -3 and "4096" in nat.last_error()
+    one = (nat.BpItem * 1)()
+    t = torch.zeros(1, device=cuda)
+    one[0].sino = one[0].trig = one[0].out = t.data_ptr()
+    one[0].nrow, one[0].ncol, one[0].center = 10, 20000, 5.0
+    rc = lib.atb_backproject_batch_noalloc(ctypes.addressof(one), 1, 0, None)
+    assert rc == -3 and "16384" in nat.last_error()
+    one[0].ncol = 16384  # 256 x 256 tiles: within the 1048576-tile limit
+    big = (nat.BpItem * 17)()
+    for it in big:
+        it.sino = it.trig = it.out = t.data_ptr()
+        it.nrow, it.ncol, it.center = 10, 16384, 5.0
+    rc = lib.atb_backproject_batch_noalloc(ctypes.addressof(big), 17, 0, None)
+    assert rc == -3 and "1048576" in nat.last_error()
