@@ -56,6 +56,25 @@ extern "C" {
 
 int atb_version(void) { return 100; }
 
+int atb_copy_2d(void *dst, int64_t dst_pitch, const void *src, int64_t src_pitch, int64_t width, int64_t height,
+                int kind, void *stream) {
+  if (!dst || !src) return atb::fail(ATB_EINVAL, "atb_copy_2d: null pointer");
+  if (width < 0 || height < 0 || dst_pitch < width || src_pitch < width)
+    return atb::fail(ATB_EINVAL, "atb_copy_2d: bad extent");
+  if (width == 0 || height == 0) return ATB_OK;
+  cudaMemcpyKind k;
+  switch (kind) {
+    case 0: k = cudaMemcpyHostToDevice; break;
+    case 1: k = cudaMemcpyDeviceToHost; break;
+    case 2: k = cudaMemcpyDeviceToDevice; break;
+    default: return atb::fail(ATB_EINVAL, "atb_copy_2d: unknown kind %d", kind);
+  }
+  cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)dst_pitch, src, (size_t)src_pitch, (size_t)width, (size_t)height,
+                                    k, atb::as_stream(stream));
+  if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_copy_2d: %s", cudaGetErrorString(e));
+  return ATB_OK;
+}
+
 const char *atb_last_error(void) { return g_last_error; }
 
 }  // extern "C"

@@ -135,16 +135,19 @@ def filter_sinograms(sino3, pad, pad_mode="edge", apply_log=False,
 
 
 def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
-                scale=1.0, out=None, kahan="chunk"):
+                scale=1.0, out=None, kahan="chunk", trig=None):
     """Device back-projection of [nrow, nslice, ncol] -> [ncol, nslice, ncol].
 
     ``sino3`` may be float32, float16 or bfloat16 (last axis contiguous).
+    ``trig`` may hold the angle table from :func:`_trig` already on the
+    device (saves its host-to-device copy per call).
     """
     nrow, nslice, ncol = sino3.shape
     dev = sino3.device
     code = {torch.float32: nat.F32, torch.float16: nat.F16,
             torch.bfloat16: nat.BF16}[sino3.dtype]
-    trig = _trig(angles, dev)
+    if trig is None:
+        trig = _trig(angles, dev)
     if out is None:
         out = torch.empty((ncol, nslice, ncol), dtype=torch.float32,
                           device=dev)
@@ -274,6 +277,80 @@ def back_projection_cpu(sinogram, angles, center, edge_pad=False):
     return back_projection_gpu(sinogram, angles, center, edge_pad=edge_pad)
 
 
+SLAB = 32  # slices per slab when a host stack is streamed through the device
+
+
+def _host_tensor(x):
+    """C-contiguous float32 CPU tensor sharing the caller's memory when it
+    can (NumPy array or CPU tensor)."""
+    if isinstance(x, torch.Tensor):
+        t = x.detach()
+        if t.dtype != torch.float32 or not t.is_contiguous():
+            t = t.to(torch.float32).contiguous()
+        return t
+    a = np.asarray(x)
+    if a.dtype != np.float32 or not a.flags.c_contiguous:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+    return torch.from_numpy(a)
+
+
+def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
+                  pad, pad_mode, apply_log, out_host, storage, kahan,
+                  slab=SLAB):
+    """FBP of a host stack [nrow, nslice, ncol] streamed through the device
+    in slabs of ``slab`` slices: while slab k is filtered and
+    back-projected, slab k+1 is copied in and slab k-1 copied out (one copy
+    stream each way, double-buffered, ordered by events)."""
+    nrow, nslice, ncol = host.shape
+    dev = _device()
+    k_sl = max(1, min(slab, nslice))
+    cmp = torch.cuda.current_stream(dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    in_buf = [torch.empty((nrow, k_sl, ncol), dtype=torch.float32, device=dev)
+              for _ in range(2)]
+    out_buf = [torch.empty((ncol, k_sl, ncol), dtype=torch.float32,
+                           device=dev) for _ in range(2)]
+    for t in in_buf:
+        t.record_stream(s_in)
+    for t in out_buf:
+        t.record_stream(s_out)
+    ev_in_ready = [torch.cuda.Event() for _ in range(2)]
+    ev_in_free = [torch.cuda.Event() for _ in range(2)]
+    ev_out_ready = [torch.cuda.Event() for _ in range(2)]
+    ev_out_free = [torch.cuda.Event() for _ in range(2)]
+    row_b, slab_b = nslice * ncol * 4, k_sl * ncol * 4
+    hp, op = host.data_ptr(), out_host.data_ptr()
+    trig = _trig(angles, dev)
+    cmp.synchronize()
+    nslab = (nslice + k_sl - 1) // k_sl
+    for k in range(nslab):
+        b, k0 = k % 2, k * k_sl
+        kk = min(k_sl, nslice - k0)
+        if k >= 2:
+            s_in.wait_event(ev_in_free[b])
+        nat.call("atb_copy_2d", in_buf[b].data_ptr(), slab_b, hp + k0 * ncol * 4,
+                 row_b, kk * ncol * 4, nrow, 0, s_in.cuda_stream)
+        ev_in_ready[b].record(s_in)
+        cmp.wait_event(ev_in_ready[b])
+        f = filter_sinograms(in_buf[b][:, :kk, :], pad, pad_mode, apply_log,
+                             ramp_win, filter_name, storage)
+        ev_in_free[b].record(cmp)
+        if k >= 2:
+            cmp.wait_event(ev_out_free[b])
+        backproject(f, angles, center, edge_pad=False, mask_r2=mask_r2,
+                    scale=scale, out=out_buf[b][:, :kk, :], kahan=kahan,
+                    trig=trig)
+        ev_out_ready[b].record(cmp)
+        s_out.wait_event(ev_out_ready[b])
+        nat.call("atb_copy_2d", op + k0 * ncol * 4, row_b, out_buf[b].data_ptr(),
+                 slab_b, kk * ncol * 4, ncol, 1, s_out.cuda_stream)
+        ev_out_free[b].record(s_out)
+        del f
+    s_out.synchronize()
+    s_in.synchronize()
+    return out_host
+
+
 def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
                        ramp_win=None, filter_name="hann", pad=None,
                        pad_mode="edge", apply_log=True, gpu=True,
@@ -293,6 +370,26 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
         _check_log_input(sinogram)
     if pad is None:
         pad = min(int(0.15 * ncol), 150)
+    on_host = not (isinstance(sinogram, torch.Tensor) and sinogram.is_cuda)
+    if on_host and len(sinogram.shape) == 3:
+        # host stack: stream slabs through the device, overlapping copies
+        host = _host_tensor(sinogram)
+        if out is None:
+            res = torch.empty((ncol, nslice, ncol), dtype=torch.float32,
+                              pin_memory=True)
+        else:
+            res = out if isinstance(out, torch.Tensor) else \
+                torch.from_numpy(out)
+            if tuple(res.shape) != (ncol, nslice, ncol) or \
+                    res.dtype != torch.float32 or not res.is_contiguous():
+                raise ValueError("out must be a C-contiguous float32 array "
+                                 "of shape %s" % ((ncol, nslice, ncol),))
+        _fbp_streamed(host, center, angles, _mask_r2(ratio, center, ncol),
+                      _scale(nrow), ramp_win, filter_name, pad, pad_mode,
+                      apply_log, res, storage, kahan)
+        if out is not None:
+            return out
+        return res if isinstance(sinogram, torch.Tensor) else res.numpy()
     t, is_np = _to_device(sinogram)
     two_d = t.dim() == 2
     f = filter_sinograms(_as3(t), pad, pad_mode, apply_log, ramp_win,

@@ -56,6 +56,18 @@ int atb_version(void);
 const char *atb_last_error(void);
 
 /*
+ * Asynchronous strided copy of `height` rows of `width` bytes (pitches in
+ * bytes), kind 0 host->device, 1 device->host, 2 device->device; one
+ * cudaMemcpy2DAsync.  Used to stream slabs of slices of a host stack
+ * [nrow][nslice][ncol] through the device while the previous slab computes
+ * (the reference copies whole chunks synchronously at each kernel launch,
+ * reconstruction.py:476-481).
+ */
+int atb_copy_2d(void *dst, int64_t dst_pitch, const void *src,
+                int64_t src_pitch, int64_t width, int64_t height, int kind,
+                void *stream);
+
+/*
  * Smallest log2 of the FFT length the row filter uses for a detector width
  * `ncol` and pad `pad`: M = 2^log2m >= (ncol + 2 pad) + ncol - 1, so that the
  * circular convolution of length ncol + 2 pad is reproduced exactly on the
