@@ -59,9 +59,11 @@ _SIGS = {
     "atb_radon_adjoint": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
         ctypes.c_double, _vp, _c_i64, _c_i64, _vp]),
-    "atb_bp_batch_plan": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
+    "atb_bp_batch_plan": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int,
+                                         ctypes.c_int]),
     "atb_backproject_batch": (ctypes.c_int, [
-        _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
+        _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+        _vp]),
     "atb_backproject_batch_noalloc": (ctypes.c_int, [
         _vp, ctypes.c_int, ctypes.c_int, _vp]),
 }

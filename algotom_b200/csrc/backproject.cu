@@ -56,22 +56,28 @@
 
 namespace {
 
-constexpr int kThreads = 256;
 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 constexpr float kEdgeTol = 2e-3f;  // bins; FP32 error of q is < 3e-5
 
-// Tile geometry per slices-per-CTA S.  Warp tile = (8 PX) x (4 PY) pixels,
-// CTA = WX x WY warps (WX * WY = 8).
-template <int S> struct Geo;
-template <> struct Geo<1> {
-  static constexpr int PX = 4, PY = 4, WX = 2, WY = 4, kChunk = 32, kWin = 96;
+// Tile geometry per slices-per-CTA S and variant V.  Warp tile = (8 PX) x
+// (4 PY) pixels, CTA = WX x WY warps; kWin >= (TX-1)+(TY-1)/sqrt(2)... i.e.
+// the tile's largest footprint sqrt((TX-1)^2 + (TY-1)^2) plus 4 bins.
+// Variant 1 of the single-slice geometry is a 32 x 32 tile on 128 threads:
+// less shared memory and fewer registers, so more CTAs share an SM (small
+// images, uneven batches); the autotuner chooses between the variants.
+template <int S, int V = 0> struct Geo;
+template <> struct Geo<1, 0> {
+  static constexpr int PX = 4, PY = 4, WX = 2, WY = 4, kChunk = 32, kWin = 96, kThreads = 256, kMinBlocks = 2;
 };
-template <> struct Geo<2> {
-  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 32, kWin = 80;
+template <> struct Geo<1, 1> {
+  static constexpr int PX = 2, PY = 4, WX = 2, WY = 2, kChunk = 32, kWin = 48, kThreads = 128, kMinBlocks = 4;
 };
-template <> struct Geo<4> {
-  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 16, kWin = 80;
+template <> struct Geo<2, 0> {
+  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 32, kWin = 80, kThreads = 256, kMinBlocks = 2;
+};
+template <> struct Geo<4, 0> {
+  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 16, kWin = 80, kThreads = 256, kMinBlocks = 2;
 };
 
 struct BPArgs {
@@ -134,9 +140,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <typename T, int S>
+template <typename T, int S, int V = 0>
 struct BPCfg {
-  using G = Geo<S>;
+  using G = Geo<S, V>;
+  static constexpr int kThreads = G::kThreads, kMinBlocks = G::kMinBlocks;
   static constexpr int PX = G::PX, PY = G::PY, WX = G::WX;
   static constexpr int TX = 8 * PX * G::WX, TY = 4 * PY * G::WY;
   static constexpr int kChunk = G::kChunk, kWin = G::kWin, kHalf = kWin / 2;
@@ -150,9 +157,10 @@ struct BPCfg {
 
 // One CTA's work: the TX x TY pixel tile (bx, by) of the slice group bz.
 // Every thread of the CTA must call it (it synchronises).
-template <typename T, int S, bool kPerAngleKahan>
+template <typename T, int S, bool kPerAngleKahan, int V = 0>
 __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz, unsigned char *smem) {
-  using K = BPCfg<T, S>;
+  using K = BPCfg<T, S, V>;
+  constexpr int kThreads = K::kThreads;
   constexpr int PX = K::PX, PY = K::PY, TX = K::TX, TY = K::TY;
   constexpr int kChunk = K::kChunk, kWin = K::kWin, kHalf = K::kHalf, kRaw = K::kRaw;
   constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
@@ -489,20 +497,20 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   }
 }
 
-template <typename T, int S, bool kPerAngleKahan>
-__global__ void __launch_bounds__(kThreads, 2) bp_kernel(BPArgs a) {
+template <typename T, int S, bool kPerAngleKahan, int V>
+__global__ void __launch_bounds__(BPCfg<T, S, V>::kThreads, BPCfg<T, S, V>::kMinBlocks) bp_kernel(BPArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  bp_tile<T, S, kPerAngleKahan>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+  bp_tile<T, S, kPerAngleKahan, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem);
 }
 
 // Persistent back-projection of a batch of single-slice items of uneven
 // shapes: every CTA pulls work units (item, tile) from counter[0] until the
 // list is exhausted; the last CTA to leave resets counter[0] and counter[1]
 // to zero, so the next launch (or graph replay) starts from a clean state.
-template <typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+template <typename T, int V>
+__global__ void __launch_bounds__(BPCfg<T, 1, V>::kThreads, BPCfg<T, 1, V>::kMinBlocks)
     bp_batch_kernel(const atb_bp_item *items, const int *units, int nunits, int *counter) {
-  using K = BPCfg<T, 1>;
+  using K = BPCfg<T, 1, V>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int unit_s;
   for (;;) {
@@ -524,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     a.vec16 = sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(it.sino) % 16) == 0 &&
               it.sino_row_stride % 4 == 0 && it.ncol % 4 == 0;
     const int tiles_x = (it.ncol + K::TX - 1) / K::TX;
-    bp_tile<T, 1, false>(a, tile % tiles_x, tile / tiles_x, 0, smem);
+    bp_tile<T, 1, false, V>(a, tile % tiles_x, tile / tiles_x, 0, smem);
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -536,20 +544,21 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
-template <typename T, int S, bool kPerAngleKahan>
+template <typename T, int S, bool kPerAngleKahan, int V = 0>
 int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
-  using K = BPCfg<T, S>;
-  auto fn = bp_kernel<T, S, kPerAngleKahan>;
+  using K = BPCfg<T, S, V>;
+  auto fn = bp_kernel<T, S, kPerAngleKahan, V>;
   const int rc = atb::ensure_smem(fn, K::kSmem, "atb_backproject");
   if (rc != ATB_OK) return rc;
   dim3 grid((a.ncol + K::TX - 1) / K::TX, (a.ncol + K::TY - 1) / K::TY, (nslices + S - 1) / S);
-  fn<<<grid, kThreads, K::kSmem, st>>>(a);
+  fn<<<grid, K::kThreads, K::kSmem, st>>>(a);
   return atb::check_launch("atb_backproject");
 }
 
 template <typename T>
-int dispatch(BPArgs a, int per_angle_kahan, cudaStream_t st) {
+int dispatch(BPArgs a, int per_angle_kahan, int variant, cudaStream_t st) {
   if (per_angle_kahan) return launch_bp<T, 1, true>(a, a.nslice, st);
+  if (a.nslice == 1 && variant == 1) return launch_bp<T, 1, false, 1>(a, 1, st);
   // four slices per CTA for the bulk of a stack, then the remainder
   const int n4 = (a.nslice / 4) * 4;
   int rc = ATB_OK;
@@ -563,6 +572,7 @@ int dispatch(BPArgs a, int per_angle_kahan, cudaStream_t st) {
     if (rc != ATB_OK || rem == 2) return rc;
     a.slice_base = n4 + 2;
   }
+  if (variant == 1) return launch_bp<T, 1, false, 1>(a, 1, st);
   return launch_bp<T, 1, false>(a, 1, st);
 }
 
@@ -590,10 +600,12 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
             sino_slice_stride % 4 == 0 && ncol % 4 == 0;
   cudaStream_t st = atb::as_stream(stream);
   const int pak = flags & 1;
+  const int variant = (flags >> 2) & 3;
+  if (variant > 1) return atb::fail(ATB_EINVAL, "atb_backproject: unknown tile variant %d", variant);
   switch (sino_dtype) {
-    case ATB_F32: return dispatch<float>(a, pak, st);
-    case ATB_F16: return dispatch<__half>(a, pak, st);
-    case ATB_BF16: return dispatch<__nv_bfloat16>(a, pak, st);
+    case ATB_F32: return dispatch<float>(a, pak, variant, st);
+    case ATB_F16: return dispatch<__half>(a, pak, variant, st);
+    case ATB_BF16: return dispatch<__nv_bfloat16>(a, pak, variant, st);
     default: return atb::fail(ATB_EINVAL, "atb_backproject: unknown sino_dtype %d", sino_dtype);
   }
 }
@@ -608,18 +620,22 @@ int sm_count() {
   cache[dev] = n;
   return n;
 }
-constexpr int kBatchTile = 64;  // tile edge of the single-slice geometry
+constexpr int kBatchTile = 64;  // tile edge of single-slice variant 0
+inline int batch_tile(int variant) { return variant == 1 ? 32 : 64; }
 }  // namespace
 
-extern "C" int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units, int capacity) {
+extern "C" int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units, int capacity, int variant) {
   if (!items || nitems < 1) return atb::fail(ATB_EINVAL, "atb_bp_batch_plan: no items");
   if (nitems > 65536) return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: nitems=%d > 65536", nitems);
+  if (variant < 0 || variant > 1) return atb::fail(ATB_EINVAL, "atb_bp_batch_plan: unknown tile variant %d", variant);
+  const int tile = batch_tile(variant);
   long long total = 0;
   for (int b = 0; b < nitems; ++b) {
     const atb_bp_item &it = items[b];
     if (it.nrow < 1 || it.ncol < 1) return atb::fail(ATB_EINVAL, "atb_bp_batch_plan: item %d bad shape", b);
-    const long long t = (long long)((it.ncol + kBatchTile - 1) / kBatchTile) * ((it.ncol + kBatchTile - 1) / kBatchTile);
-    if (t > 65536) return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: item %d has ncol=%d > 16384", b, it.ncol);
+    const long long t = (long long)((it.ncol + tile - 1) / tile) * ((it.ncol + tile - 1) / tile);
+    if (t > 65536)
+      return atb::fail(ATB_ERANGE, "atb_bp_batch_plan: item %d has ncol=%d > %d", b, it.ncol, 256 * tile);
     total += t;
   }
   if (!units) return (int)total;  // size query
@@ -637,26 +653,40 @@ extern "C" int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *unit
   int n = 0;
   for (int q = 0; q < nitems; ++q) {
     const int b = order[q];
-    const int tx = (items[b].ncol + kBatchTile - 1) / kBatchTile;
+    const int tx = (items[b].ncol + tile - 1) / tile;
     for (int t = 0; t < tx * tx; ++t) units[n++] = (int)(((unsigned)b << 16) | (unsigned)t);
   }
   delete[] order;
   return n;
 }
 
-extern "C" int atb_backproject_batch(const atb_bp_item *items, int nitems, const int *units, int nunits,
-                                     int *counter, int max_ctas, void *stream) {
-  if (!items || !units || !counter) return atb::fail(ATB_EINVAL, "atb_backproject_batch: null pointer");
-  if (nitems < 1 || nunits < 1) return atb::fail(ATB_EINVAL, "atb_backproject_batch: empty batch");
-  using K = BPCfg<float, 1>;
-  static_assert(K::TX == kBatchTile && K::TY == kBatchTile, "batch tiles are square");
-  const int rc = atb::ensure_smem(bp_batch_kernel<float>, K::kSmem, "atb_backproject_batch");
+namespace {
+template <int V>
+int launch_batch(const atb_bp_item *items, int nitems, const int *units, int nunits, int *counter, int max_ctas,
+                 cudaStream_t st) {
+  using K = BPCfg<float, 1, V>;
+  const int rc = atb::ensure_smem(bp_batch_kernel<float, V>, K::kSmem, "atb_backproject_batch");
   if (rc != ATB_OK) return rc;
-  int grid = 2 * sm_count();
+  int grid = K::kMinBlocks * sm_count();
   if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
   if (grid > nunits) grid = nunits;
-  bp_batch_kernel<float><<<grid, kThreads, K::kSmem, atb::as_stream(stream)>>>(items, units, nunits, counter);
+  bp_batch_kernel<float, V><<<grid, K::kThreads, K::kSmem, st>>>(items, units, nunits, counter);
   return atb::check_launch("atb_backproject_batch");
+}
+}  // namespace
+
+extern "C" int atb_backproject_batch(const atb_bp_item *items, int nitems, const int *units, int nunits,
+                                     int *counter, int max_ctas, int variant, void *stream) {
+  if (!items || !units || !counter) return atb::fail(ATB_EINVAL, "atb_backproject_batch: null pointer");
+  if (nitems < 1 || nunits < 1) return atb::fail(ATB_EINVAL, "atb_backproject_batch: empty batch");
+  static_assert(BPCfg<float, 1, 0>::TX == kBatchTile && BPCfg<float, 1, 0>::TY == kBatchTile, "square tiles");
+  static_assert(BPCfg<float, 1, 1>::TX == 32 && BPCfg<float, 1, 1>::TY == 32, "square tiles");
+  cudaStream_t st = atb::as_stream(stream);
+  switch (variant) {
+    case 0: return launch_batch<0>(items, nitems, units, nunits, counter, max_ctas, st);
+    case 1: return launch_batch<1>(items, nitems, units, nunits, counter, max_ctas, st);
+    default: return atb::fail(ATB_EINVAL, "atb_backproject_batch: unknown tile variant %d", variant);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -762,12 +792,12 @@ extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitem
       (e = cudaMemcpyAsync(units_dev, g_noalloc_units, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st)) !=
           cudaSuccess)
     return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: %s", cudaGetErrorString(e));
-  using K = BPCfg<float, 1>;
-  const int rc = atb::ensure_smem(bp_batch_kernel<float>, K::kSmem, "atb_backproject_batch_noalloc");
+  using K = BPCfg<float, 1, 0>;
+  const int rc = atb::ensure_smem(bp_batch_kernel<float, 0>, K::kSmem, "atb_backproject_batch_noalloc");
   if (rc != ATB_OK) return rc;
   int grid = 2 * sm_count();
   if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
   if (grid > n) grid = n;
-  bp_batch_kernel<float><<<grid, kThreads, K::kSmem, st>>>(items_dev, units_dev, n, counter);
+  bp_batch_kernel<float, 0><<<grid, K::kThreads, K::kSmem, st>>>(items_dev, units_dev, n, counter);
   return atb::check_launch("atb_backproject_batch_noalloc");
 }

@@ -34,7 +34,7 @@ class BatchedFBP:
     """
 
     def __init__(self, shapes, centers, angles, filter_name="hann", pad=None,
-                 pad_mode="edge", ratio=1.0, device=None):
+                 pad_mode="edge", ratio=1.0, device=None, variant=None):
         self.dev = torch.device(device) if device is not None else R._device()
         self.n = len(shapes)
         if not (len(centers) == len(angles) == self.n) or self.n == 0:
@@ -81,20 +81,35 @@ class BatchedFBP:
             it.scale = R._scale(nrow)
             it.nrow, it.ncol, it.edge_pad = nrow, ncol, 0
         self.items_host = items
-        nunits = nat.call("atb_bp_batch_plan", ctypes.addressof(items),
-                          self.n, None, 0)
-        units = (ctypes.c_int * nunits)()
-        nat.call("atb_bp_batch_plan", ctypes.addressof(items), self.n,
-                 ctypes.addressof(units), nunits)
-        self.nunits = nunits
         raw = bytes(items)
         self.items_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8
                                           ).to(self.dev)
-        self.units_dev = torch.frombuffer(bytearray(bytes(units)),
-                                          dtype=torch.int32).to(self.dev)
         self.counter = torch.zeros(2, dtype=torch.int32, device=self.dev)
         self.graph = None
         self.updates = int(sum(r * c * c for r, c in shapes))
+        self.shapes = [(int(r), int(c)) for r, c in shapes]
+        self._units = {}
+        if variant is None:
+            from .autotune import tuned_batch_variant
+            variant = tuned_batch_variant(self)
+        self.set_variant(variant)
+
+    def set_variant(self, variant):
+        """Select the tile variant (0: 64 x 64, 1: 32 x 32) and its plan."""
+        variant = int(variant)
+        if variant not in self._units:
+            nunits = nat.call("atb_bp_batch_plan",
+                              ctypes.addressof(self.items_host), self.n, None,
+                              0, variant)
+            units = (ctypes.c_int * nunits)()
+            nat.call("atb_bp_batch_plan", ctypes.addressof(self.items_host),
+                     self.n, ctypes.addressof(units), nunits, variant)
+            self._units[variant] = (
+                nunits, torch.frombuffer(bytearray(bytes(units)),
+                                         dtype=torch.int32).to(self.dev))
+        self.variant = variant
+        self.nunits, self.units_dev = self._units[variant]
+        self.graph = None
 
     def launch(self, max_ctas=0):
         """Filter every item, then one persistent back-projection launch."""
@@ -109,7 +124,7 @@ class BatchedFBP:
                      st)
         nat.call("atb_backproject_batch", self.items_dev.data_ptr(), self.n,
                  self.units_dev.data_ptr(), self.nunits,
-                 self.counter.data_ptr(), int(max_ctas), st)
+                 self.counter.data_ptr(), int(max_ctas), self.variant, st)
 
     def capture(self):
         """Capture :meth:`launch` into a CUDA graph (after one warm launch)."""

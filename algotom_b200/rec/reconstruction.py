@@ -135,12 +135,13 @@ def filter_sinograms(sino3, pad, pad_mode="edge", apply_log=False,
 
 
 def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
-                scale=1.0, out=None, kahan="chunk", trig=None):
+                scale=1.0, out=None, kahan="chunk", trig=None, variant=0):
     """Device back-projection of [nrow, nslice, ncol] -> [ncol, nslice, ncol].
 
     ``sino3`` may be float32, float16 or bfloat16 (last axis contiguous).
     ``trig`` may hold the angle table from :func:`_trig` already on the
-    device (saves its host-to-device copy per call).
+    device (saves its host-to-device copy per call).  ``variant`` selects
+    the single-slice tile variant (0: 64 x 64, 1: 32 x 32).
     """
     nrow, nslice, ncol = sino3.shape
     dev = sino3.device
@@ -155,8 +156,22 @@ def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
              sino3.stride(1), nrow, nslice, ncol, trig.data_ptr(),
              float(np.float32(center)), int(bool(edge_pad)), float(mask_r2),
              float(scale), out.data_ptr(), out.stride(0), out.stride(1),
-             1 if kahan == "angle" else 0, _stream_ptr(dev))
+             (1 if kahan == "angle" else 0) | (int(variant) << 2),
+             _stream_ptr(dev))
     return out
+
+
+def _backproject_tuned(f, angles, center, **kw):
+    """Back-projection of a single slice with the autotuned tile variant."""
+    from .autotune import tuned_single_variant
+    nrow, nslice, ncol = f.shape
+    if nslice != 1 or kw.get("kahan") == "angle":
+        return backproject(f, angles, center, **kw)
+    trig = _trig(angles, f.device)
+    out = torch.empty((ncol, 1, ncol), dtype=torch.float32, device=f.device)
+    v = tuned_single_variant(ncol, nrow, lambda var: backproject(
+        f, angles, center, out=out, trig=trig, variant=var, **kw))
+    return backproject(f, angles, center, out=out, trig=trig, variant=v, **kw)
 
 
 def _neg_log(sino3):
@@ -395,9 +410,9 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
     f = filter_sinograms(_as3(t), pad, pad_mode, apply_log, ramp_win,
                          filter_name, storage)
     del t
-    rec = backproject(f, angles, center, edge_pad=False,
-                      mask_r2=_mask_r2(ratio, center, ncol),
-                      scale=_scale(nrow), kahan=kahan)
+    rec = _backproject_tuned(f, angles, center, edge_pad=False,
+                             mask_r2=_mask_r2(ratio, center, ncol),
+                             scale=_scale(nrow), kahan=kahan)
     del f
     return _finish(rec, two_d, is_np, out)
 

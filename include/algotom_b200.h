@@ -135,7 +135,10 @@ int atb_neg_log(const float *src, int64_t src_row_stride,
  *            p = 0, -s[ncol-1] at p = ncol-1) smoothed over one bin; this
  *            is the derivative of the back-projection with respect to the
  *            centre (no counterpart in the reference; used by the autograd
- *            path; edge_pad must be 0)
+ *            path; edge_pad must be 0);
+ *            bits 2-3: tile variant for single-slice launches: 0 = 64 x 64
+ *            pixels on 256 threads, 1 = 32 x 32 on 128 threads (chosen by the
+ *            autotuner; stacks of 2 or more slices always use 64 x 32 tiles)
  */
 int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int64_t sino_slice_stride, int nrow, int nslice, int ncol,
@@ -183,15 +186,17 @@ typedef struct {
 
 /*
  * Host-side work list of a batch for atb_backproject_batch: one entry per
- * (item, 64 x 64 pixel tile), item index << 16 | tile, items ordered by
- * angle count, largest first (longest-processing-time order).  With
- * units == NULL returns the number of entries; otherwise fills up to
- * `capacity` and returns the count.  ncol <= 16384, nitems <= 65536.
- * No counterpart in the reference, which loops over slices on the host
+ * (item, pixel tile), item index << 16 | tile, items ordered by angle
+ * count, largest first (longest-processing-time order).  Tiles are
+ * 64 x 64 pixels for variant 0 and 32 x 32 for variant 1 (as the flags of
+ * atb_backproject); at most 65536 tiles per item (ncol <= 16384 or 8192)
+ * and 65536 items.  With units == NULL returns the number of entries;
+ * otherwise fills up to `capacity` and returns the count.  No counterpart in
+ * the reference, which loops over slices on the host
  * (reconstruction.py:482-487).
  */
 int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units,
-                      int capacity);
+                      int capacity, int variant);
 
 /*
  * Back-projection of a batch of single-slice sinograms of uneven width,
@@ -204,13 +209,15 @@ int atb_bp_batch_plan(const atb_bp_item *items, int nitems, int *units,
  *   units    device array [nunits] from atb_bp_batch_plan
  *   counter  device scratch, two int32, zero before the first call; the
  *            kernel returns it to zero, so a CUDA graph can replay the launch
- *   max_ctas 0: two CTAs per SM; otherwise at most this many CTAs
+ *   max_ctas 0: as many CTAs as fit (2 per SM for variant 0, 4 for
+ *            variant 1); otherwise at most this many CTAs
+ *   variant  tile variant the units were planned for (0 or 1)
  *
  * Calls that share `counter` must not overlap on the device.
  */
 int atb_backproject_batch(const atb_bp_item *items, int nitems,
                           const int *units, int nunits, int *counter,
-                          int max_ctas, void *stream);
+                          int max_ctas, int variant, void *stream);
 
 /*
  * atb_backproject_batch for callers that cannot allocate device memory.

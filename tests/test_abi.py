@@ -83,17 +83,21 @@ def test_batch_plan_orders_by_cost():
     items = (nat.BpItem * 3)()
     for it, (nrow, ncol) in zip(items, [(100, 64), (300, 130), (200, 65)]):
         it.nrow, it.ncol = nrow, ncol
-    n = nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3, None, 0)
+    n = nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3, None, 0, 0)
     assert n == 1 + 9 + 4
     units = (ctypes.c_int * n)()
     assert nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3,
-                    ctypes.addressof(units), n) == n
+                    ctypes.addressof(units), n, 0) == n
     got = [(u >> 16, u & 0xffff) for u in units]
     assert got == [(1, t) for t in range(9)] + [(2, t) for t in range(4)] + \
         [(0, 0)]
+    # 32 x 32 tiles for variant 1
+    assert nat.call("atb_bp_batch_plan", ctypes.addressof(items), 3, None, 0,
+                    1) == 4 + 25 + 9
     lib = nat.load()
     assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3,
-                                 ctypes.addressof(units), 5) == -3
+                                 ctypes.addressof(units), 5, 0) == -3
+    assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3, None, 0, 2) == -1
     items[0].ncol = 20000
-    assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3, None, 0) == -3
+    assert lib.atb_bp_batch_plan(ctypes.addressof(items), 3, None, 0, 0) == -3
     assert "16384" in nat.last_error()

@@ -79,3 +79,25 @@ def test_uneven_geometry_is_seeded():
     assert len(g1) == 64
     assert all(361 <= d["nrow"] <= 3601 for d in g1)
     assert sum(d["half_acquisition"] for d in g1) == 8
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_batch_tile_variants(cuda, variant):
+    sinos, angs, shapes, cens = _small_batch()
+    bf = B.BatchedFBP(shapes, cens, angs, variant=variant)
+    outs = [o.cpu().numpy() for o in bf([torch.from_numpy(s) for s in sinos])]
+    for s, a, c, o in zip(sinos, angs, cens, outs):
+        ref = O.fbp_reconstruction(s, c, angles=a, apply_log=False)
+        assert O.rel_l2(o, ref) < 1e-5
+
+
+def test_batch_autotuned(cuda, tmp_path, monkeypatch):
+    monkeypatch.setenv("ALGOTOM_B200_AUTOTUNE_CACHE", str(tmp_path / "t.json"))
+    sinos, angs, shapes, cens = _small_batch()
+    bf = B.BatchedFBP(shapes, cens, angs)
+    assert bf.variant in (0, 1)
+    assert (tmp_path / "t.json").exists()
+    outs = [o.cpu().numpy() for o in bf([torch.from_numpy(s) for s in sinos])]
+    for s, a, c, o in zip(sinos, angs, cens, outs):
+        assert O.rel_l2(o, O.fbp_reconstruction(s, c, angles=a,
+                                                apply_log=False)) < 1e-5

@@ -300,3 +300,13 @@ def test_host_stack_streamed_in_slabs(cuda):
         ref = O.fbp_reconstruction(s3[:, k], 47.3, angles=ang, apply_log=False)
         assert O.rel_l2(got[:, k], ref) < TOL
     del rng
+
+
+@pytest.mark.parametrize("ncol,cen", [(33, 16.0), (257, 130.2), (1000, 499.5)])
+def test_single_slice_tile_variant_1(cuda, ncol, cen):
+    s, ang, _ = phantom.ellipse_sinogram(ncol, 121, ncol, cen)
+    t = torch.from_numpy(s).cuda()[:, None]
+    ref = O.back_projection(s, ang, cen)
+    for v in (0, 1):
+        got = R.backproject(t, ang, cen, variant=v)[:, 0].cpu().numpy()
+        assert O.rel_l2(got, ref) < 1e-6

@@ -125,3 +125,33 @@ def test_dropin_mask_and_scale_helpers():
     # ratio 0: largest disc inside the centred field
     assert R._mask_r2(0.0, 7.0, 20) == pytest.approx((0.7 * 10) ** 2)
     assert R._scale(181) == pytest.approx(np.pi / 180, rel=1e-7)
+
+
+def test_autotuner_picks_fastest_and_caches(tmp_path):
+    from algotom_b200.rec import autotune as AT
+    path = tmp_path / "tune.json"
+    t = AT.Autotuner(str(path))
+    calls = []
+
+    def run(v):
+        calls.append(v)
+        return {0: 2.0, 1: 1.0}[v]
+    key = AT.Autotuner.key("single", "gpu", ncol=1000, nrow=900)
+    assert key == AT.Autotuner.key("single", "gpu", ncol=1024, nrow=1000)
+    assert t.choose(key, (0, 1), run) == 1
+    assert calls == [0, 1]
+    assert t.choose(key, (0, 1), run) == 1 and calls == [0, 1]  # cached
+    t2 = AT.Autotuner(str(path))  # persisted
+    assert t2.choose(key, (0, 1), lambda v: 1 / 0) == 1
+
+
+def test_autotuner_survives_corrupt_cache(tmp_path):
+    from algotom_b200.rec import autotune as AT
+    path = tmp_path / "tune.json"
+    path.write_text("{not json")
+    with pytest.warns(UserWarning, match="unreadable"):
+        t = AT.Autotuner(str(path))
+    assert t.table == {}
+    assert t.choose("k", (0, 1), lambda v: [3.0, 1.0][v]) == 1
+    import json
+    assert json.loads(path.read_text())["k"]["choice"] == 1
