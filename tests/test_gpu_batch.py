@@ -26,7 +26,8 @@ def _small_batch():
     return sinos, angs, shapes, cens
 
 
-def test_batch_matches_single_slice_and_oracle(cuda):
+def test_batch_matches_single_slice_and_oracle(cuda, monkeypatch):
+    monkeypatch.setenv("ALGOTOM_B200_AUTOTUNE", "0")  # variant 0 both ways
     sinos, angs, shapes, cens = _small_batch()
     bf = B.BatchedFBP(shapes, cens, angs)
     outs = [o.cpu().numpy() for o in bf([torch.from_numpy(s) for s in sinos])]
