@@ -433,32 +433,66 @@ def apply_circular_ramp_filter(rec_img, ramp_win=None, filter_name=None,
     return r.cpu().numpy().astype(np.float64) if is_np else r
 
 
-def _circular_filter(stack, ramp_win, filter_name, pad, pad_mode):
-    """[nslice, ncol, ncol] float32 -> filtered, same shape (library 2-D FFT)."""
-    nslice, ncol, _ = stack.shape
-    n = ncol + 2 * pad
+_circ_cache = {}
+
+
+def _circular_spectrum(ramp_win, filter_name, n, device):
+    """Half spectrum [n, n//2+1] for irfft2 of the 2-D circular window.
+
+    The reference keeps ``real(ifft2(fft2(x) * ifftshift(W2)))``; for a real
+    image only the Hermitian part ``(H[k] + conj(H[-k])) / 2`` of
+    ``H = ifftshift(W2)`` reaches the real part, so the product can be taken
+    on the real-to-complex half spectrum.
+    """
+    key = None
     if ramp_win is None or np.shape(ramp_win) != (n, n):
+        key = (filter_name, n, device)
+        hit = _circ_cache.get(key)
+        if hit is not None:
+            return hit
         ramp_win = make_circular_ramp_window(n, filter_name)
     h = np.fft.ifftshift(np.asarray(ramp_win.cpu() if isinstance(
-        ramp_win, torch.Tensor) else ramp_win))
-    ht = torch.from_numpy(np.ascontiguousarray(h)).to(stack.device,
-                                                      torch.complex64)
+        ramp_win, torch.Tensor) else ramp_win, dtype=np.complex128))
+    hm = np.roll(np.flip(h, axis=(0, 1)), 1, axis=(0, 1))  # H[-k1, -k2]
+    hh = 0.5 * (h + np.conj(hm))
+    t = torch.from_numpy(np.ascontiguousarray(hh[:, :n // 2 + 1])).to(
+        device, torch.complex64)
+    if key is not None:
+        if len(_circ_cache) > 8:
+            _circ_cache.clear()
+        _circ_cache[key] = t
+    return t
+
+
+def _circular_filter(stack, ramp_win, filter_name, pad, pad_mode, slab=16):
+    """[nslice, ncol, ncol] float32 -> filtered, same shape.
+
+    2-D circular ramp filter of ``reconstruction.py:527-560`` on the device,
+    a slab of slices at a time through the library real-to-complex FFT
+    (cuFFT via torch): pad (numpy mode), rfft2, product with the Hermitian
+    half window, irfft2, crop.
+    """
+    nslice, ncol, _ = stack.shape
+    n = ncol + 2 * pad
+    hh = _circular_spectrum(ramp_win, filter_name, n, stack.device)
     mode = {"edge": "replicate", "reflect": "reflect", "wrap": "circular",
             "constant": "constant"}.get(pad_mode)
     out = torch.empty_like(stack)
-    for k in range(nslice):
-        x = stack[k]
+    for k0 in range(0, nslice, slab):
+        x = stack[k0:k0 + slab]
         if pad > 0:
-            if mode is None:
-                xp = torch.from_numpy(np.pad(x.cpu().numpy(), pad,
+            if mode is None or (mode == "reflect" and pad >= ncol):
+                xp = torch.from_numpy(np.pad(x.cpu().numpy(), ((0, 0),
+                                                               (pad, pad),
+                                                               (pad, pad)),
                                              mode=pad_mode)).to(stack.device)
             else:
-                xp = torch.nn.functional.pad(x[None, None], (pad,) * 4,
-                                             mode=mode)[0, 0]
+                xp = torch.nn.functional.pad(x[:, None], (pad,) * 4,
+                                             mode=mode)[:, 0]
         else:
             xp = x
-        y = torch.fft.ifft2(torch.fft.fft2(xp.to(torch.float32)) * ht).real
-        out[k] = y[pad:pad + ncol, pad:pad + ncol]
+        y = torch.fft.irfft2(torch.fft.rfft2(xp) * hh, s=(n, n))
+        out[k0:k0 + slab] = y[:, pad:pad + ncol, pad:pad + ncol]
     return out
 
 

@@ -55,8 +55,9 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
     ap.add_argument("--workload", default="stack",
-                    choices=["stack", "batch", "single"],
-                    help="stack: the 256-slice benchmark (default); batch: "
+                    choices=["stack", "batch", "single", "bpf"],
+                    help="stack: the 256-slice benchmark (default); bpf: the "
+                         "same data through bpf_reconstruction; batch: "
                          "64 uneven sinograms in one persistent launch under "
                          "a CUDA graph; single: one 1024^2 x 900 slice")
     return ap.parse_args()
@@ -464,8 +465,58 @@ def run_single(args):
         flush=True)
 
 
+def run_bpf(args):
+    """The stacked benchmark data through bpf_reconstruction (device)."""
+    import torch
+    from algotom_b200.rec import reconstruction as R
+    dev = torch.device("cuda", 0)
+    nslice = args.slices
+    sino, ang = make_sinograms(nslice, dev)
+    torch.cuda.synchronize()
+
+    def step():
+        return R.bpf_reconstruction(sino, CENTER, angles=ang, ratio=1.0,
+                                    filter_name="hann", apply_log=False)
+    for _ in range(args.warmup):
+        r = step()
+        del r
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), \
+        torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        r = step()
+        del r
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    err = None
+    if not args.no_oracle:
+        from oracle import cpu_port
+        from oracle import fbp_oracle as O
+        s0 = sino[:, 0, :].cpu().numpy()
+        bp = cpu_port.back_projection(s0, ang, CENTER, edge_pad=True,
+                                      ref_arith=False)
+        ref = O.apply_circular_ramp_filter(bp, None, "hann", 150, "edge")
+        ref = ref * O.make_circle_mask(NCOL, 1.0) * (np.pi / (NROW - 1))
+        got = step()[:, 0, :].cpu().numpy()
+        err = {"rel_l2": O.rel_l2(got, ref), "slices_checked": 1}
+    upd = nslice * NCOL * NCOL * NROW
+    print(json.dumps({
+        "metric": "BPF pixel-angle updates/s at 2560 det",
+        "value": upd / t, "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "stacked BPF: %d slices x 1801 angles x 2560 "
+                               "det, 2-D circular filter on 2860^2" % nslice},
+        "slices_per_s": nslice / t, "accuracy": err}), flush=True)
+
+
 def main():
     args = _args()
+    if args.workload == "bpf":
+        run_bpf(args)
+        return
     if args.workload == "batch":
         run_batch(args)
         return
