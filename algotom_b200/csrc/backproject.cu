@@ -147,11 +147,12 @@ struct BPCfg {
   static constexpr int PX = G::PX, PY = G::PY, WX = G::WX;
   static constexpr int TX = 8 * PX * G::WX, TY = 4 * PY * G::WY;
   static constexpr int kChunk = G::kChunk, kWin = G::kWin, kHalf = kWin / 2;
-  static constexpr int kRaw = ((kWin + 1 + 3 + 3) / 4) * 4;  // raw floats per window, 4-aligned start
-  static constexpr bool kAsync = sizeof(T) == 4;
+  // raw window: elements of T from a start rounded down to a 16-byte vector
+  static constexpr int kVecElems = 16 / (int)sizeof(T);
+  static constexpr int kRaw = ((kWin + 1 + (kVecElems - 1) + (kVecElems - 1)) / kVecElems) * kVecElems;
   static constexpr int kPairBytes = 8 * S;  // per bin: S (a, D) pairs
   static constexpr size_t kPairsSmem = (size_t)kChunk * kWin * kPairBytes;
-  static constexpr size_t kRawSmem = kAsync ? 2 * (size_t)kChunk * S * kRaw * 4 : 0;
+  static constexpr size_t kRawSmem = 2 * (size_t)kChunk * S * kRaw * sizeof(T);
   static constexpr size_t kSmem = kPairsSmem + kRawSmem;
 };
 
@@ -166,7 +167,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
 
   unsigned char *pairs = smem;  // S == 1: [kChunk][kWin] float2; else [kChunk][S/2][kWin] float4
-  float *raw = reinterpret_cast<float *>(smem + K::kPairsSmem);  // [2][kChunk][S][kRaw]
+  T *raw = reinterpret_cast<T *>(smem + K::kPairsSmem);  // [2][kChunk][S][kRaw]
   __shared__ AngleParam prm[2][kChunk];
   __shared__ int lo_s[2][kChunk];
   __shared__ int flag_s[2][kChunk];  // bit 0: skip angle, bit 1: checked path
@@ -253,35 +254,42 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   const long long srs = a.srs, sss = a.sss;
   const bool edge_pad = a.edge_pad, slope = a.slope, vec16 = a.vec16;
 
-  // raw windows (and, for edge padding, the two edge samples) of chunk k
-  // into raw[buf]; float32 storage only.  Elements outside the detector row
-  // are never copied.
+  // raw windows (and, for edge padding or slope mode, the two edge samples)
+  // of chunk k into raw[buf], from a start rounded down to a 16-byte vector.
+  // Aligned rows stream in with 16-byte cp.async; float32 rows that are not
+  // 16-byte aligned use 4-byte cp.async, 16-bit ones plain loads.  Elements
+  // outside the detector row are never read.
   auto issue_raw = [&](int k, int buf) {
-    if constexpr (K::kAsync) {
-      const int i = k * kChunk + s_ai;
-      if (i < a.nrow && !(flag_s[buf][s_ai] & 1)) {
-        const int base = (lo_s[buf][s_ai] >> 2) << 2;
-        const float *src = reinterpret_cast<const float *>(sino) + i * srs;
-        float *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
-        if (vec16) {
-          constexpr int kVec = kRaw / 4;
-          for (int idx = s_jl; idx < S * kVec; idx += kTPA) {
-            const int ks = idx / kVec, v = idx - ks * kVec;
-            const int d = base + 4 * v;
-            if (ks < nsl && d >= 0 && d < ncol)  // ncol % 4 == 0: a vector is in or out
-              cp_async16(rb + ks * kRaw + 4 * v, src + ks * sss + d);
-          }
-        } else {
-          for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
-            const int ks = idx / kRaw, v = idx - ks * kRaw;
-            const int d = base + v;
-            if (ks < nsl && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
-          }
+    constexpr int kV = K::kVecElems;
+    const int i = k * kChunk + s_ai;
+    if (i < a.nrow && !(flag_s[buf][s_ai] & 1)) {
+      const int base = (lo_s[buf][s_ai] / kV - (lo_s[buf][s_ai] % kV < 0)) * kV;  // floor to a vector
+      const T *src = sino + i * srs;
+      T *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
+      if (vec16) {
+        constexpr int kVec = kRaw / kV;
+        for (int idx = s_jl; idx < S * kVec; idx += kTPA) {
+          const int ks = idx / kVec, v = idx - ks * kVec;
+          const int d = base + kV * v;
+          if (ks < nsl && d >= 0 && d < ncol)  // ncol % kV == 0: a vector is in or out
+            cp_async16(rb + ks * kRaw + kV * v, src + ks * sss + d);
         }
-        if ((edge_pad || slope) && s_jl < nsl) {
-          cp_async4(&edge_s[buf][s_ai][s_jl][0], src + s_jl * sss);
-          cp_async4(&edge_s[buf][s_ai][s_jl][1], src + s_jl * sss + ncol1);
+      } else if constexpr (sizeof(T) == 4) {
+        for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
+          const int ks = idx / kRaw, v = idx - ks * kRaw;
+          const int d = base + v;
+          if (ks < nsl && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
         }
+      } else {
+        for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
+          const int ks = idx / kRaw, v = idx - ks * kRaw;
+          const int d = base + v;
+          if (ks < nsl && d >= 0 && d < ncol) rb[ks * kRaw + v] = src[ks * sss + d];
+        }
+      }
+      if ((edge_pad || slope) && s_jl < nsl) {
+        edge_s[buf][s_ai][s_jl][0] = atb::load_as_float(src + s_jl * sss);
+        edge_s[buf][s_ai][s_jl][1] = atb::load_as_float(src + s_jl * sss + ncol1);
       }
     }
     cp_async_commit();
@@ -293,21 +301,17 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     const int i = k * kChunk + s_ai;
     if (i >= a.nrow || (flag_s[buf][s_ai] & 1)) return;
     const int lo = lo_s[buf][s_ai];
-    const int base = (lo >> 2) << 2;
+    constexpr int kV = K::kVecElems;
+    const int base = (lo / kV - (lo % kV < 0)) * kV;
     // every d and d+1 of the window inside [0, ncol-1] with d <= ncol-2
     // (slope mode: also clear of the smoothed edges at bins 0 and ncol-2)
     const bool interior = slope ? (lo >= 1 && lo + kWin <= ncol1 - 1) : (lo >= 0 && lo + kWin <= ncol1);
-    const float *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
-    const T *row = sino + i * srs;
+    const T *rb = raw + ((size_t)buf * kChunk + s_ai) * S * kRaw;
     // detector sample x (0 <= x <= ncol-1) of slice ks
     auto val = [&](int ks, int x) -> float {
-      if constexpr (K::kAsync) {
-        const int r = x - base;
-        if (r >= 0 && r < kRaw) return rb[ks * kRaw + r];
-        return edge_s[buf][s_ai][ks][x == 0 ? 0 : 1];  // clamped edge sample
-      } else {
-        return atb::load_as_float(row + ks * sss + x);
-      }
+      const int r = x - base;
+      if (r >= 0 && r < kRaw) return atb::to_float(rb[ks * kRaw + r]);
+      return edge_s[buf][s_ai][ks][x == 0 ? 0 : 1];  // clamped edge sample
     };
 #pragma unroll 2
     for (int t = 0; t < kJPT; ++t) {
@@ -320,13 +324,8 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
         float v = 0.f, w = 0.f;
         if (ks < nsl) {
           if (interior) {
-            if constexpr (K::kAsync) {
-              v = rb[ks * kRaw + d - base];
-              w = rb[ks * kRaw + d + 1 - base] - v;
-            } else {
-              v = atb::load_as_float(row + ks * sss + d);
-              w = atb::load_as_float(row + ks * sss + d + 1) - v;
-            }
+            v = atb::to_float(rb[ks * kRaw + d - base]);
+            w = atb::to_float(rb[ks * kRaw + d + 1 - base]) - v;
           } else if (slope) {
             // derivative in p of the back-projected interpolant with its two
             // edge steps (+s[0] at p = 0, -s[ncol-1] at p = ncol-1) smoothed
@@ -596,8 +595,11 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
   a.center = center; a.edge_pad = edge_pad ? 1 : 0; a.mask_r2 = mask_r2; a.scale = scale;
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride;
   a.slope = (flags >> 1) & 1;
-  a.vec16 = sino_dtype == ATB_F32 && (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % 4 == 0 &&
-            sino_slice_stride % 4 == 0 && ncol % 4 == 0;
+  {
+    const int ve = sino_dtype == ATB_F32 ? 4 : 8;  // elements per 16-byte vector
+    a.vec16 = (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % ve == 0 &&
+              sino_slice_stride % ve == 0 && ncol % ve == 0;
+  }
   cudaStream_t st = atb::as_stream(stream);
   const int pak = flags & 1;
   const int variant = (flags >> 2) & 3;

@@ -35,6 +35,10 @@ __device__ __forceinline__ float load_as_float(const __nv_bfloat16 *p) {
   return __bfloat162float(__ldg(p));
 }
 
+__device__ __forceinline__ float to_float(float v) { return v; }
+__device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+
 __device__ __forceinline__ void store_from_float(float *p, float v) { *p = v; }
 __device__ __forceinline__ void store_from_float(__half *p, float v) { *p = __float2half_rn(v); }
 __device__ __forceinline__ void store_from_float(__nv_bfloat16 *p, float v) {
