@@ -150,7 +150,10 @@ struct BPCfg {
   // raw window: elements of T from a start rounded down to a 16-byte vector
   static constexpr int kVecElems = 16 / (int)sizeof(T);
   static constexpr int kRaw = ((kWin + 1 + (kVecElems - 1) + (kVecElems - 1)) / kVecElems) * kVecElems;
-  static constexpr int kPairBytes = 8 * S;  // per bin: S (a, D) pairs
+  // 16-bit storage with S >= 2 keeps 16-bit (value, difference) pairs in
+  // shared memory: 4 bytes per bin and slice instead of 8
+  static constexpr bool kHalfPairs = sizeof(T) == 2 && S >= 2;
+  static constexpr int kPairBytes = (kHalfPairs ? 4 : 8) * S;  // per bin: S pairs
   static constexpr size_t kPairsSmem = (size_t)kChunk * kWin * kPairBytes;
   static constexpr size_t kRawSmem = 2 * (size_t)kChunk * S * kRaw * sizeof(T);
   static constexpr size_t kSmem = kPairsSmem + kRawSmem;
@@ -364,7 +367,17 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
           dv[ks] = w;
         }
       }
-      if constexpr (S == 1) {
+      if constexpr (K::kHalfPairs) {
+        // (value, difference) of two slices as two 32-bit words; the value
+        // is v + D f with f = p - d, so store v itself (not the centred a)
+        uint2 *p2 = reinterpret_cast<uint2 *>(pairs) + (size_t)s_ai * (S / 2) * kWin + j;
+#pragma unroll
+        for (int g = 0; g < S / 2; ++g) {
+          float v0 = av[2 * g] + jc * dv[2 * g], v1 = av[2 * g + 1] + jc * dv[2 * g + 1];
+          if (slope && interior) { v0 = av[2 * g]; v1 = av[2 * g + 1]; }
+          p2[g * kWin] = make_uint2(atb::pack_pair<T>(v0, v1), atb::pack_pair<T>(dv[2 * g], dv[2 * g + 1]));
+        }
+      } else if constexpr (S == 1) {
         reinterpret_cast<float2 *>(pairs)[s_ai * kWin + j] = make_float2(av[0], dv[0]);
       } else {
         float4 *p4 = reinterpret_cast<float4 *>(pairs) + (size_t)s_ai * (S / 2) * kWin + j;
@@ -398,7 +411,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
       const float c8 = 8.f * p.c, s4 = 4.f * p.s;
       // this angle's pairs, indexed by floor(q) (window centre at 0)
       const unsigned char *w = pairs + ((size_t)ai * kWin + kHalf) * K::kPairBytes;
-      if constexpr (S > 1) w = pairs + ((size_t)ai * (S / 2) * kWin + kHalf) * 16;
+      if constexpr (S > 1) w = pairs + ((size_t)ai * (S / 2) * kWin + kHalf) * (K::kHalfPairs ? 8 : 16);
       auto body = [&](auto checked_tag) {
         constexpr bool kChecked = decltype(checked_tag)::value;
 #pragma unroll
@@ -407,8 +420,10 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
 #pragma unroll
           for (int c = 0; c < PX; ++c) {
             const float q = fmaf((float)c, c8, qr);
-            int j = __float_as_int(__fadd_rd(q, kMagic)) - kMagicBits;
+            const float tq = __fadd_rd(q, kMagic);
+            int j = __float_as_int(tq) - kMagicBits;
             bool inr = true;
+            bool moved = false;
             if constexpr (kChecked) {
               const float dl = q - p.qlo, dr = q - p.qmax;
               inr = (dl >= 0.f) && (dr <= 0.f);
@@ -420,10 +435,27 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
                 const double pe =
                     __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)), a.center);
                 inr = (pe >= 0.0) && (pe <= (double)(ncol - 1));
+                moved = j < p.j0 - kHalf;
                 j = max(j, p.j0 - kHalf);
               }
             }
-            if constexpr (S == 1) {
+            if constexpr (K::kHalfPairs) {
+              // fraction of q in its bin, then v + D f on two slices at once
+              const float f = moved ? q - (float)j : q - __fsub_rn(tq, kMagic);
+              const unsigned long long F = pack2(f, f);
+              const uint2 *w2 = reinterpret_cast<const uint2 *>(w) + j;
+#pragma unroll
+              for (int g = 0; g < S / 2; ++g) {
+                uint2 pw = w2[g * kWin];
+                if constexpr (kChecked) {
+                  if (!inr) pw = make_uint2(0u, 0u);
+                }
+                float v0, v1, d0, d1;
+                atb::unpack_pair<T>(pw.x, v0, v1);
+                atb::unpack_pair<T>(pw.y, d0, d1);
+                fma_acc2(acc2[b][c][g], pack2(v0, v1), pack2(d0, d1), F);
+              }
+            } else if constexpr (S == 1) {
               const float2 pr = reinterpret_cast<const float2 *>(w)[j];
               float v = fmaf(pr.y, q, pr.x);
               if constexpr (kChecked) v = inr ? v : 0.f;

@@ -39,6 +39,28 @@ __device__ __forceinline__ float to_float(float v) { return v; }
 __device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
 __device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
 
+// two floats as one 32-bit word of two 16-bit values (first in the low half)
+template <typename T> __device__ __forceinline__ unsigned pack_pair(float lo, float hi);
+template <> __device__ __forceinline__ unsigned pack_pair<__half>(float lo, float hi) {
+  const __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<const unsigned *>(&h);
+}
+template <> __device__ __forceinline__ unsigned pack_pair<__nv_bfloat16>(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const unsigned *>(&h);
+}
+// and back: bfloat16 widens by a shift, float16 by conversion
+template <typename T> __device__ __forceinline__ void unpack_pair(unsigned w, float &lo, float &hi);
+template <> __device__ __forceinline__ void unpack_pair<__half>(unsigned w, float &lo, float &hi) {
+  const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w));
+  lo = f.x;
+  hi = f.y;
+}
+template <> __device__ __forceinline__ void unpack_pair<__nv_bfloat16>(unsigned w, float &lo, float &hi) {
+  lo = __uint_as_float(w << 16);
+  hi = __uint_as_float(w & 0xffff0000u);
+}
+
 __device__ __forceinline__ void store_from_float(float *p, float v) { *p = v; }
 __device__ __forceinline__ void store_from_float(__half *p, float v) { *p = __float2half_rn(v); }
 __device__ __forceinline__ void store_from_float(__nv_bfloat16 *p, float v) {

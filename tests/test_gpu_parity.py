@@ -310,3 +310,20 @@ def test_single_slice_tile_variant_1(cuda, ncol, cen):
     for v in (0, 1):
         got = R.backproject(t, ang, cen, variant=v)[:, 0].cpu().numpy()
         assert O.rel_l2(got, ref) < 1e-6
+
+
+@pytest.mark.parametrize("storage,bound", [("float16", 5e-4), ("bfloat16", 4e-3)])
+def test_reduced_storage_stack(cuda, storage, bound):
+    """Stacks (4- and 2-slice CTAs keep 16-bit pairs in shared memory):
+    FP32 accumulation, error bounded by the storage precision."""
+    nrow, ncol, nslice = 181, 192, 6
+    s3 = np.stack([phantom.ellipse_sinogram(60 + k, nrow, ncol, 95.3)[0]
+                   for k in range(nslice)], axis=1)
+    ang = np.linspace(0, np.pi, nrow, endpoint=False)
+    t = torch.from_numpy(s3).cuda()
+    got = R.fbp_reconstruction(t, 95.3, angles=ang, apply_log=False,
+                               storage=storage).cpu().numpy()
+    for k in range(nslice):
+        ref = O.fbp_reconstruction(s3[:, k], 95.3, angles=ang,
+                                   apply_log=False)
+        assert O.rel_l2(got[:, k], ref) < bound, (k, O.rel_l2(got[:, k], ref))
