@@ -54,6 +54,9 @@ def _args():
     ap.add_argument("--slices", type=int, default=NSLICE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--storage", default="float32",
+                    choices=["float32", "float16", "bfloat16"],
+                    help="element type of the filtered sinogram (stack)")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
@@ -223,7 +226,7 @@ def run_ours(args, rank, world, local_rank):
     def step(src, out=None):
         return R.fbp_reconstruction(src, CENTER, angles=ang, ratio=1.0,
                                     filter_name="hann", apply_log=False,
-                                    out=out)
+                                    out=out, storage=args.storage)
 
     def barrier():
         if world > 1:
@@ -259,7 +262,8 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- per-kernel timing (roofline): filter and back-projection alone
     from algotom_b200.rec import reconstruction as RR
-    filt = RR.filter_sinograms(sino, 150, "edge", False, None, "hann")
+    filt = RR.filter_sinograms(sino, 150, "edge", False, None, "hann",
+                               args.storage)
     mask_r2 = RR._mask_r2(1.0, CENTER, NCOL)
     scale = RR._scale(NROW)
     outb = torch.empty((NCOL, nslice, NCOL), dtype=torch.float32, device=dev)
@@ -354,7 +358,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded 12-ellipse phantoms, Poisson 5e3 photons)",
         "config": {"workload": WORKLOAD, "slices_per_gpu": nslice,
                    "nrow": NROW, "ncol": NCOL, "center": CENTER,
-                   "storage": "float32", "kahan": "chunk",
+                   "storage": args.storage, "kahan": "chunk",
                    "l2": "inputs larger than L2 (4.7 GB sinogram per GPU)"},
         "slices_per_s": world * nslice * args.steps / t_dev,
         "accuracy": err,
