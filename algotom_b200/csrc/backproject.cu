@@ -150,9 +150,12 @@ struct BPCfg {
   // raw window: elements of T from a start rounded down to a 16-byte vector
   static constexpr int kVecElems = 16 / (int)sizeof(T);
   static constexpr int kRaw = ((kWin + 1 + (kVecElems - 1) + (kVecElems - 1)) / kVecElems) * kVecElems;
-  // 16-bit storage with S >= 2 keeps 16-bit (value, difference) pairs in
-  // shared memory: 4 bytes per bin and slice instead of 8
-  static constexpr bool kHalfPairs = sizeof(T) == 2 && S >= 2;
+  // bfloat16 storage with S >= 2 keeps 16-bit (value, difference) pairs in
+  // shared memory: 4 bytes per bin and slice instead of 8 (bfloat16 widens
+  // to FP32 with one shift; float16 would need conversions, which cost more
+  // issue slots than the halved shared-memory traffic saves, so float16
+  // stages FP32 pairs)
+  static constexpr bool kHalfPairs = std::is_same<T, __nv_bfloat16>::value && S >= 2;
   static constexpr int kPairBytes = (kHalfPairs ? 4 : 8) * S;  // per bin: S pairs
   static constexpr size_t kPairsSmem = (size_t)kChunk * kWin * kPairBytes;
   static constexpr size_t kRawSmem = 2 * (size_t)kChunk * S * kRaw * sizeof(T);
