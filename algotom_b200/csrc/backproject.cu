@@ -129,6 +129,90 @@ __device__ __forceinline__ void fma_acc2(unsigned long long &acc, unsigned long 
   asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc) : "l"(v));
 }
 
+// Tensor memory (TMEM, 128 lanes x 512 columns of 32-bit cells per SM)
+// holds the compensated running totals between chunk folds, which keeps
+// them out of the registers of the accumulation loop.  Warp w of a CTA
+// reaches lanes 32 (w % 4) .. 32 (w % 4) + 31 only; every thread uses the
+// cells of its own lane.  An address is (lane << 16) | column.  Each
+// transfer waits for its own completion, so the registers are free after it.
+template <int N> __device__ __forceinline__ void tmem_ld(uint32_t taddr, float *r);
+template <int N> __device__ __forceinline__ void tmem_st(uint32_t taddr, const float *r);
+template <> __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7]), "=f"(r[8]), "=f"(r[9]), "=f"(r[10]), "=f"(r[11]), "=f"(r[12]), "=f"(r[13]), "=f"(r[14]), "=f"(r[15])
+      : "r"(taddr)
+      : "memory");
+}
+template <> __device__ __forceinline__ void tmem_st<16>(uint32_t taddr, const float *r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};\n\t"
+      "tcgen05.wait::st.sync.aligned;"
+      :
+      : "r"(taddr), "f"(r[0]), "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7]), "f"(r[8]), "f"(r[9]), "f"(r[10]), "f"(r[11]), "f"(r[12]), "f"(r[13]), "f"(r[14]), "f"(r[15])
+      : "memory");
+}
+template <> __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7]), "=f"(r[8]), "=f"(r[9]), "=f"(r[10]), "=f"(r[11]), "=f"(r[12]), "=f"(r[13]), "=f"(r[14]), "=f"(r[15]), "=f"(r[16]), "=f"(r[17]), "=f"(r[18]), "=f"(r[19]), "=f"(r[20]), "=f"(r[21]), "=f"(r[22]), "=f"(r[23]), "=f"(r[24]), "=f"(r[25]), "=f"(r[26]), "=f"(r[27]), "=f"(r[28]), "=f"(r[29]), "=f"(r[30]), "=f"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+template <> __device__ __forceinline__ void tmem_st<32>(uint32_t taddr, const float *r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n\t"
+      "tcgen05.wait::st.sync.aligned;"
+      :
+      : "r"(taddr), "f"(r[0]), "f"(r[1]), "f"(r[2]), "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7]), "f"(r[8]), "f"(r[9]), "f"(r[10]), "f"(r[11]), "f"(r[12]), "f"(r[13]), "f"(r[14]), "f"(r[15]), "f"(r[16]), "f"(r[17]), "f"(r[18]), "f"(r[19]), "f"(r[20]), "f"(r[21]), "f"(r[22]), "f"(r[23]), "f"(r[24]), "f"(r[25]), "f"(r[26]), "f"(r[27]), "f"(r[28]), "f"(r[29]), "f"(r[30]), "f"(r[31])
+      : "memory");
+}
+
+// Columns of TMEM a CTA of BPCfg<T, S, V> takes: two cells (total,
+// compensation) per pixel and slice for each thread, times the warps that
+// share a lane quarter, rounded up to a power of two >= 32.
+constexpr int tmem_cols(int cells_per_thread, int threads) {
+  int need = cells_per_thread * (threads / 128), c = 32;
+  while (c < need) c *= 2;
+  return c;
+}
+
+// Warp 0 allocates kCols columns for the CTA (and gives up the right to
+// allocate more, so other CTAs of the SM never wait on this one); every
+// thread returns the base address.  All threads of the CTA must call it.
+template <int kCols>
+__device__ __forceinline__ uint32_t tmem_alloc_cta(uint32_t *slot) {
+  if (threadIdx.x < 32) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(slot);
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n\t"
+        "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::"r"(a),
+        "n"(kCols)
+        : "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return *reinterpret_cast<volatile uint32_t *>(slot);
+}
+
+// Warp 0 frees the CTA's columns once every thread is done with them.  All
+// threads of the CTA must call it.
+template <int kCols>
+__device__ __forceinline__ void tmem_free_cta(uint32_t base) {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    asm volatile(
+        "tcgen05.fence::after_thread_sync;\n\t"
+        "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base),
+        "n"(kCols)
+        : "memory");
+  }
+}
+
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
@@ -160,12 +244,20 @@ struct BPCfg {
   static constexpr size_t kPairsSmem = (size_t)kChunk * kWin * kPairBytes;
   static constexpr size_t kRawSmem = 2 * (size_t)kChunk * S * kRaw * sizeof(T);
   static constexpr size_t kSmem = kPairsSmem + kRawSmem;
+  // compensated totals in TMEM: kAcc accumulators per thread, as (total,
+  // compensation) cells in 2 kAcc columns; moved kXfer accumulators at a time
+  static constexpr int kAcc = PX * G::PY * S;
+  static constexpr int kXfer = kAcc % 16 == 0 ? 16 : 8;
+  static constexpr int kTmemCols = tmem_cols(2 * kAcc, kThreads);
+  static_assert(kThreads % 128 == 0 && kAcc % 8 == 0, "TMEM layout");
 };
 
 // One CTA's work: the TX x TY pixel tile (bx, by) of the slice group bz.
-// Every thread of the CTA must call it (it synchronises).
+// Every thread of the CTA must call it (it synchronises).  tmem is the
+// base of the CTA's K::kTmemCols TMEM columns (chunked Kahan only).
 template <typename T, int S, bool kPerAngleKahan, int V = 0>
-__device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz, unsigned char *smem) {
+__device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz, unsigned char *smem,
+                                        uint32_t tmem) {
   using K = BPCfg<T, S, V>;
   constexpr int kThreads = K::kThreads;
   constexpr int PX = K::PX, PY = K::PY, TX = K::TX, TY = K::TY;
@@ -193,7 +285,9 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   const int ty = (warp / K::WX) * (4 * PY) + (lane >> 3);
 
   // accumulators: FP32 chunk partials (packed two slices per word when
-  // S >= 2) and the compensated running totals
+  // S >= 2) and the compensated running totals, in registers for per-angle
+  // Kahan and in TMEM (accumulator n = (b PX + c) S + k at columns 2n,
+  // 2n + 1 of this thread's span) for chunked Kahan
   float accf[PY][PX];
   unsigned long long acc2[PY][PX][NP];
   float sum[PY][PX][S], comp[PY][PX][S];
@@ -207,6 +301,26 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
 #pragma unroll
       for (int k = 0; k < S; ++k) { sum[b][c][k] = 0.f; comp[b][c][k] = 0.f; }
     }
+  constexpr int kAcc = K::kAcc, kXfer = K::kXfer;
+  const uint32_t tm = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * 2 * kAcc);
+  // chunk partial of accumulator n
+  auto partial = [&](int n) -> float {
+    const int k = n % S, c = (n / S) % PX, b = n / (S * PX);
+    if constexpr (S == 1) {
+      return accf[b][c];
+    } else {
+      float lo, hi;
+      unpack2(acc2[b][c][k / 2], lo, hi);
+      return (k & 1) ? hi : lo;
+    }
+  };
+  if constexpr (!kPerAngleKahan) {
+    float z[2 * kXfer];
+#pragma unroll
+    for (int i = 0; i < 2 * kXfer; ++i) z[i] = 0.f;
+#pragma unroll
+    for (int n0 = 0; n0 < kAcc; n0 += kXfer) tmem_st<2 * kXfer>(tm + 2 * n0, z);
+  }
 
   const double ic = 0.5 * (double)(ncol - 1);
   const int nchunk = (a.nrow + kChunk - 1) / kChunk;
@@ -482,26 +596,39 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
       if (flag & 2) body(std::true_type{});
       else body(std::false_type{});
     }
-    // fold this chunk's partials into the compensated totals
-    if (!kPerAngleKahan) {
+    // fold this chunk's partials into the compensated totals in TMEM
+    if constexpr (!kPerAngleKahan) {
+      __syncwarp();
+#pragma unroll
+      for (int n0 = 0; n0 < kAcc; n0 += kXfer) {
+        float r[2 * kXfer];
+        tmem_ld<2 * kXfer>(tm + 2 * n0, r);
+#pragma unroll
+        for (int i = 0; i < kXfer; ++i) kahan_add(r[2 * i], r[2 * i + 1], partial(n0 + i));
+        tmem_st<2 * kXfer>(tm + 2 * n0, r);
+      }
 #pragma unroll
       for (int b = 0; b < PY; ++b)
 #pragma unroll
         for (int c = 0; c < PX; ++c) {
-          if constexpr (S == 1) {
-            kahan_add(sum[b][c][0], comp[b][c][0], accf[b][c]);
-            accf[b][c] = 0.f;
-          } else {
+          accf[b][c] = 0.f;
 #pragma unroll
-            for (int g = 0; g < S / 2; ++g) {
-              float lo, hi;
-              unpack2(acc2[b][c][g], lo, hi);
-              kahan_add(sum[b][c][2 * g], comp[b][c][2 * g], lo);
-              kahan_add(sum[b][c][2 * g + 1], comp[b][c][2 * g + 1], hi);
-              acc2[b][c][g] = 0ull;
-            }
-          }
+          for (int g = 0; g < NP; ++g) acc2[b][c][g] = 0ull;
         }
+    }
+  }
+  if constexpr (!kPerAngleKahan) {
+    __syncwarp();
+#pragma unroll
+    for (int n0 = 0; n0 < kAcc; n0 += kXfer) {
+      float r[2 * kXfer];
+      tmem_ld<2 * kXfer>(tm + 2 * n0, r);
+#pragma unroll
+      for (int i = 0; i < kXfer; ++i) {
+        const int n = n0 + i, k = n % S, c = (n / S) % PX, b = n / (S * PX);
+        sum[b][c][k] = r[2 * i];
+        comp[b][c][k] = r[2 * i + 1];
+      }
     }
   }
 
@@ -533,8 +660,16 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
 
 template <typename T, int S, bool kPerAngleKahan, int V>
 __global__ void __launch_bounds__(BPCfg<T, S, V>::kThreads, BPCfg<T, S, V>::kMinBlocks) bp_kernel(BPArgs a) {
+  using K = BPCfg<T, S, V>;
   extern __shared__ __align__(16) unsigned char smem[];
-  bp_tile<T, S, kPerAngleKahan, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+  if constexpr (kPerAngleKahan) {
+    bp_tile<T, S, true, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0u);
+  } else {
+    __shared__ uint32_t tmem_slot;
+    const uint32_t tmem = tmem_alloc_cta<K::kTmemCols>(&tmem_slot);
+    bp_tile<T, S, false, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, tmem);
+    tmem_free_cta<K::kTmemCols>(tmem);
+  }
 }
 
 // Persistent back-projection of a batch of single-slice items of uneven
@@ -547,6 +682,8 @@ __global__ void __launch_bounds__(BPCfg<T, 1, V>::kThreads, BPCfg<T, 1, V>::kMin
   using K = BPCfg<T, 1, V>;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int unit_s;
+  __shared__ uint32_t tmem_slot;
+  const uint32_t tmem = tmem_alloc_cta<K::kTmemCols>(&tmem_slot);
   for (;;) {
     __syncthreads();  // the previous unit is done with unit_s
     if (threadIdx.x == 0) unit_s = atomicAdd(counter, 1);
@@ -566,8 +703,9 @@ __global__ void __launch_bounds__(BPCfg<T, 1, V>::kThreads, BPCfg<T, 1, V>::kMin
     a.vec16 = sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(it.sino) % 16) == 0 &&
               it.sino_row_stride % 4 == 0 && it.ncol % 4 == 0;
     const int tiles_x = (it.ncol + K::TX - 1) / K::TX;
-    bp_tile<T, 1, false, V>(a, tile % tiles_x, tile / tiles_x, 0, smem);
+    bp_tile<T, 1, false, V>(a, tile % tiles_x, tile / tiles_x, 0, smem, tmem);
   }
+  tmem_free_cta<K::kTmemCols>(tmem);
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(counter + 1, 1) == (int)gridDim.x - 1) {
@@ -582,7 +720,7 @@ template <typename T, int S, bool kPerAngleKahan, int V = 0>
 int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
   using K = BPCfg<T, S, V>;
   auto fn = bp_kernel<T, S, kPerAngleKahan, V>;
-  const int rc = atb::ensure_smem(fn, K::kSmem, "atb_backproject");
+  const int rc = atb::ensure_smem(fn, K::kSmem, "atb_backproject", K::kThreads, kPerAngleKahan ? 0 : K::kTmemCols);
   if (rc != ATB_OK) return rc;
   dim3 grid((a.ncol + K::TX - 1) / K::TX, (a.ncol + K::TY - 1) / K::TY, (nslices + S - 1) / S);
   fn<<<grid, K::kThreads, K::kSmem, st>>>(a);
@@ -702,7 +840,7 @@ template <int V>
 int launch_batch(const atb_bp_item *items, int nitems, const int *units, int nunits, int *counter, int max_ctas,
                  cudaStream_t st) {
   using K = BPCfg<float, 1, V>;
-  const int rc = atb::ensure_smem(bp_batch_kernel<float, V>, K::kSmem, "atb_backproject_batch");
+  const int rc = atb::ensure_smem(bp_batch_kernel<float, V>, K::kSmem, "atb_backproject_batch", K::kThreads, K::kTmemCols);
   if (rc != ATB_OK) return rc;
   int grid = K::kMinBlocks * sm_count();
   if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
@@ -830,7 +968,8 @@ extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitem
           cudaSuccess)
     return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: %s", cudaGetErrorString(e));
   using K = BPCfg<float, 1, 0>;
-  const int rc = atb::ensure_smem(bp_batch_kernel<float, 0>, K::kSmem, "atb_backproject_batch_noalloc");
+  const int rc =
+      atb::ensure_smem(bp_batch_kernel<float, 0>, K::kSmem, "atb_backproject_batch_noalloc", K::kThreads, K::kTmemCols);
   if (rc != ATB_OK) return rc;
   int grid = 2 * sm_count();
   if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;

@@ -22,11 +22,14 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 
 // Raises a kernel's dynamic shared-memory limit once per (kernel, device),
 // so that launches made while a stream is being captured into a CUDA graph
-// issue no configuration calls.  Thread-safe.  Returns 0 or ATB_ECUDA.
-int ensure_smem_raw(const void *fn, size_t bytes, const char *what);
+// issue no configuration calls.  For a kernel whose CTAs of `threads`
+// threads each allocate `tmem_cols` TMEM columns, it also checks once that
+// all CTAs an SM can hold fit in its 512 columns.  Thread-safe.  Returns 0
+// or ATB_ECUDA.
+int ensure_smem_raw(const void *fn, size_t bytes, const char *what, int threads = 0, int tmem_cols = 0);
 template <typename F>
-int ensure_smem(F *fn, size_t bytes, const char *what) {
-  return ensure_smem_raw(reinterpret_cast<const void *>(fn), bytes, what);
+int ensure_smem(F *fn, size_t bytes, const char *what, int threads = 0, int tmem_cols = 0) {
+  return ensure_smem_raw(reinterpret_cast<const void *>(fn), bytes, what, threads, tmem_cols);
 }
 
 __device__ __forceinline__ float load_as_float(const float *p) { return __ldg(p); }

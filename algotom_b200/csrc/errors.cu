@@ -19,7 +19,7 @@ int fail(int code, const char *fmt, ...) {
   return code;
 }
 
-int ensure_smem_raw(const void *fn, size_t bytes, const char *what) {
+int ensure_smem_raw(const void *fn, size_t bytes, const char *what, int threads, int tmem_cols) {
   struct Entry {
     const void *fn;
     int dev;
@@ -35,6 +35,15 @@ int ensure_smem_raw(const void *fn, size_t bytes, const char *what) {
     if (table[i].fn == fn && table[i].dev == dev && table[i].bytes >= bytes) return ATB_OK;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return fail(ATB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  if (tmem_cols > 0) {
+    // every CTA that can be resident on an SM must find its TMEM columns
+    // free, so that no allocation ever waits
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, bytes);
+    if (e != cudaSuccess) return fail(ATB_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+    if ((long long)per_sm * tmem_cols > 512)
+      return fail(ATB_ECUDA, "%s: %d resident CTAs x %d TMEM columns exceed 512", what, per_sm, tmem_cols);
+  }
   for (int i = 0; i < used; ++i)
     if (table[i].fn == fn && table[i].dev == dev) {
       table[i].bytes = bytes;
