@@ -15,9 +15,12 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
            "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
-           "atb_backproject_batch_noalloc")
+           "atb_backproject_batch_noalloc", "atb_gaussian_rows",
+           "atb_zoom_linear", "atb_image_range", "atb_slice_metric_workspace",
+           "atb_slice_metric")
 
 F32, F16, BF16 = 0, 1, 2
+METRICS = {"entropy": 0, "sharpness": 1}
 PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
              "wrap": 4, "linear_ramp": 5, "mean": 6, "maximum": 7,
              "minimum": 8, "median": 9}
@@ -66,6 +69,20 @@ _SIGS = {
         _vp]),
     "atb_backproject_batch_noalloc": (ctypes.c_int, [
         _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "atb_gaussian_rows": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+        _c_i64, _vp]),
+    "atb_zoom_linear": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, _c_i64, ctypes.c_int,
+        ctypes.c_int, _vp]),
+    "atb_image_range": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "atb_slice_metric_workspace": (_c_i64, [
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "atb_slice_metric": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, ctypes.c_float, ctypes.c_float, _vp, _c_i64, _vp,
+        _vp]),
 }
 
 _lib = None

@@ -1,0 +1,325 @@
+"""Centre-of-rotation search by slice metrics on the device.
+
+Drop-in for ``find_center_based_slice_metric`` and
+``_find_center_based_slice_metric`` of ``algotom/rec/reconstruction.py``
+(algotom 1.6.0, ``:1254-1458``) for the FBP and BPF methods: same names,
+signatures, defaults, errors, warnings and results.
+
+The reference reconstructs the slice once per candidate centre, each time
+filtering the sinogram again, and evaluates the metric on the host.  Here
+the ramp filter (independent of the centre) runs once; the candidates are
+then back-projected by ONE persistent batched launch whose work items share
+the filtered sinogram and differ only in their centre
+(``atb_backproject_batch``), and the metric of every candidate image is
+computed on the device (``atb_slice_metric``).  The pre-steps -- Gaussian
+smoothing along the detector and the linear zoom of the coarse pass -- are
+device kernels with scipy's float32 results (``atb_gaussian_rows``,
+``atb_zoom_linear``).  Only the per-candidate metric values (8 bytes each)
+come back to the host; a custom ``metric_function`` gets each
+reconstruction as a NumPy array, as in the reference.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from .. import _native as nat
+from . import reconstruction as R
+
+# device bytes of candidate reconstructions held at once
+_CHUNK_BYTES = 8 << 30
+
+
+# --------------------------------------------------------------------------
+# device steps
+# --------------------------------------------------------------------------
+def _gaussian_weights(sigma, truncate=4.0):
+    """Half kernel w[0..r] of scipy's unit-sum sampled Gaussian."""
+    sigma = float(sigma)
+    r = int(truncate * sigma + 0.5)
+    x = np.arange(-r, r + 1)
+    phi = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+    phi = phi / phi.sum()
+    return np.ascontiguousarray(phi[r:])
+
+
+def gaussian_filter_rows(x, sigma):
+    """``scipy.ndimage.gaussian_filter1d(x, sigma, axis=1)`` of a 2-D float32
+    CUDA tensor (mode "reflect"); returns a new tensor."""
+    w = _gaussian_weights(sigma)
+    wd = torch.from_numpy(w).to(x.device)
+    out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
+    nat.call("atb_gaussian_rows", x.data_ptr(), x.stride(0), x.shape[0],
+             x.shape[1], wd.data_ptr(), len(w) - 1, out.data_ptr(),
+             out.stride(0), R._stream_ptr(x.device))
+    return out
+
+
+def zoom_image(x, zoom):
+    """``scipy.ndimage.zoom(x, zoom, order=1, mode="nearest")`` of a 2-D
+    float32 CUDA tensor."""
+    rows, cols = (int(round(s * float(zoom))) for s in x.shape)
+    out = torch.empty((rows, cols), dtype=torch.float32, device=x.device)
+    nat.call("atb_zoom_linear", x.data_ptr(), x.stride(0), x.shape[0],
+             x.shape[1], out.data_ptr(), out.stride(0), rows, cols,
+             R._stream_ptr(x.device))
+    return out
+
+
+def image_range(img):
+    """(min, max) of a 2-D float32 CUDA tensor as NumPy float32 scalars."""
+    work = torch.empty(3, dtype=torch.int32, device=img.device)
+    out = torch.empty(2, dtype=torch.float32, device=img.device)
+    nat.call("atb_image_range", img.data_ptr(), img.stride(0), img.shape[0],
+             img.shape[1], work.data_ptr(), out.data_ptr(),
+             R._stream_ptr(img.device))
+    lo, hi = out.cpu().numpy()
+    return np.float32(lo), np.float32(hi)
+
+
+def slice_metrics(imgs, metric="entropy", nmin=0.0, nmax=1.0):
+    """Metric of every image of a [n, rows, cols] float32 CUDA tensor.
+
+    ``"entropy"``: histogram entropy after normalising by (nmin, nmax);
+    ``"sharpness"``: mean gradient magnitude.  Returns float64 [n].
+    """
+    code = nat.METRICS[metric]
+    n, rows, cols = imgs.shape
+    if imgs.stride(2) != 1:
+        imgs = imgs.contiguous()
+    nbytes = nat.call("atb_slice_metric_workspace", n, rows, cols, code)
+    work = torch.empty(max(int(nbytes), 8), dtype=torch.uint8,
+                       device=imgs.device)
+    out = torch.empty(n, dtype=torch.float64, device=imgs.device)
+    nat.call("atb_slice_metric", imgs.data_ptr(), imgs.stride(0),
+             imgs.stride(1), n, rows, cols, code, float(np.float32(nmin)),
+             float(np.float32(nmax)), work.data_ptr(), work.numel(),
+             out.data_ptr(), R._stream_ptr(imgs.device))
+    return out.cpu().numpy()
+
+
+def _backproject_items(items, device, variant):
+    """One persistent batched back-projection of ``nat.BpItem`` s."""
+    n = len(items)
+    arr = (nat.BpItem * n)(*items)
+    nunits = nat.call("atb_bp_batch_plan", ctypes.addressof(arr), n, None, 0,
+                      variant)
+    units = (ctypes.c_int * nunits)()
+    nat.call("atb_bp_batch_plan", ctypes.addressof(arr), n,
+             ctypes.addressof(units), nunits, variant)
+    items_dev = torch.frombuffer(bytearray(bytes(arr)),
+                                 dtype=torch.uint8).to(device)
+    units_dev = torch.frombuffer(bytearray(bytes(units)),
+                                 dtype=torch.int32).to(device)
+    counter = torch.zeros(2, dtype=torch.int32, device=device)
+    nat.call("atb_backproject_batch", items_dev.data_ptr(), n,
+             units_dev.data_ptr(), nunits, counter.data_ptr(), 0, variant,
+             R._stream_ptr(device))
+    # the caching allocator keeps these until the stream has used them
+    return items_dev, units_dev, counter
+
+
+class _Source:
+    """The sinogram of one search, prepared once for every candidate: the
+    ramp-filtered rows for FBP, the -log rows for BPF."""
+
+    def __init__(self, sino, angles, method, filter_name):
+        if method not in ("fbp", "bpf"):
+            raise NotImplementedError(
+                "method %r: this library reconstructs with 'fbp' or 'bpf'"
+                % (method,))
+        self.nrow, self.ncol = sino.shape
+        self.method, self.filter_name = method, filter_name
+        self.angles = R._validate(sino, 0.0, angles)[3]
+        self.sino = sino
+        self.pad = min(int(0.15 * self.ncol), 150)
+        if method == "fbp":
+            f = R.filter_sinograms(sino.unsqueeze(1), self.pad, "edge", False,
+                                   None, filter_name)
+            self.src, self.src_rs = f, f.stride(0)
+        else:
+            src = sino if sino.stride(1) == 1 else sino.contiguous()
+            self.src, self.src_rs = src, src.stride(0)
+        self.trig = R._trig(self.angles, sino.device)
+
+    def reconstruct(self, centers, ratio):
+        """float32 [len(centers), ncol, ncol] reconstructions."""
+        nrow, ncol, dev = self.nrow, self.ncol, self.sino.device
+        for c in centers:
+            R._validate(self.sino, float(c), self.angles)
+        out = torch.empty((len(centers), ncol, ncol), dtype=torch.float32,
+                          device=dev)
+        scale = R._scale(nrow)
+        fbp = self.method == "fbp"
+        items = []
+        for k, c in enumerate(centers):
+            it = nat.BpItem()
+            it.sino, it.sino_row_stride = self.src.data_ptr(), self.src_rs
+            it.trig = self.trig.data_ptr()
+            it.out, it.out_row_stride = out[k].data_ptr(), out.stride(1)
+            it.center = float(np.float32(c))
+            it.nrow, it.ncol = nrow, ncol
+            if fbp:
+                it.mask_r2, it.scale, it.edge_pad = R._mask_r2(
+                    ratio, float(c), ncol), scale, 0
+            else:
+                it.mask_r2, it.scale, it.edge_pad = -1.0, 1.0, 1
+            items.append(it)
+        keep = _backproject_items(items, dev, 1 if ncol <= 512 else 0)
+        if not fbp:
+            out = R._circular_filter(out, None, self.filter_name, self.pad,
+                                     "edge")
+            idx = torch.arange(ncol, device=dev) - ncol // 2
+            d2 = (idx[None, :] ** 2 + idx[:, None] ** 2).to(torch.float64)
+            for k, c in enumerate(centers):
+                r2 = R._mask_r2(ratio, float(c), ncol)
+                if r2 >= 0:
+                    out[k] *= (d2 <= r2).to(out.dtype)
+            out *= scale
+        del keep
+        return out
+
+
+def reconstruct_centers(sino, centers, angles=None, method="fbp", ratio=1.0,
+                        filter_name="hann"):
+    """Reconstructions of one sinogram at several centres.
+
+    ``sino``: 2-D float32 CUDA tensor, already in attenuation (-log) form.
+    Returns a float32 [len(centers), ncol, ncol] CUDA tensor equal, slice by
+    slice, to ``fbp_reconstruction`` / ``bpf_reconstruction`` (with
+    ``apply_log=False`` and default pad) at each centre.
+    """
+    return _Source(sino, angles, method, filter_name).reconstruct(centers,
+                                                                  ratio)
+
+
+# --------------------------------------------------------------------------
+# drop-in API
+# --------------------------------------------------------------------------
+def _prepare(sinogram, sigma, apply_log):
+    """Smoothing and -log of ``reconstruction.py:1317-1325`` on the device.
+
+    As in the reference, the replacement of values <= 0 by 1 happens in the
+    array being searched: a fresh smoothed copy when ``sigma > 0``, the
+    caller's own array otherwise.
+    """
+    if sigma > 0:
+        t, _ = R._to_device(sinogram)
+        if t.dim() != 2:
+            raise ValueError("sinogram must be 2-D")
+        t = gaussian_filter_rows(t, sigma)
+        if apply_log:
+            R._check_log_input(t)
+    else:
+        if apply_log:
+            R._check_log_input(sinogram)
+        t, _ = R._to_device(sinogram)
+        if t.dim() != 2:
+            raise ValueError("sinogram must be 2-D")
+    if apply_log:
+        t = R._neg_log(t.unsqueeze(1))[:, 0, :]
+    return t
+
+
+def _find_center_based_slice_metric(sinogram, start, stop, step=1,
+                                    metric="entropy", method="fbp", gpu=True,
+                                    angles=None, ratio=1.0, filter_name="hann",
+                                    apply_log=True, ncore=None,
+                                    prefer="threads", sigma=2,
+                                    return_metric=True, invert_metric=False,
+                                    metric_function=None, **kwargs):
+    """Metric of the reconstruction at every centre of
+    ``np.arange(start, stop, step)``; ``reconstruction.py:1254-1346``.
+
+    Returns ``(centers, metrics)`` if ``return_metric`` else the centre of
+    the smallest metric.  ``gpu``, ``ncore`` and ``prefer`` are accepted
+    for compatibility; the work always runs on the device.
+    """
+    list_center = np.arange(start, stop, step)
+    num_center = len(list_center)
+    if num_center == 0:
+        raise ValueError("Invalid searching parameters: (start, stop, step)={}"
+                         "!!!".format((start, stop, step)))
+    sino = _prepare(sinogram, sigma, apply_log)
+    ncol = sino.shape[1]
+    source = _Source(sino, angles, method, filter_name)
+    nmin, nmax = 0.0, 1.0
+    if metric_function is None and metric == "entropy":
+        img = source.reconstruct([np.mean(list_center)], ratio)[0]
+        nmin, nmax = image_range(img)
+        del img
+        if nmin == nmax:
+            raise ValueError("Empty image!!!")
+    per_chunk = max(1, int(_CHUNK_BYTES // (4 * ncol * ncol)))
+    list_metric = np.ones(num_center)
+    for k0 in range(0, num_center, per_chunk):
+        cs = list_center[k0:k0 + per_chunk]
+        imgs = source.reconstruct(cs, ratio)
+        if metric_function is None:
+            m = "entropy" if metric == "entropy" else "sharpness"
+            list_metric[k0:k0 + len(cs)] = slice_metrics(imgs, m, nmin, nmax)
+        else:
+            host = imgs.cpu().numpy()
+            if method == "bpf":
+                host = host.astype(np.float64)
+            for i in range(len(cs)):
+                list_metric[k0 + i] = metric_function(host[i], **kwargs)
+        del imgs
+    if invert_metric:
+        list_metric = np.max(list_metric) - list_metric
+    opt_center = list_center[np.argmin(list_metric)]
+    if return_metric:
+        return list_center, list_metric
+    return opt_center
+
+
+def find_center_based_slice_metric(sinogram, start, stop, step=0.5,
+                                   metric="entropy", radius=2, zoom=1.0,
+                                   method="fbp", gpu=True, angles=None,
+                                   ratio=1.0, filter_name="hann",
+                                   apply_log=True, ncore=None, sigma=2,
+                                   invert_metric=False, metric_function=None,
+                                   **kwargs):
+    """Centre of rotation from slice metrics; ``reconstruction.py:1349-1458``.
+
+    A coarse pass at unit steps on the sinogram zoomed by ``zoom`` (device
+    linear zoom), then a fine pass at ``step`` within ``radius`` of the
+    coarse centre.  Metrics: ``"entropy"`` (histogram entropy) or
+    ``"sharpness"``; a custom ``metric_function(recon, **kwargs)`` must be
+    smallest at the best centre.
+    """
+    import scipy.ndimage as ndi
+    zoom = np.clip(zoom, 0.01, 1.0)
+    angles_zoom = angles
+    t, _ = R._to_device(sinogram)
+    sino_zoom = t.clone() if t is sinogram else t
+    if zoom < 1.0:
+        sino_zoom = zoom_image(t, zoom)
+        start, stop = start * zoom, stop * zoom
+        if angles is not None:
+            # the angle table is host setup: scipy's own 1-D zoom
+            a = angles.detach().cpu().numpy() if isinstance(
+                angles, torch.Tensor) else np.asarray(angles)
+            angles_zoom = ndi.zoom(np.tile(a, (1, 1)), (1.0, zoom))[0]
+    del t
+    kw = dict(metric=metric, method=method, gpu=gpu, ratio=ratio,
+              filter_name=filter_name, apply_log=apply_log, ncore=ncore,
+              sigma=sigma, return_metric=False, invert_metric=invert_metric,
+              metric_function=metric_function)
+    if stop > start:
+        coarse_center = _find_center_based_slice_metric(
+            sino_zoom, start, stop + 1, 1.0, angles=angles_zoom, **kw,
+            **kwargs)
+        coarse_center = coarse_center / zoom
+    else:
+        coarse_center = start / zoom
+    del sino_zoom
+    if radius != 0.0:
+        radius = max(radius, step + 1.0 / zoom)
+        start, stop = coarse_center - radius, coarse_center + radius + step
+        center = _find_center_based_slice_metric(sinogram, start, stop, step,
+                                                 angles=angles, **kw,
+                                                 **kwargs)
+    else:
+        center = coarse_center
+    return center

@@ -529,3 +529,9 @@ def bpf_reconstruction(sinogram, center, angles=None, ratio=1.0,
     rec = filt.permute(1, 0, 2)
     return _finish(rec, two_d, is_np, out,
                    np.float64 if two_d else np.float32)
+
+
+# centre search by slice metrics (reconstruction.py:1254-1458), kept in this
+# module's namespace like the reference's
+from .center import (find_center_based_slice_metric,  # noqa: E402,F401
+                     _find_center_based_slice_metric)

@@ -58,14 +58,16 @@ def _args():
                     choices=["float32", "float16", "bfloat16"],
                     help="element type of the filtered sinogram (stack)")
     ap.add_argument("--workload", default="stack",
-                    choices=["stack", "batch", "single", "bpf", "volume"],
+                    choices=["stack", "batch", "single", "bpf", "volume",
+                             "center"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
                          "/ bfloat16 filtered storage and errors on 16 sampled "
                          "slices; batch: "
                          "64 uneven sinograms in one persistent launch under "
-                         "a CUDA graph; single: one 1024^2 x 900 slice")
+                         "a CUDA graph; single: one 1024^2 x 900 slice; "
+                         "center: centre search over 128 candidates")
     return ap.parse_args()
 
 
@@ -604,8 +606,117 @@ def run_volume(args):
     print(json.dumps(out), flush=True)
 
 
+def run_center(args):
+    """Centre search on one benchmark slice (1801 angles x 2560 det, centre
+    1278.3): the entropy metric of 128 candidate centres at step 0.25
+    through ``_find_center_based_slice_metric`` (Gaussian smoothing sigma 2,
+    one ramp filter, a batched back-projection of all candidates, device
+    metrics), from a device tensor (``value``) and from a host NumPy array
+    (``e2e``); plus the two-pass ``find_center_based_slice_metric`` (coarse
+    zoom 0.5, +/-16 px).  CPU baseline: the oracle port's reference-
+    arithmetic FBP and the metric on 2 candidates (plus the normalisation
+    image); its metrics also check the device ones."""
+    import torch
+    from algotom_b200 import phantom
+    from algotom_b200.rec import center as CC
+    from algotom_b200.rec import reconstruction as R
+    dev = torch.device("cuda", 0)
+    ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
+    s, _, _ = phantom.ellipse_sinogram(2000, NROW, NCOL, CENTER,
+                                       photons=PHOTONS, angles=ang)
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    host = torch.from_numpy(s).pin_memory()
+    sdev = host.to(dev)
+    ncand, step = 128, 0.25
+    start = CENTER - 16.0
+    stop = start + (ncand - 0.5) * step
+    kw = dict(angles=ang, apply_log=False, sigma=2, metric="entropy",
+              return_metric=True)
+
+    def timed(src, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            res = R._find_center_based_slice_metric(src, start, stop, step,
+                                                    **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / n, res
+
+    for _ in range(args.warmup):
+        timed(sdev, 1)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t_dev, (cs, ms) = timed(sdev, args.steps)
+    t_e2e, _ = timed(host.numpy(), args.steps)
+    clocks = sampler.stop()
+    assert len(cs) == ncand
+    upd = ncand * NCOL * NCOL * NROW
+    # two-pass search (coarse on the half-size sinogram, fine at 0.25)
+    t0 = time.perf_counter()
+    found = R.find_center_based_slice_metric(sdev, CENTER - 16, CENTER + 16,
+                                             step=0.25, zoom=0.5, angles=ang,
+                                             apply_log=False)
+    t_find = time.perf_counter() - t0
+    cpu = acc = None
+    if not args.no_oracle:
+        from oracle import center_oracle as CO
+        from oracle import cpu_port
+        nt = cpu_port.max_threads()
+        sm = CC.gaussian_filter_rows(sdev, 2).cpu().numpy()
+        picks = [int(np.argmin(ms)), 0]
+        t0 = time.perf_counter()
+        mean_img = cpu_port.fbp_reconstruction(sm[:, None, :],
+                                               float(np.mean(cs)), ang,
+                                               nthreads=nt)[:, 0, :]
+        nmin, nmax = np.min(mean_img), np.max(mean_img)
+        ref = []
+        for k in picks:
+            img = cpu_port.fbp_reconstruction(sm[:, None, :], float(cs[k]),
+                                              ang, nthreads=nt)[:, 0, :]
+            ref.append(CO.histogram_entropy(CO.normalise_u8(img, nmin,
+                                                            nmax)))
+        t_cpu = time.perf_counter() - t0
+        cpu = {"value": (len(picks) + 1) * NCOL * NCOL * NROW / t_cpu,
+               "unit": "updates/s", "cores": nt, "kind": "port",
+               "sample": "%d FBPs of one 1801 x 2560 slice (normalisation "
+                         "image + 2 candidates), reference arithmetic, "
+                         "%.1f s" % (len(picks) + 1, t_cpu)}
+        acc = {"metric_rel_diff_vs_port": max(
+            abs(ms[k] - r) / abs(r) for k, r in zip(picks, ref)),
+            "candidates_checked": len(picks)}
+    print(json.dumps({
+        "metric": "centre-search pixel-angle updates/s at 2560 det "
+                  "(candidate reconstructions + entropy metric)",
+        "value": upd / t_dev, "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_dev * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 12-ellipse phantom, Poisson 5e3)",
+        "config": {"workload": "centre search: 128 candidates x 1801 angles "
+                               "x 2560^2, step 0.25, entropy, sigma 2",
+                   "candidates": ncand},
+        "candidates_per_s": ncand / t_dev,
+        "e2e": {"value": upd / t_e2e, "unit": "updates/s",
+                "h2d_bytes_per_step": int(s.nbytes),
+                "d2h_bytes_per_step": 8 * ncand + 8,
+                "ms_per_step": t_e2e * 1e3},
+        "find_center": {"seconds": t_find, "center": float(found),
+                        "true_center": CENTER},
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
+        # per step: Gaussian rows, row filter, normalisation image
+        # (batched back-projection + 2 range kernels), candidates (batched
+        # back-projection, histogram, entropy)
+        "gpu_launches": 8 * args.steps}), flush=True)
+
+
 def main():
     args = _args()
+    if args.workload == "center":
+        run_center(args)
+        return
     if args.workload == "volume":
         run_volume(args)
         return

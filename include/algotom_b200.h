@@ -49,6 +49,10 @@ extern "C" {
 #define ATB_PAD_MINIMUM 8
 #define ATB_PAD_MEDIAN 9
 
+/* slice metrics of the centre search */
+#define ATB_METRIC_ENTROPY 0
+#define ATB_METRIC_SHARPNESS 1
+
 /* Library version as major*10000 + minor*100 + patch. */
 int atb_version(void);
 
@@ -245,6 +249,65 @@ int atb_backproject_batch(const atb_bp_item *items, int nitems,
  */
 int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems,
                                   int max_ctas, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Centre search by slice metrics (find_center_based_slice_metric,        */
+/* algotom/rec/reconstruction.py:1212-1458).  The candidate centres are   */
+/* reconstructed by one atb_backproject_batch launch whose items share    */
+/* the filtered sinogram; these entry points cover the steps around it.   */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * scipy.ndimage.gaussian_filter1d(x, sigma, axis=1) of float32 rows, mode
+ * "reflect"; replaces the smoothing of the sinogram before a search
+ * (reconstruction.py:1317-1318).  Same float32 results as scipy.
+ *
+ *   weights   device float64 [radius + 1]: the half kernel w[0..radius] of
+ *             the unit-sum sampled Gaussian, radius = int(4 sigma + 0.5)
+ *   dst       must not overlap src; radius <= 8192, nrow <= 65535
+ */
+int atb_gaussian_rows(const float *src, int64_t src_row_stride, int nrow,
+                      int ncol, const double *weights, int radius,
+                      float *dst, int64_t dst_row_stride, void *stream);
+
+/*
+ * scipy.ndimage.zoom(x, zoom, order=1, mode="nearest") of a float32 image
+ * to out_rows x out_cols (the caller computes round(n * zoom)); replaces
+ * the coarse-search resize (reconstruction.py:1426-1428).  Same float32
+ * results as scipy.  out_rows <= 65535.
+ */
+int atb_zoom_linear(const float *src, int64_t src_row_stride, int in_rows,
+                    int in_cols, float *dst, int64_t dst_row_stride,
+                    int out_rows, int out_cols, void *stream);
+
+/*
+ * out2 = (min, max) of a float32 image (both NaN if any pixel is NaN), the
+ * entropy normalisation range (reconstruction.py:1327-1330).
+ *
+ *   work   device scratch of 12 bytes
+ *   out2   device float32 [2]
+ */
+int atb_image_range(const float *img, int64_t row_stride, int rows, int cols,
+                    void *work, float *out2, void *stream);
+
+/* Bytes of device scratch atb_slice_metric needs (0 for a bad argument). */
+int64_t atb_slice_metric_workspace(int nimg, int rows, int cols, int metric);
+
+/*
+ * One metric per image of a batch: ATB_METRIC_ENTROPY, the histogram
+ * entropy of the image normalised by (nmin, nmax) to uint8 levels
+ * (reconstruction.py:1212-1221 with the normalisation of :1243-1245), or
+ * ATB_METRIC_SHARPNESS, the mean gradient magnitude (:1224-1229; needs
+ * rows, cols >= 2).  Deterministic.
+ *
+ *   imgs      float32 [nimg] images of rows x cols at img_stride, row_stride
+ *   work      device scratch of atb_slice_metric_workspace() bytes
+ *   out       device float64 [nimg]
+ */
+int atb_slice_metric(const float *imgs, int64_t img_stride,
+                     int64_t row_stride, int nimg, int rows, int cols,
+                     int metric, float nmin, float nmax, void *work,
+                     int64_t work_bytes, double *out, void *stream);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,7 @@ sys.path.insert(0, REF)
 sys.path.insert(0, REPO)
 
 import scipy.ndimage as ndi  # noqa: E402
+import scipy.signal as ssig  # noqa: E402
 import algotom.rec.reconstruction as rec  # noqa: E402
 import algotom.util.utility as util  # noqa: E402
 from algotom_b200 import phantom  # noqa: E402
@@ -169,12 +170,93 @@ def make_reference_test_fixture():
     np.savez_compressed(os.path.join(HERE, "golden_unittest.npz"), **out)
 
 
+def make_center():
+    """Centre search by slice metrics (reconstruction.py:1212-1458).
+
+    The reference's own pre-steps on fixed inputs (Gaussian smoothing along
+    the detector, linear zoom, the two metrics), the metric of every
+    candidate centre of ``_find_center_based_slice_metric`` and the centre
+    chosen by ``find_center_based_slice_metric`` (FBP and BPF methods).
+    """
+    entropy = getattr(rec, "__calculate_histogram_entropy")
+    sharp = getattr(rec, "__calculate_edge_sharpness")
+    n, nrow, cen = 96, 91, 46.3
+    sino, ang, _ = phantom.ellipse_sinogram(41, nrow, n, cen, photons=2e4)
+    trans = np.exp(-sino).astype(np.float32)
+    trans[7, 11] = 0.0
+    out = {"sino": sino, "trans": trans, "angles": ang,
+           "center": np.float64(cen)}
+    # pre-steps
+    for sigma in (1, 2, 3.5):
+        out[_key("gauss", sigma)] = ndi.gaussian_filter1d(sino, sigma, axis=1)
+    narrow = sino[:, 40:45].copy()
+    out["narrow"] = narrow
+    out[_key("gauss", "narrow", 2)] = ndi.gaussian_filter1d(narrow, 2,
+                                                             axis=1)
+    for z in (0.5, 0.8, 0.33):
+        out[_key("zoom", z)] = ndi.zoom(sino, z, order=1, mode="nearest")
+        out[_key("zoom", "angles", z)] = ndi.zoom(np.tile(ang, (1, 1)),
+                                                  (1.0, z))[0]
+    # metrics of fixed images (the reconstruction at the true centre)
+    img = rec.fbp_reconstruction(sino.copy(), cen, angles=ang,
+                                 apply_log=False, gpu=False)
+    nmin, nmax = np.min(img), np.max(img)
+    img1 = np.clip((img - nmin) / (nmax - nmin), 0, 1)
+    out["metric_img"] = img
+    out[_key("metric", "entropy")] = np.float64(
+        entropy(img1, ssig.windows.boxcar(7)))
+    out[_key("metric", "sharpness")] = np.float64(sharp(img))
+    # every candidate's metric
+    f = rec._find_center_based_slice_metric
+    cases = {
+        "fbp_entropy": dict(metric="entropy", method="fbp", sigma=2,
+                            ratio=1.0),
+        "fbp_sharp": dict(metric="sharpness", method="fbp", sigma=0,
+                          ratio=1.0),
+        "fbp_entropy_r0": dict(metric="entropy", method="fbp", sigma=1,
+                               ratio=0.0),
+        "fbp_entropy_nomask": dict(metric="entropy", method="fbp", sigma=2,
+                                   ratio=None),
+        "bpf_entropy": dict(metric="entropy", method="bpf", sigma=2,
+                            ratio=1.0),
+        "bpf_sharp": dict(metric="sharpness", method="bpf", sigma=2,
+                          ratio=1.0),
+    }
+    for name, kw in cases.items():
+        cs, ms = f(sino.copy(), cen - 3, cen + 3, 0.5, angles=ang,
+                   apply_log=False, gpu=False, ncore=1, return_metric=True,
+                   **kw)
+        out[_key("list", name, "centers")] = cs
+        out[_key("list", name, "metrics")] = ms
+    cs, ms = f(trans.copy(), cen - 2, cen + 2, 1.0, angles=ang,
+               apply_log=True, gpu=False, ncore=1, return_metric=True)
+    out[_key("list", "log", "centers")] = cs
+    out[_key("list", "log", "metrics")] = ms
+    # chosen centres of the two-pass search
+    g = rec.find_center_based_slice_metric
+    finds = {
+        "z1": dict(zoom=1.0, angles=ang),
+        "z05": dict(zoom=0.5, angles=ang),
+        "z08_default_angles": dict(zoom=0.8, angles=None),
+        "sharp": dict(zoom=1.0, angles=ang, metric="sharpness"),
+        "bpf": dict(zoom=1.0, angles=ang, method="bpf"),
+        "r0": dict(zoom=1.0, angles=ang, radius=0.0),
+    }
+    for name, kw in finds.items():
+        out[_key("find", name)] = np.float64(g(
+            sino.copy(), cen - 6, cen + 6, step=0.25, gpu=False,
+            apply_log=False, ncore=1, **kw))
+    np.savez_compressed(os.path.join(HERE, "golden_center.npz"), **out)
+
+
+GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
+              "recon": make_recon, "unittest": make_reference_test_fixture,
+              "center": make_center}
+
 if __name__ == "__main__":
-    make_windows()
-    make_filter()
-    make_bp()
-    make_recon()
-    make_reference_test_fixture()
+    # python make_golden.py [name ...]  (default: every fixture)
+    for name in (sys.argv[1:] or list(GENERATORS)):
+        GENERATORS[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
