@@ -17,9 +17,9 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
            "atb_backproject_batch_noalloc", "atb_gaussian_rows",
            "atb_zoom_linear", "atb_image_range", "atb_slice_metric_workspace",
-           "atb_slice_metric")
+           "atb_slice_metric", "atb_vertical_backproject", "atb_flat_log")
 
-F32, F16, BF16 = 0, 1, 2
+F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
 PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
              "wrap": 4, "linear_ramp": 5, "mean": 6, "maximum": 7,
@@ -83,6 +83,14 @@ _SIGS = {
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, ctypes.c_float, ctypes.c_float, _vp, _c_i64, _vp,
         _vp]),
+    "atb_vertical_backproject": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+        ctypes.c_int, _vp, _c_i64, _c_i64, _vp]),
+    "atb_flat_log": (ctypes.c_int, [
+        _vp, ctypes.c_int, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, _vp, _vp, _c_i64, ctypes.c_int, _vp, _c_i64, _c_i64,
+        _vp, _vp]),
 }
 
 _lib = None

@@ -41,6 +41,7 @@ __device__ __forceinline__ float load_as_float(const __nv_bfloat16 *p) {
 __device__ __forceinline__ float to_float(float v) { return v; }
 __device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
 __device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_float(unsigned short v) { return (float)v; }
 
 // two floats as one 32-bit word of two 16-bit values (first in the low half)
 template <typename T> __device__ __forceinline__ unsigned pack_pair(float lo, float hi);

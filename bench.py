@@ -59,7 +59,7 @@ def _args():
                     help="element type of the filtered sinogram (stack)")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
-                             "center"],
+                             "center", "vertical"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
@@ -67,7 +67,8 @@ def _args():
                          "slices; batch: "
                          "64 uneven sinograms in one persistent launch under "
                          "a CUDA graph; single: one 1024^2 x 900 slice; "
-                         "center: centre search over 128 candidates")
+                         "center: centre search over 128 candidates; "
+                         "vertical: vertical slices from 1801 projections")
     return ap.parse_args()
 
 
@@ -712,8 +713,113 @@ def run_center(args):
         "gpu_launches": 8 * args.steps}), flush=True)
 
 
+def run_vertical(args):
+    """Vertical slices from a projection stack of 1801 x 512 x 2560 float32
+    (the benchmark's 512 slices read as projections, 9.4 GB, device-
+    resident): one vertical slice through the middle at 30 degrees
+    (``vertical_reconstruction``, ramp filter after, chunks of 30
+    projections) and 64 parallel slices 32 px apart
+    (``vertical_reconstruction_multiple``).  The single slice reads every
+    projection byte once: its roofline is HBM.  e2e: the single slice from
+    a pinned host array (9.4 GB host-to-device per step).  CPU baseline: the
+    FP64 oracle's vertical back-projection on 4 detector rows; accuracy: the
+    device slice against the FP64 oracle on those rows."""
+    import torch
+    from algotom_b200.rec import vertrec as VR
+    dev = torch.device("cuda", 0)
+    height = 512
+    proj, ang = make_sinograms(height, dev)  # [1801][512][2560]
+    torch.cuda.synchronize()
+    kw = dict(angles=ang, apply_log=False, show_progress=False)
+
+    def single(src):
+        return VR.vertical_reconstruction(src, NCOL // 2, CENTER, alpha=30.0,
+                                          **kw)
+
+    def multi(src):
+        return VR.vertical_reconstruction_multiple(src, 256, 256 + 63 * 32,
+                                                   CENTER, alpha=30.0,
+                                                   step_index=32, **kw)
+
+    def timed(fn, src, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            r = fn(src)
+            del r
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / n
+
+    for _ in range(args.warmup):
+        single(proj)
+        multi(proj)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t1 = timed(single, proj, args.steps)
+    t64 = timed(multi, proj, args.steps)
+    clocks = sampler.stop()
+    t_e2e = None
+    nbytes = proj.numel() * 4
+    if not args.no_e2e:
+        host = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+        host.copy_(proj)
+        single(host.numpy())
+        t_e2e = timed(single, host.numpy(), max(1, args.steps // 2))
+        del host
+    upd1 = NROW * height * NCOL
+    pk, src = _peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    acc = cpu = None
+    if not args.no_oracle:
+        from oracle import fbp_oracle as O
+        from oracle import vertical_oracle as VO
+        rows = [0, 100, 300, 511]
+        sub = proj[:, rows, :].cpu().numpy()
+        xs, ys = VO.points_single_line(NCOL // 2, 30.0, NCOL)
+        t0 = time.perf_counter()
+        bp = VO.vertical_back_projection(sub, ang, xs, ys, CENTER, True)
+        t_cpu = time.perf_counter() - t0
+        ref = VO.ver_ramp_filter(bp, "hann", 150, "edge") * np.pi / (NROW - 1)
+        got = single(proj)[rows].cpu().numpy()
+        acc = {"rel_l2_vs_fp64_oracle": O.rel_l2(got, ref),
+               "rows_checked": len(rows)}
+        cpu = {"value": len(rows) * NROW * NCOL / t_cpu, "unit": "updates/s",
+               "cores": 1, "kind": "port",
+               "sample": "FP64 NumPy vertical back-projection of %d detector "
+                         "rows, %.1f s" % (len(rows), t_cpu)}
+    print(json.dumps({
+        "metric": "vertical-slice FBP pixel-angle updates/s at 2560 det",
+        "value": upd1 / t1, "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t1 * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded 12-ellipse phantoms)",
+        "config": {"workload": "vertical slice at 30 deg through 1801 "
+                               "projections of 512 x 2560 (device-resident)",
+                   "l2": "inputs larger than L2 (9.4 GB)"},
+        "roofline": {"bound": "hbm", "achieved": nbytes / t1 / 1e9,
+                     "peak": hbm, "unit": "GB/s",
+                     "frac": nbytes / t1 / 1e9 / hbm, "traffic": None,
+                     "bytes": "projections read once per step",
+                     "peak_source": src},
+        "multiple_64": {"value": 64 * upd1 / t64, "unit": "updates/s",
+                        "ms_per_step": t64 * 1e3},
+        "e2e": None if t_e2e is None else {
+            "value": upd1 / t_e2e, "unit": "updates/s",
+            "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": height * NCOL * 8,
+            "ms_per_step": t_e2e * 1e3},
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
+        "gpu_launches": None}), flush=True)
+
+
 def main():
     args = _args()
+    if args.workload == "vertical":
+        run_vertical(args)
+        return
     if args.workload == "center":
         run_center(args)
         return

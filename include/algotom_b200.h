@@ -36,6 +36,7 @@ extern "C" {
 #define ATB_F32 0
 #define ATB_F16 1
 #define ATB_BF16 2
+#define ATB_U16 3  /* raw detector counts (atb_flat_log input only) */
 
 /* numpy.pad modes along the detector axis (reconstruction.py:146) */
 #define ATB_PAD_EDGE 0
@@ -308,6 +309,56 @@ int atb_slice_metric(const float *imgs, int64_t img_stride,
                      int64_t row_stride, int nimg, int rows, int cols,
                      int metric, float nmin, float nmax, void *work,
                      int64_t work_bytes, double *out, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Vertical slices (algotom/rec/vertrec.py)                               */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Back-projection of projections onto vertical slices; replaces
+ * vertical_back_projection_cpu / vertical_back_projection_gpu
+ * (vertrec.py:53-109, 175-252) and their _chunk forms for several slices
+ * (vertrec.py:112-172, 255-335).  Slice s is a line of npts points
+ * (x, y) in the horizontal plane; for every detector row i and point j
+ *
+ *   acc[s][i][j] += sum_n value(proj[n][i][.], x cos a_n + y sin a_n + center)
+ *
+ * with the reference's interpolation, inclusive bounds [0, width-1] and
+ * optional edge padding.  Positions in FP64, interpolation FP32, sums over
+ * 32 angles FP32, accumulation FP64.
+ *
+ *   proj    float32 [nproj][height][width] at proj_stride / row_stride
+ *   trig    float64 [nproj][2] = (cos a, sin a)  (note: +a, not -a)
+ *   points  float64 [nline][npts][2] = (x, y), line_stride between lines
+ *           (in points)
+ *   acc     float64 [nline][height][npts], added to (not overwritten)
+ */
+int atb_vertical_backproject(const float *proj, int64_t proj_stride,
+                             int64_t row_stride, int nproj, int height,
+                             int width, const double *trig,
+                             const double *points, int64_t line_stride,
+                             int npts, int nline, double center, int edge_pad,
+                             double *acc, int64_t acc_line_stride,
+                             int64_t acc_row_stride, void *stream);
+
+/*
+ * Flat-field correction and -log of a chunk of projections; replaces the
+ * pre-step of vertical_reconstruction* (vertrec.py:594-606):
+ *   v = (src - dark) / flat_dark   (when dark / flat_dark are given)
+ *   v = -log(v), values <= 0 replaced by 1 first (when apply_log)
+ * in float32.  *nonpos (device, not cleared) is increased by the number of
+ * replaced values, for the reference's warning.
+ *
+ *   src        ATB_F32 or ATB_U16 [nproj][height][width]
+ *   dark, flat_dark  float32 [height][width] at field_row_stride, both or
+ *              neither (flat_dark = flat - dark with zeros set to 1)
+ */
+int atb_flat_log(const void *src, int src_dtype, int64_t src_proj_stride,
+                 int64_t src_row_stride, int nproj, int height, int width,
+                 const float *dark, const float *flat_dark,
+                 int64_t field_row_stride, int apply_log, float *dst,
+                 int64_t dst_proj_stride, int64_t dst_row_stride,
+                 unsigned *nonpos, void *stream);
 
 #ifdef __cplusplus
 }

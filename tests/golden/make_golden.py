@@ -249,9 +249,80 @@ def make_center():
     np.savez_compressed(os.path.join(HERE, "golden_center.npz"), **out)
 
 
+def make_vertical():
+    """Vertical slices (algotom/rec/vertrec.py): the back-projectors, the
+    slice geometry and the three chunked reconstructions, CPU path."""
+    import algotom.rec.vertrec as vrec
+    nproj, height, width, cen = 73, 10, 64, 31.7
+    ang = np.deg2rad(np.linspace(0.0, 180.0, nproj))
+    att = np.zeros((nproj, height, width), np.float32)
+    for i in range(height):
+        att[:, i, :] = phantom.ellipse_sinogram(60 + i, nproj, width, cen,
+                                                photons=None, angles=ang)[0]
+    trans = np.exp(-att).astype(np.float32)
+    rng = np.random.default_rng(7)
+    flat = (1.0 + 0.05 * rng.random((height, width))).astype(np.float32)
+    dark = (0.01 * rng.random((height, width))).astype(np.float32)
+    raw = (trans * (flat - dark) + dark).astype(np.float32)
+    out = {"att": att, "trans": trans, "angles": ang, "flat": flat,
+           "dark": dark, "raw": raw, "center": np.float64(cen)}
+    for w in (64, 65, 9):
+        for idx, alpha in ((0, 0.0), (w // 2, 30.0), (w - 1, 45.0),
+                           (w // 3, 60.0), (w // 2, 90.0), (1, 135.0),
+                           (w - 2, 150.0), (w // 2, 180.0)):
+            xs, ys = vrec._get_points_single_line(idx, alpha, w)
+            out[_key("pts", w, idx, alpha, "x")] = xs
+            out[_key("pts", w, idx, alpha, "y")] = ys
+    lines = ((32, 0.0), (20, 30.0), (40, 60.0), (10, 90.0), (50, 150.0))
+    for idx, alpha in lines:
+        xs, ys = vrec._get_points_single_line(idx, alpha, width)
+        for ep in (False, True):
+            out[_key("vbp", idx, alpha, ep)] = vrec.vertical_back_projection_cpu(
+                att, ang, xs, ys, cen, edge_pad=ep)
+    xm, ym = vrec._get_points_multiple_lines(20, 44, 45.0, width, 8)
+    out["xm"], out["ym"] = xm, ym
+    for ep in (False, True):
+        out[_key("vbpchunk", ep)] = vrec.vertical_back_projection_cpu_chunk(
+            att, ang, xm, ym, cen, edge_pad=ep)
+    common = dict(gpu=False, show_progress=False, ncore=1)
+    rec_cases = {
+        "after": dict(),
+        "before": dict(ramp_filter="before"),
+        "none": dict(ramp_filter=None),
+        "crop_range": dict(crop=(1, 2, 3, 4), proj_start=2, proj_stop=70,
+                           chunk_size=16, masking=True),
+        "flat": dict(flat_field=flat, dark_field=dark, chunk_size=20,
+                     ramp_filter="before", pad=10, pad_mode="reflect"),
+        "alpha": dict(alpha=70.0, filter_name="hamming", chunk_size=None),
+    }
+    for name, kw in rec_cases.items():
+        src = raw if "flat_field" in kw else trans
+        a = ang[2:70] if "proj_stop" in kw else ang
+        out[_key("vrec", name)] = vrec.vertical_reconstruction(
+            src.copy(), 30, cen - (3 if "crop" in kw else 0), angles=a,
+            **kw, **common)
+    out["vrec_multi"] = vrec.vertical_reconstruction_multiple(
+        trans.copy(), 20, 40, cen, alpha=45.0, step_index=5, angles=ang,
+        chunk_size=25, **common)
+    out["vrec_diff"] = vrec.vertical_reconstruction_different_angles(
+        trans.copy(), [10, 30, 50], [0.0, 60.0, 120.0], cen, angles=ang,
+        ramp_filter="before", chunk_size=30, masking=True, **common)
+    bad = trans.copy()
+    bad[5, 3, 7] = 0.0
+    bad[40, 8, 20] = -1.0
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        out["vrec_log"] = vrec.vertical_reconstruction(
+            bad, 30, cen, angles=ang, chunk_size=30, **common)
+    out["vrec_log_warnings"] = np.array([str(w.message) for w in caught
+                                         if "logarithm" in str(w.message)])
+    out["vrec_log_mutated"] = bad
+    np.savez_compressed(os.path.join(HERE, "golden_vertical.npz"), **out)
+
+
 GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
               "recon": make_recon, "unittest": make_reference_test_fixture,
-              "center": make_center}
+              "center": make_center, "vertical": make_vertical}
 
 if __name__ == "__main__":
     # python make_golden.py [name ...]  (default: every fixture)
