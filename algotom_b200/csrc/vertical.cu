@@ -19,10 +19,13 @@
 // Interpolation is FP32; the sums over each table's 32 angles are FP32
 // partials, folded into FP64 registers and finally added to a caller FP64
 // accumulator, so that chunks of projections streamed through the device
-// sum without FP32 rounding across chunks.  The grid runs all (line, point
-// block) CTAs of one row block next to each other, so a row block's
-// projection rows are read from HBM about once per launch however many
-// lines share them.
+// sum without FP32 rounding across chunks.  When the tile grid alone would
+// not fill the GPU, the angles are also split over CTAs (grid z): each group
+// writes its FP64 partial sums to caller scratch and a second kernel adds
+// the groups in a fixed order, so results do not depend on scheduling.  The
+// grid runs all (line, point block) CTAs of one row block next to each
+// other, so a row block's projection rows are read from HBM about once per
+// angle group however many lines share them.
 #include <cmath>
 
 #include "common.cuh"
@@ -47,6 +50,8 @@ struct VArgs {
   int edge_pad;
   double *acc;
   long long als, ars;  // accumulator line / row strides
+  int apg;             // angles per group (blockIdx.z)
+  double *part;        // group partials [ngroups][nline][height][npts], or null
 };
 
 // table entry: bin d and fraction f >= 0 (f == 0: the single sample y[d]),
@@ -56,7 +61,35 @@ struct __align__(8) VPos {
   float f;
 };
 
-__global__ void __launch_bounds__(kThreads) vbp_kernel(VArgs a) {
+__device__ __forceinline__ VPos make_pos(const VArgs &a, const double2 *pts, int n, int je) {
+  VPos v = {0, -1.0f};
+  const double2 cs = a.trig[n];
+  const double2 xy = pts[je];
+  // same expression and rounding order as the reference: (x cos + y sin) + center
+  const double p = __dadd_rn(__dadd_rn(__dmul_rn(xy.x, cs.x), __dmul_rn(xy.y, cs.y)), a.center);
+  const int width1 = a.width - 1;
+  if (p >= 0.0 && p <= (double)width1) {
+    const double fl = floor(p);
+    v.d = (int)fl;
+    v.f = (float)(p - fl);  // exact difference; 0 when u == d
+  } else if (a.edge_pad) {
+    v.d = p < 0.0 ? 0 : width1;
+    v.f = 0.0f;
+  }
+  return v;
+}
+
+// the two samples of entry v in one row (both y[d] when f == 0; nothing
+// read when f < 0)
+__device__ __forceinline__ void taps(const float *row, VPos v, float &y0, float &y1) {
+  y0 = y1 = 0.0f;
+  if (v.f >= 0.0f) {
+    y0 = __ldg(row + v.d);
+    y1 = __ldg(row + (v.f > 0.0f ? v.d + 1 : v.d));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 3) vbp_kernel(VArgs a) {
   __shared__ VPos tab[kAng][kPts];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int line = blockIdx.x / a.npb, pb = blockIdx.x - line * a.npb;
@@ -64,54 +97,61 @@ __global__ void __launch_bounds__(kThreads) vbp_kernel(VArgs a) {
   const int pl = lane + 32 * (warp & 1);  // this thread's point in the block
   const int j = j0 + pl;
   const int r0 = blockIdx.y * kRows + (warp >> 1) * kRowsPerThread;
-  const int width1 = a.width - 1;
+  const int nr = min(kRowsPerThread, a.height - r0);  // live rows (may be <= 0)
   const double2 *pts = a.points + line * a.pls;
+  const int g0 = blockIdx.z * a.apg, g1 = min(a.nproj, g0 + a.apg);
+  // 32-bit row offsets: one projection holds fewer than 2^31 samples
+  int roff[kRowsPerThread];
+#pragma unroll
+  for (int r = 0; r < kRowsPerThread; ++r) roff[r] = r < nr ? (r0 + r) * (int)a.rs : 0;
   double acc[kRowsPerThread];
 #pragma unroll
   for (int r = 0; r < kRowsPerThread; ++r) acc[r] = 0.0;
 
-  for (int n0 = 0; n0 < a.nproj; n0 += kAng) {
-    const int nang = min(kAng, a.nproj - n0);
+  for (int n0 = g0; n0 < g1; n0 += kAng) {
+    const int nang = min(kAng, g1 - n0);
     __syncthreads();  // the previous table is no longer read
     for (int e = tid; e < kAng * kPts; e += kThreads) {
       const int an = e / kPts, pe = e - an * kPts, je = j0 + pe;
-      VPos v = {0, -1.0f};
-      if (an < nang && je < a.npts) {
-        const double2 cs = a.trig[n0 + an];
-        const double2 xy = pts[je];
-        // same expression and rounding order as the reference:
-        // (x cos + y sin) + center
-        const double p = __dadd_rn(__dadd_rn(__dmul_rn(xy.x, cs.x), __dmul_rn(xy.y, cs.y)), a.center);
-        if (p >= 0.0 && p <= (double)width1) {
-          const double fl = floor(p);
-          v.d = (int)fl;
-          v.f = (float)(p - fl);  // exact difference; 0 when u == d
-        } else if (a.edge_pad) {
-          v.d = p < 0.0 ? 0 : width1;
-          v.f = 0.0f;
-        }
-      }
-      tab[an][pe] = v;
+      tab[an][pe] = (an < nang && je < a.npts) ? make_pos(a, pts, n0 + an, je) : VPos{0, -1.0f};
     }
     __syncthreads();
-    if (j < a.npts) {
+    if (j < a.npts && nr > 0) {
       // FP32 partial sums over this table's angles, folded into FP64 below
       float part[kRowsPerThread];
 #pragma unroll
       for (int r = 0; r < kRowsPerThread; ++r) part[r] = 0.0f;
-#pragma unroll 2
-      for (int an = 0; an < nang; ++an) {
-        const VPos v = tab[an][pl];
-        if (v.f < 0.0f) continue;
-        const int d1 = v.f > 0.0f ? v.d + 1 : v.d;
-        const float *base = a.proj + (long long)(n0 + an) * a.ps;
+      const float *base = a.proj + (long long)n0 * a.ps;
+      int an = 0;
+      for (; an + 1 < nang; an += 2, base += 2 * a.ps) {
+        // both angles' samples are requested before any is used
+        const VPos v0 = tab[an][pl], v1 = tab[an + 1][pl];
+        float y[2][kRowsPerThread][2];
 #pragma unroll
         for (int r = 0; r < kRowsPerThread; ++r) {
-          const int i = r0 + r;
-          if (i < a.height) {
-            const float *row = base + (long long)i * a.rs;
-            const float y0 = __ldg(row + v.d), y1 = __ldg(row + d1);
-            part[r] += y0 + (y1 - y0) * v.f;
+          if (r < nr) {
+            taps(base + roff[r], v0, y[0][r][0], y[0][r][1]);
+            taps(base + a.ps + roff[r], v1, y[1][r][0], y[1][r][1]);
+          }
+        }
+        const float f0 = fmaxf(v0.f, 0.0f), f1 = fmaxf(v1.f, 0.0f);
+#pragma unroll
+        for (int r = 0; r < kRowsPerThread; ++r) {
+          if (r < nr) {
+            part[r] += y[0][r][0] + (y[0][r][1] - y[0][r][0]) * f0;
+            part[r] += y[1][r][0] + (y[1][r][1] - y[1][r][0]) * f1;
+          }
+        }
+      }
+      if (an < nang) {
+        const VPos v0 = tab[an][pl];
+        const float f0 = fmaxf(v0.f, 0.0f);
+#pragma unroll
+        for (int r = 0; r < kRowsPerThread; ++r) {
+          if (r < nr) {
+            float y0, y1;
+            taps(base + roff[r], v0, y0, y1);
+            part[r] += y0 + (y1 - y0) * f0;
           }
         }
       }
@@ -122,10 +162,41 @@ __global__ void __launch_bounds__(kThreads) vbp_kernel(VArgs a) {
   if (j < a.npts) {
 #pragma unroll
     for (int r = 0; r < kRowsPerThread; ++r) {
-      const int i = r0 + r;
-      if (i < a.height) a.acc[line * a.als + (long long)i * a.ars + j] += acc[r];
+      if (r < nr) {
+        const long long i = r0 + r;
+        if (a.part)
+          a.part[((long long)blockIdx.z * a.nline + line) * a.height * (long long)a.npts + i * a.npts + j] = acc[r];
+        else
+          a.acc[line * a.als + i * a.ars + j] += acc[r];
+      }
     }
   }
+}
+
+// acc += the angle groups' partial sums, added in group order
+__global__ void vbp_reduce_kernel(const double *__restrict__ part, int ngroups, int nline, int height, int npts,
+                                  double *acc, long long als, long long ars) {
+  const long long total = (long long)nline * height * npts;
+  const long long gs = total;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(e % npts);
+    const long long t = e / npts;
+    const int i = (int)(t % height), line = (int)(t / height);
+    double s = 0.0;
+    for (int g = 0; g < ngroups; ++g) s += part[g * gs + e];
+    acc[line * als + (long long)i * ars + j] += s;
+  }
+}
+
+// angle groups for a launch of `base` CTAs: enough for about four full
+// waves of 3 CTAs per SM, at least one 32-angle table per group
+int vbp_groups(int nproj, long long base) {
+  const long long want = 4LL * 148 * 3;
+  long long g = (want + base - 1) / base;
+  const long long gmax = (nproj + kAng - 1) / kAng;
+  if (g > gmax) g = gmax;
+  return (int)(g < 1 ? 1 : g);
 }
 
 // dst = -log((src - dark) / flat_dark) with the reference's <= 0 -> 1
@@ -159,11 +230,18 @@ __global__ void flat_log_kernel(const T *__restrict__ src, long long sps, long l
 
 }  // namespace
 
+extern "C" int64_t atb_vertical_workspace(int nproj, int height, int npts, int nline) {
+  if (nproj < 1 || height < 1 || npts < 1 || nline < 1) return 0;
+  const long long base = (long long)((npts + kPts - 1) / kPts) * nline * ((height + kRows - 1) / kRows);
+  const int g = vbp_groups(nproj, base);
+  return g > 1 ? (int64_t)g * nline * height * (int64_t)npts * (int64_t)sizeof(double) : 0;
+}
+
 extern "C" int atb_vertical_backproject(const float *proj, int64_t proj_stride, int64_t row_stride, int nproj,
                                         int height, int width, const double *trig, const double *points,
                                         int64_t line_stride, int npts, int nline, double center, int edge_pad,
-                                        double *acc, int64_t acc_line_stride, int64_t acc_row_stride,
-                                        void *stream) {
+                                        double *acc, int64_t acc_line_stride, int64_t acc_row_stride, void *work,
+                                        int64_t work_bytes, void *stream) {
   if (!proj || !trig || !points || !acc) return atb::fail(ATB_EINVAL, "atb_vertical_backproject: null pointer");
   if (nproj < 1 || height < 1 || width < 1 || npts < 1 || nline < 1)
     return atb::fail(ATB_EINVAL, "atb_vertical_backproject: bad shape nproj=%d height=%d width=%d npts=%d nline=%d",
@@ -172,6 +250,8 @@ extern "C" int atb_vertical_backproject(const float *proj, int64_t proj_stride, 
   if ((long long)npb * nline > 2147483647LL || nrb > 65535)
     return atb::fail(ATB_ERANGE, "atb_vertical_backproject: %d lines x %d points x %d rows too large", nline, npts,
                      height);
+  if ((long long)height * row_stride > 2147483647LL)
+    return atb::fail(ATB_ERANGE, "atb_vertical_backproject: one projection spans more than 2^31 samples");
   if (!std::isfinite(center)) return atb::fail(ATB_EINVAL, "atb_vertical_backproject: center is not finite");
   VArgs a;
   a.proj = proj; a.ps = proj_stride; a.rs = row_stride;
@@ -181,7 +261,23 @@ extern "C" int atb_vertical_backproject(const float *proj, int64_t proj_stride, 
   a.pls = line_stride; a.npts = npts; a.nline = nline; a.npb = npb;
   a.center = center; a.edge_pad = edge_pad ? 1 : 0;
   a.acc = acc; a.als = acc_line_stride; a.ars = acc_row_stride;
-  vbp_kernel<<<dim3(npb * nline, nrb), kThreads, 0, atb::as_stream(stream)>>>(a);
+  // split the angles over CTAs when the caller's scratch holds the partials
+  const long long elems = (long long)nline * height * npts;
+  int g = vbp_groups(nproj, (long long)npb * nline * nrb);
+  if (work == nullptr) g = 1;
+  while (g > 1 && (long long)g * elems * (long long)sizeof(double) > work_bytes) --g;
+  if (g > 65535) g = 65535;
+  a.apg = (nproj + g - 1) / g;
+  g = (nproj + a.apg - 1) / a.apg;
+  a.part = g > 1 ? static_cast<double *>(work) : nullptr;
+  cudaStream_t st = atb::as_stream(stream);
+  vbp_kernel<<<dim3(npb * nline, nrb, g), kThreads, 0, st>>>(a);
+  int rc = atb::check_launch("atb_vertical_backproject");
+  if (rc != ATB_OK || g == 1) return rc;
+  long long blocks = (elems + 255) / 256;
+  if (blocks > 148LL * 8) blocks = 148LL * 8;
+  vbp_reduce_kernel<<<(int)blocks, 256, 0, st>>>(a.part, g, nline, height, npts, acc, acc_line_stride,
+                                                  acc_row_stride);
   return atb::check_launch("atb_vertical_backproject");
 }
 

@@ -131,14 +131,19 @@ def _points(x_mat, y_mat, width, device, round32):
 
 def _backproject(proj, trig, pts, center, edge_pad, acc):
     """acc [nline, height, npts] += vertical back-projection of the float32
-    CUDA slab ``proj`` [n, height, width] (last axis contiguous)."""
+    CUDA slab ``proj`` [n, height, width] (last axis contiguous), with
+    scratch for the split of the angles over CTAs when the output is small."""
     n, height, width = proj.shape
     nline, npts = pts.shape[0], pts.shape[1]
+    nbytes = nat.call("atb_vertical_workspace", n, height, npts, nline)
+    work = torch.empty(int(nbytes), dtype=torch.uint8, device=proj.device) \
+        if nbytes > 0 else None
     nat.call("atb_vertical_backproject", proj.data_ptr(), proj.stride(0),
              proj.stride(1), n, height, width, trig.data_ptr(),
              pts.data_ptr(), npts, npts, nline, float(center),
              int(bool(edge_pad)), acc.data_ptr(), acc.stride(0),
-             acc.stride(1), R._stream_ptr(proj.device))
+             acc.stride(1), work.data_ptr() if work is not None else None,
+             int(nbytes), R._stream_ptr(proj.device))
 
 
 def _flat_log(raw, code, dark, flat_dark, apply_log, out, nonpos):

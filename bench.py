@@ -57,6 +57,8 @@ def _args():
     ap.add_argument("--storage", default="float32",
                     choices=["float32", "float16", "bfloat16"],
                     help="element type of the filtered sinogram (stack)")
+    ap.add_argument("--rows", type=int, default=512,
+                    help="detector rows of the vertical workload")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
                              "center", "vertical"],
@@ -727,8 +729,8 @@ def run_vertical(args):
     import torch
     from algotom_b200.rec import vertrec as VR
     dev = torch.device("cuda", 0)
-    height = 512
-    proj, ang = make_sinograms(height, dev)  # [1801][512][2560]
+    height = args.rows
+    proj, ang = make_sinograms(height, dev)  # [1801][rows][2560]
     torch.cuda.synchronize()
     kw = dict(angles=ang, apply_log=False, show_progress=False)
 
@@ -776,11 +778,15 @@ def run_vertical(args):
     if not args.no_oracle:
         from oracle import fbp_oracle as O
         from oracle import vertical_oracle as VO
-        rows = [0, 100, 300, 511]
+        rows = sorted({0, height // 5, (3 * height) // 5, height - 1})
         sub = proj[:, rows, :].cpu().numpy()
         xs, ys = VO.points_single_line(NCOL // 2, 30.0, NCOL)
+        # the default gpu=True takes float32-rounded angles, points and
+        # centre (as the reference's GPU kernel); the oracle gets the same
+        r32 = lambda v: np.float32(v).astype(np.float64)  # noqa: E731
         t0 = time.perf_counter()
-        bp = VO.vertical_back_projection(sub, ang, xs, ys, CENTER, True)
+        bp = VO.vertical_back_projection(sub, r32(ang), r32(xs), r32(ys),
+                                         float(np.float32(CENTER)), True)
         t_cpu = time.perf_counter() - t0
         ref = VO.ver_ramp_filter(bp, "hann", 150, "edge") * np.pi / (NROW - 1)
         got = single(proj)[rows].cpu().numpy()
@@ -797,7 +803,8 @@ def run_vertical(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded 12-ellipse phantoms)",
         "config": {"workload": "vertical slice at 30 deg through 1801 "
-                               "projections of 512 x 2560 (device-resident)",
+                               "projections of %d x 2560 (device-resident)"
+                               % height,
                    "l2": "inputs larger than L2 (9.4 GB)"},
         "roofline": {"bound": "hbm", "achieved": nbytes / t1 / 1e9,
                      "peak": hbm, "unit": "GB/s",
@@ -812,7 +819,9 @@ def run_vertical(args):
             "d2h_bytes_per_step": height * NCOL * 8,
             "ms_per_step": t_e2e * 1e3},
         "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
-        "gpu_launches": None}), flush=True)
+        # one vertical back-projection launch per step (the FP64 filter
+        # after it is library FFT work)
+        "gpu_launches": args.steps}), flush=True)
 
 
 def main():

@@ -325,13 +325,18 @@ int atb_slice_metric(const float *imgs, int64_t img_stride,
  *
  * with the reference's interpolation, inclusive bounds [0, width-1] and
  * optional edge padding.  Positions in FP64, interpolation FP32, sums over
- * 32 angles FP32, accumulation FP64.
+ * 32 angles FP32, accumulation FP64.  Deterministic.
  *
  *   proj    float32 [nproj][height][width] at proj_stride / row_stride
+ *           (height * row_stride < 2^31)
  *   trig    float64 [nproj][2] = (cos a, sin a)  (note: +a, not -a)
  *   points  float64 [nline][npts][2] = (x, y), line_stride between lines
  *           (in points)
  *   acc     float64 [nline][height][npts], added to (not overwritten)
+ *   work    device scratch of up to atb_vertical_workspace() bytes, or
+ *           NULL: with it, the angles are also split over CTAs when the
+ *           output alone is too small to fill the GPU (fewer bytes give a
+ *           smaller split)
  */
 int atb_vertical_backproject(const float *proj, int64_t proj_stride,
                              int64_t row_stride, int nproj, int height,
@@ -339,7 +344,12 @@ int atb_vertical_backproject(const float *proj, int64_t proj_stride,
                              const double *points, int64_t line_stride,
                              int npts, int nline, double center, int edge_pad,
                              double *acc, int64_t acc_line_stride,
-                             int64_t acc_row_stride, void *stream);
+                             int64_t acc_row_stride, void *work,
+                             int64_t work_bytes, void *stream);
+
+/* Bytes of scratch that let atb_vertical_backproject split its angles
+ * fully (0: no split is useful, or a bad argument). */
+int64_t atb_vertical_workspace(int nproj, int height, int npts, int nline);
 
 /*
  * Flat-field correction and -log of a chunk of projections; replaces the
