@@ -1,0 +1,166 @@
+// 360-degree sinograms with an offset rotation axis, sm_100a: the row
+// operations of algotom's extend_sinogram, convert_sinogram_360_to_180 and
+// convert_sinogram_180_to_360 (algotom/prep/conversion.py:76-454).
+//
+// One CTA per sinogram row.  The row (optionally mirrored left-right and
+// -log'ed in float32, as the reference's NumPy float32 arithmetic does) is
+// staged in shared memory as FP64 with 12 copies of each end sample on
+// either side; a sub-pixel shift then follows scipy.ndimage.shift(x, (0, s),
+// order 3, mode "nearest"), the published cubic B-spline method: one thread
+// turns the padded row into spline coefficients with the recursive filter
+// of pole z = sqrt(3) - 2 (gain (1 - z)(1 - 1/z); causal start value of the
+// half-sample symmetric extension; anti-causal start z / (z - 1) c[n-1]),
+// and every thread samples the spline at x - s with the cubic B-spline
+// weights, coefficient indices clamped to the padded row.  (Along the angle
+// axis the shift is zero and a cubic spline sampled at its knots returns its
+// samples, so rows are independent.)  The shifted row is rounded to float32
+// as scipy's output is.  extend_sinogram then scales the overlap columns by
+// a linear ramp, pads with the edge sample and doubles
+// (conversion.py:425-454), all in the same pass.
+#include <cmath>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int kPad = 12;       // end samples replicated on each side
+constexpr int kThreads = 256;
+constexpr int kMaxCols = 16384;
+
+struct RowArgs {
+  const float *src;
+  long long srs;
+  int nrow, ncol;
+  int flip, apply_log;
+  double shift;  // 0: no shift
+  int ov, side;  // extend: overlap columns and side; ov == 0: plain shift
+  float *dst;
+  long long drs;
+};
+
+// cubic B-spline coefficients of c[0..n-1] in place (one thread); every
+// product and sum rounded on its own (no contraction), as NumPy does
+__device__ void spline_coefficients(double *c, int n) {
+  const double z = sqrt(3.0) - 2.0;
+  const double gain = __dmul_rn(1.0 - z, 1.0 - 1.0 / z);
+  for (int i = 0; i < n; ++i) c[i] = __dmul_rn(c[i], gain);
+  if (n == 1) return;
+  const double z_n = pow(z, (double)n);
+  const double c0 = c[0];
+  double z_i = z;
+  double s = __dadd_rn(c[0], __dmul_rn(z_n, c[n - 1]));
+  for (int i = 1; i < n; ++i) {
+    s = __dadd_rn(s, __dmul_rn(z_i, __dadd_rn(c[i], __dmul_rn(z_n, c[n - 1 - i]))));
+    z_i = __dmul_rn(z_i, z);
+  }
+  c[0] = __dadd_rn(__dmul_rn(s, z / (1.0 - __dmul_rn(z_n, z_n))), c0);
+  for (int i = 1; i < n; ++i) c[i] = __dadd_rn(c[i], __dmul_rn(z, c[i - 1]));
+  c[n - 1] = __dmul_rn(c[n - 1], z / (z - 1.0));
+  for (int i = n - 2; i >= 0; --i) c[i] = __dmul_rn(z, __dsub_rn(c[i + 1], c[i]));
+}
+
+__global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int n = a.ncol, big = n + 2 * kPad;
+  double *c = reinterpret_cast<double *>(smem);   // [big]
+  float *y = reinterpret_cast<float *>(c + big);  // [n] the (shifted) row
+  const int row = blockIdx.x;
+  const float *src = a.src + row * a.srs;
+  for (int k = threadIdx.x; k < big; k += kThreads) {
+    const int col = min(max(k - kPad, 0), n - 1);
+    float v = src[a.flip ? n - 1 - col : col];
+    if (a.apply_log) v = -logf(v);
+    c[k] = (double)v;
+  }
+  __syncthreads();
+  if (a.shift != 0.0) {
+    if (threadIdx.x == 0) spline_coefficients(c, big);
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += kThreads) {
+      const double cc = __dadd_rn(__dsub_rn((double)k, a.shift), (double)kPad);
+      const double f = floor(cc), t = __dsub_rn(cc, f), u = __dsub_rn(1.0, t);
+      const double t2 = __dmul_rn(t, t), t3 = pow(t, 3.0);
+      const int i0 = (int)f;
+      // cubic B-spline weights of the taps floor - 1 .. floor + 2
+      const double w0 = pow(u, 3.0) / 6.0;
+      const double w1 = __dadd_rn(__dsub_rn(4.0, __dmul_rn(6.0, t2)), __dmul_rn(3.0, t3)) / 6.0;
+      const double w2 =
+          __dsub_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(3.0, t)), __dmul_rn(3.0, t2)), __dmul_rn(3.0, t3)) / 6.0;
+      const double w3 = t3 / 6.0;
+      double v = __dmul_rn(w0, c[min(max(i0 - 1, 0), big - 1)]);
+      v = __dadd_rn(v, __dmul_rn(w1, c[min(max(i0, 0), big - 1)]));
+      v = __dadd_rn(v, __dmul_rn(w2, c[min(max(i0 + 1, 0), big - 1)]));
+      v = __dadd_rn(v, __dmul_rn(w3, c[min(max(i0 + 2, 0), big - 1)]));
+      y[k] = __double2float_rn(v);
+    }
+  } else {
+    for (int k = threadIdx.x; k < n; k += kThreads) y[k] = (float)c[k + kPad];
+  }
+  __syncthreads();
+  float *dst = a.dst + row * a.drs;
+  if (a.ov == 0) {
+    for (int k = threadIdx.x; k < n; k += kThreads) dst[k] = y[k];
+    return;
+  }
+  // extend: ramp over the overlap, edge padding to 2 n - ov columns, x 2
+  const int ov = a.ov, pad = n - ov;
+  const double step = ov > 1 ? 1.0 / (double)(ov - 1) : 0.0;
+  // NumPy's linspace(start, stop, ov): m * step + start, the last value
+  // exactly stop (a single value is start)
+  auto weighted = [&](int k) -> float {  // column k of the ramped row
+    if (a.side == 1) {
+      if (k < n - ov) return y[k];
+      const int m = k - (n - ov);  // linspace(1, 0, ov)[m]
+      const double w = ov == 1 ? 1.0 : (m == ov - 1 ? 0.0 : __dadd_rn(__dmul_rn((double)m, -step), 1.0));
+      return __double2float_rn(__dmul_rn((double)y[k], w));
+    }
+    if (k >= ov) return y[k];
+    const double w = ov == 1 ? 0.0 : (k == ov - 1 ? 1.0 : __dmul_rn((double)k, step));  // linspace(0, 1, ov)[k]
+    return __double2float_rn(__dmul_rn((double)y[k], w));
+  };
+  for (int k = threadIdx.x; k < n + pad; k += kThreads) {
+    float v;
+    if (a.side == 1) v = weighted(min(k, n - 1));
+    else v = weighted(max(k - pad, 0));
+    dst[k] = 2.0f * v;
+  }
+}
+
+int launch_rows(const RowArgs &a, const char *what, void *stream) {
+  const size_t smem = sizeof(double) * (a.ncol + 2 * kPad) + sizeof(float) * a.ncol;
+  int rc = atb::ensure_smem(row_kernel, smem, what);
+  if (rc != ATB_OK) return rc;
+  row_kernel<<<a.nrow, kThreads, smem, atb::as_stream(stream)>>>(a);
+  return atb::check_launch(what);
+}
+
+}  // namespace
+
+extern "C" int atb_shift_rows(const float *src, int64_t src_row_stride, int nrow, int ncol, double shift, int flip,
+                              float *dst, int64_t dst_row_stride, void *stream) {
+  if (!src || !dst) return atb::fail(ATB_EINVAL, "atb_shift_rows: null pointer");
+  if (nrow < 1 || ncol < 1) return atb::fail(ATB_EINVAL, "atb_shift_rows: bad shape %dx%d", nrow, ncol);
+  if (ncol > kMaxCols) return atb::fail(ATB_ERANGE, "atb_shift_rows: ncol=%d > %d", ncol, kMaxCols);
+  if (!std::isfinite(shift)) return atb::fail(ATB_EINVAL, "atb_shift_rows: shift is not finite");
+  RowArgs a;
+  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol;
+  a.flip = flip ? 1 : 0; a.apply_log = 0; a.shift = shift; a.ov = 0; a.side = 0;
+  a.dst = dst; a.drs = dst_row_stride;
+  return launch_rows(a, "atb_shift_rows", stream);
+}
+
+extern "C" int atb_extend_rows(const float *src, int64_t src_row_stride, int nrow, int ncol, int apply_log,
+                               double shift, int overlap, int side, float *dst, int64_t dst_row_stride,
+                               void *stream) {
+  if (!src || !dst) return atb::fail(ATB_EINVAL, "atb_extend_rows: null pointer");
+  if (nrow < 1 || ncol < 1) return atb::fail(ATB_EINVAL, "atb_extend_rows: bad shape %dx%d", nrow, ncol);
+  if (ncol > kMaxCols) return atb::fail(ATB_ERANGE, "atb_extend_rows: ncol=%d > %d", ncol, kMaxCols);
+  if (overlap < 1 || overlap > ncol || (side != 0 && side != 1))
+    return atb::fail(ATB_EINVAL, "atb_extend_rows: overlap %d / side %d invalid for %d columns", overlap, side, ncol);
+  if (!std::isfinite(shift)) return atb::fail(ATB_EINVAL, "atb_extend_rows: shift is not finite");
+  RowArgs a;
+  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol;
+  a.flip = 0; a.apply_log = apply_log ? 1 : 0; a.shift = shift; a.ov = overlap; a.side = side;
+  a.dst = dst; a.drs = dst_row_stride;
+  return launch_rows(a, "atb_extend_rows", stream);
+}

@@ -370,6 +370,32 @@ int atb_flat_log(const void *src, int src_dtype, int64_t src_proj_stride,
                  int64_t dst_proj_stride, int64_t dst_row_stride,
                  unsigned *nonpos, void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* 360-degree sinograms (algotom/prep/conversion.py)                      */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * scipy.ndimage.shift(x, (0, shift), mode="nearest") of float32 rows
+ * (cubic spline, the sub-pixel shift of stitch_image and
+ * convert_sinogram_180_to_360, conversion.py:104-110, 389-391); with
+ * `flip` the rows are mirrored left-right first (np.fliplr).  shift == 0
+ * copies.  ncol <= 16384.
+ */
+int atb_shift_rows(const float *src, int64_t src_row_stride, int nrow,
+                   int ncol, double shift, int flip, float *dst,
+                   int64_t dst_row_stride, void *stream);
+
+/*
+ * The row work of extend_sinogram (conversion.py:425-454): optional -log,
+ * the sub-pixel shift (0: none), the linear ramp over `overlap` columns on
+ * `side` (1: right, 0: left), edge padding to 2 ncol - overlap columns and
+ * the factor 2.  dst rows hold 2 ncol - overlap floats.  ncol <= 16384.
+ */
+int atb_extend_rows(const float *src, int64_t src_row_stride, int nrow,
+                    int ncol, int apply_log, double shift, int overlap,
+                    int side, float *dst, int64_t dst_row_stride,
+                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

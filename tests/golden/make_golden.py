@@ -320,9 +320,52 @@ def make_vertical():
     np.savez_compressed(os.path.join(HERE, "golden_vertical.npz"), **out)
 
 
+def make_conversion():
+    """360-degree conversions (algotom/prep/conversion.py:43-454) and the
+    scipy sub-pixel shift they call."""
+    import algotom.prep.conversion as conv
+    from scipy.ndimage import shift as ndi_shift
+    nrow, ncol = 181, 64
+    ang = np.linspace(0.0, 2.0 * np.pi, nrow)
+    out = {}
+    for cor in (50.3, 12.7, 45.5, 20.0):
+        att = phantom.ellipse_sinogram(70, nrow, ncol, cor, photons=None,
+                                       angles=ang)[0]
+        trans = np.exp(-0.2 * att).astype(np.float32)
+        out[_key("att", cor)] = att
+        out[_key("trans", cor)] = trans
+        sino, c = conv.extend_sinogram(trans.copy(), cor)
+        out[_key("extend", cor)], out[_key("extend", cor, "cor")] = sino, c
+        sino, c = conv.extend_sinogram(att.copy(), cor, apply_log=False)
+        out[_key("extend_nolog", cor)] = sino
+        sino, c = conv.convert_sinogram_360_to_180(att.copy(), cor)
+        out[_key("to180", cor)], out[_key("to180", cor, "cor")] = sino, c
+        sino, _ = conv.convert_sinogram_360_to_180(att.copy(), cor,
+                                                   norm=False,
+                                                   total_width=2 * ncol)
+        out[_key("to180_nonorm_wide", cor)] = sino
+    att = out[_key("att", 50.3)]
+    sino, c = conv.extend_sinogram(att.copy(), (27.4, 1), apply_log=False)
+    out["extend_tuple"], out["extend_tuple_cor"] = sino, c
+    sino, c = conv.convert_sinogram_360_to_180(att.copy(), (27.4, 1))
+    out["to180_tuple"], out["to180_tuple_cor"] = sino, c
+    s180 = out[_key("att", 20.0)][:91]
+    for center in (30.4, 33.0, 18.25):
+        out[_key("to360", center)] = conv.convert_sinogram_180_to_360(
+            s180.copy(), center)
+    out["s180"] = s180
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((12, 97)).astype(np.float32)
+    out["shift_x"] = x
+    for sh in (0.3, -0.45, 11.3, -15.6, 40.2):
+        out[_key("shift", sh)] = ndi_shift(x, (0, sh), mode="nearest")
+    np.savez_compressed(os.path.join(HERE, "golden_conversion.npz"), **out)
+
+
 GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
               "recon": make_recon, "unittest": make_reference_test_fixture,
-              "center": make_center, "vertical": make_vertical}
+              "center": make_center, "vertical": make_vertical,
+              "conversion": make_conversion}
 
 if __name__ == "__main__":
     # python make_golden.py [name ...]  (default: every fixture)
