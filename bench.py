@@ -61,7 +61,7 @@ def _args():
                     help="detector rows of the vertical workload")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
-                             "center", "vertical"],
+                             "center", "vertical", "halfacq"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
@@ -70,7 +70,9 @@ def _args():
                          "64 uneven sinograms in one persistent launch under "
                          "a CUDA graph; single: one 1024^2 x 900 slice; "
                          "center: centre search over 128 candidates; "
-                         "vertical: vertical slices from 1801 projections")
+                         "vertical: vertical slices from 1801 projections; "
+                         "halfacq: a 360-degree offset-axis slice extended "
+                         "and reconstructed")
     return ap.parse_args()
 
 
@@ -824,8 +826,100 @@ def run_vertical(args):
         "gpu_launches": args.steps}), flush=True)
 
 
+def run_halfacq(args):
+    """Half-acquisition slice: a 360-degree sinogram of 3601 angles x 2560
+    detector pixels whose rotation axis sits at 2300.4 (offset), extended on
+    the device (``extend_sinogram``: -log, sub-pixel cubic-spline shift,
+    overlap ramp, padding to 2 x 2560 - 518 = 4602 columns) and
+    reconstructed by FBP at the returned centre (4602^2 pixels).  ``value``: pixel-angle updates/s of
+    extend + FBP from a device-resident transmission sinogram; the extend
+    step alone is reported against HBM (4 B read + 6.8 B written per input
+    sample).  CPU baseline: the oracle's FP64 extend_sinogram on 64 rows."""
+    import torch
+    from algotom_b200 import phantom
+    from algotom_b200.prep import conversion as PC
+    from algotom_b200.rec import reconstruction as R
+    dev = torch.device("cuda", 0)
+    nrow, ncol, cor = 3601, NCOL, 2300.4
+    ang = np.linspace(0.0, 2.0 * np.pi, nrow)
+    att, _, _ = phantom.ellipse_sinogram(3000, nrow, ncol, cor, photons=None,
+                                         angles=ang)
+    trans = torch.as_tensor(np.exp(-0.2 * att).astype(np.float32),
+                            device=dev)
+
+    def extend():
+        return PC.extend_sinogram(trans, cor)
+
+    def step():
+        e, c = extend()
+        return R.fbp_reconstruction(e, c, angles=ang, apply_log=False)
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            r = fn()
+            del r
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / n
+
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(0)
+    sampler.start()
+    t_ext = timed(extend, args.steps)
+    t_all = timed(step, args.steps)
+    clocks = sampler.stop()
+    e, c = extend()
+    width = e.shape[1]
+    upd = nrow * width * width
+    pk, src = _peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    ext_bytes = nrow * ncol * 4 + nrow * width * 4
+    acc = cpu = None
+    if not args.no_oracle:
+        from oracle import conversion_oracle as CO
+        from oracle import fbp_oracle as O
+        rows = np.arange(0, nrow, nrow // 64)[:64]
+        sub = trans[rows].cpu().numpy()
+        t0 = time.perf_counter()
+        ref, _ = CO.extend_sinogram(sub, cor)
+        t_cpu = time.perf_counter() - t0
+        acc = {"extend_rel_l2_vs_fp64_oracle": O.rel_l2(e[rows].cpu().numpy(),
+                                                         ref),
+               "rows_checked": len(rows)}
+        cpu = {"value": len(rows) / t_cpu, "unit": "rows/s (extend)",
+               "cores": 1, "kind": "port",
+               "sample": "FP64 NumPy extend_sinogram of %d rows, %.2f s"
+                         % (len(rows), t_cpu)}
+    print(json.dumps({
+        "metric": "half-acquisition FBP pixel-angle updates/s (extend + FBP)",
+        "value": upd / t_all, "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_all * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 12-ellipse phantom, 360 degrees)",
+        "config": {"workload": "360-degree sinogram 3601 x 2560, rotation "
+                               "axis 2300.4, extended to %d columns, FBP "
+                               "%d^2" % (width, width), "centre": c},
+        "extend": {"ms": t_ext * 1e3, "rows_per_s": nrow / t_ext,
+                   "roofline": {"bound": "hbm",
+                                "achieved": ext_bytes / t_ext / 1e9,
+                                "peak": hbm, "unit": "GB/s",
+                                "frac": ext_bytes / t_ext / 1e9 / hbm,
+                                "peak_source": src}},
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
+        "gpu_launches": 3 * args.steps}), flush=True)
+
+
 def main():
     args = _args()
+    if args.workload == "halfacq":
+        run_halfacq(args)
+        return
     if args.workload == "vertical":
         run_vertical(args)
         return
