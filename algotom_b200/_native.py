@@ -19,7 +19,7 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_zoom_linear", "atb_image_range", "atb_slice_metric_workspace",
            "atb_slice_metric", "atb_vertical_backproject",
            "atb_vertical_workspace", "atb_flat_log", "atb_shift_rows",
-           "atb_extend_rows")
+           "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid")
 
 F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
@@ -97,6 +97,11 @@ _SIGS = {
     "atb_extend_rows": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _c_i64, _vp]),
+    "atb_spline_prefilter": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, ctypes.c_int, _vp]),
+    "atb_dfi_regrid": (ctypes.c_int, [
+        _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "atb_flat_log": (ctypes.c_int, [
         _vp, ctypes.c_int, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, _vp, _vp, _c_i64, ctypes.c_int, _vp, _c_i64, _c_i64,

@@ -124,14 +124,17 @@ class _Source:
     ramp-filtered rows for FBP, the -log rows for BPF."""
 
     def __init__(self, sino, angles, method, filter_name):
-        if method not in ("fbp", "bpf"):
+        if method not in ("fbp", "bpf", "dfi"):
             raise NotImplementedError(
-                "method %r: this library reconstructs with 'fbp' or 'bpf'"
-                % (method,))
+                "method %r: this library reconstructs with 'fbp', 'bpf' or "
+                "'dfi'" % (method,))
         self.nrow, self.ncol = sino.shape
         self.method, self.filter_name = method, filter_name
-        self.angles = R._validate(sino, 0.0, angles)[3]
         self.sino = sino
+        if method == "dfi":  # DFI takes the angles as given (None allowed)
+            self.dfi_angles = angles
+            return
+        self.angles = R._validate(sino, 0.0, angles)[3]
         self.pad = min(int(0.15 * self.ncol), 150)
         if method == "fbp":
             f = R.filter_sinograms(sino.unsqueeze(1), self.pad, "edge", False,
@@ -145,6 +148,12 @@ class _Source:
     def reconstruct(self, centers, ratio):
         """float32 [len(centers), ncol, ncol] reconstructions."""
         nrow, ncol, dev = self.nrow, self.ncol, self.sino.device
+        if self.method == "dfi":
+            from .dfi import dfi_reconstruction
+            return torch.stack([dfi_reconstruction(
+                self.sino, float(c), angles=self.dfi_angles, ratio=ratio,
+                filter_name=self.filter_name, apply_log=False).to(
+                    torch.float32) for c in centers])
         for c in centers:
             R._validate(self.sino, float(c), self.angles)
         out = torch.empty((len(centers), ncol, ncol), dtype=torch.float32,
@@ -260,7 +269,7 @@ def _find_center_based_slice_metric(sinogram, start, stop, step=1,
             list_metric[k0:k0 + len(cs)] = slice_metrics(imgs, m, nmin, nmax)
         else:
             host = imgs.cpu().numpy()
-            if method == "bpf":
+            if method in ("bpf", "dfi"):
                 host = host.astype(np.float64)
             for i in range(len(cs)):
                 list_metric[k0 + i] = metric_function(host[i], **kwargs)

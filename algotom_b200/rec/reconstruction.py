@@ -535,3 +535,7 @@ def bpf_reconstruction(sinogram, center, angles=None, ratio=1.0,
 # module's namespace like the reference's
 from .center import (find_center_based_slice_metric,  # noqa: E402,F401
                      _find_center_based_slice_metric)
+
+# direct Fourier inversion (reconstruction.py:687-907)
+from .dfi import (dfi_reconstruction,  # noqa: E402,F401
+                  generate_mapping_coordinate)

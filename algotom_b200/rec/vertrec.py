@@ -36,6 +36,7 @@ import torch
 from .. import _native as nat
 from . import reconstruction as R
 from . import windows as win
+from .padding import pad_rows
 
 _WARN_FULL = ("!!! Applying logarithm is enabled but there are values <= 0.0"
               " in the data !!!")
@@ -168,56 +169,6 @@ def _filter_rows(x3, pad, pad_mode, spec, log2m, out3):
              R._stream_ptr(dev))
 
 
-def _pad_rows64(x, pad, mode):
-    """``np.pad(x, ((0, 0), (pad, pad)), mode)`` of a 2-D float64 tensor on
-    its device, for numpy's ten modes (end / constant values 0, statistics
-    over the whole row)."""
-    rows, n = x.shape
-    if pad == 0:
-        return x
-    dev = x.device
-    i = torch.arange(-pad, n + pad, device=dev)
-    if mode in ("edge", "reflect", "symmetric", "wrap"):
-        if mode == "edge":
-            idx = i.clamp(0, n - 1)
-        elif mode == "wrap":
-            idx = torch.remainder(i, n)
-        elif mode == "symmetric":
-            r = torch.remainder(i, 2 * n)
-            idx = torch.where(r >= n, 2 * n - 1 - r, r)
-        elif n == 1:
-            idx = torch.zeros_like(i)
-        else:  # reflect: period 2 (n - 1), edges not repeated
-            r = torch.remainder(i, 2 * (n - 1))
-            idx = torch.where(r >= n, 2 * (n - 1) - r, r)
-        return x[:, idx]
-    out = torch.empty((rows, n + 2 * pad), dtype=x.dtype, device=dev)
-    out[:, pad:pad + n] = x
-    if mode == "constant":
-        out[:, :pad] = 0.0
-        out[:, pad + n:] = 0.0
-    elif mode == "linear_ramp":  # from 0 at the ends to the edge samples
-        k = torch.arange(pad, device=dev, dtype=x.dtype)
-        out[:, :pad] = k[None, :] * (x[:, :1] / pad)
-        out[:, pad + n:] = torch.flip(k, [0])[None, :] * (x[:, -1:] / pad)
-    elif mode in ("mean", "maximum", "minimum", "median"):
-        if mode == "mean":
-            v = x.mean(dim=1, keepdim=True)
-        elif mode == "maximum":
-            v = x.amax(dim=1, keepdim=True)
-        elif mode == "minimum":
-            v = x.amin(dim=1, keepdim=True)
-        else:
-            srt = torch.sort(x, dim=1).values
-            v = 0.5 * (srt[:, (n - 1) // 2:(n - 1) // 2 + 1] +
-                       srt[:, n // 2:n // 2 + 1])
-        out[:, :pad] = v
-        out[:, pad + n:] = v
-    else:
-        raise ValueError("pad_mode %r is not supported" % (mode,))
-    return out
-
-
 def _after_filter64(ver, filter_name, pad, pad_mode, slab_bytes=1 << 30):
     """The ramp filter applied to every row of the vertical slices after
     the back-projection (``vertrec.py:684-688``, ``:698-706``):
@@ -234,7 +185,7 @@ def _after_filter64(ver, filter_name, pad, pad_mode, slab_bytes=1 << 30):
     out = torch.empty_like(rows)
     step = max(1, int(slab_bytes // (16 * n)))
     for r0 in range(0, rows.shape[0], step):
-        xp = _pad_rows64(rows[r0:r0 + step], pad, pad_mode)
+        xp = pad_rows(rows[r0:r0 + step], pad, pad_mode)
         y = torch.fft.ifft(torch.fft.fft(xp, dim=1) * hd, dim=1).real
         out[r0:r0 + step] = y[:, pad:pad + width]
     return out.reshape(nline, height, width)

@@ -396,6 +396,42 @@ int atb_extend_rows(const float *src, int64_t src_row_stride, int nrow,
                     int side, float *dst, int64_t dst_row_stride,
                     void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* Direct Fourier inversion (dfi_reconstruction, reconstruction.py:687)   */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * B-spline coefficients of order 3 or 5 along many strided lines, in place;
+ * replaces scipy.ndimage.spline_filter1d inside the map_coordinates of
+ * dfi_reconstruction (reconstruction.py:776-781, order 5, "reflect") and
+ * the shift along angles of __dfi_handle_angles (:746, order 3, "wrap").
+ *
+ *   data      float64; line L = (outer, comp) starts at
+ *             data + (L / ncomp) * line_stride + (L % ncomp), elements
+ *             elem_stride apart (strides in doubles); ncomp = 2 walks the
+ *             real and imaginary parts of interleaved complex data
+ *   boundary  0: half-sample symmetric start values (scipy's "reflect";
+ *             also "nearest" after 12 edge samples of padding),
+ *             1: whole-sample symmetric (scipy's "mirror" and "wrap")
+ */
+int atb_spline_prefilter(double *data, int64_t line_stride,
+                         int64_t elem_stride, int nlines, int ncomp, int n,
+                         int order, int boundary, void *stream);
+
+/*
+ * Regrid the polar spectrum of a sinogram onto the width x width Cartesian
+ * frequency grid; replaces generate_mapping_coordinate
+ * (reconstruction.py:687-728) plus util.mapping(order=5, mode="reflect")
+ * and the unit circle mask in __dfi_single_slice (:767-787).
+ *
+ *   coef   complex128 [nrow][width]: quintic B-spline coefficients of the
+ *          centred row spectra (atb_spline_prefilter, order 5, boundary 0,
+ *          along both axes)
+ *   out    complex128 [width][width], natural (not shifted) order
+ */
+int atb_dfi_regrid(const double *coef, int nrow, int width, double *out,
+                   void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -362,10 +362,52 @@ def make_conversion():
     np.savez_compressed(os.path.join(HERE, "golden_conversion.npz"), **out)
 
 
+def make_dfi():
+    """DFI reconstruction (reconstruction.py:687-907)."""
+    nrow, ncol, cen = 181, 96, 47.3
+    ang = np.linspace(0.0, np.pi, nrow)
+    sino = phantom.ellipse_sinogram(80, nrow, ncol, cen, photons=2e4,
+                                    angles=ang)[0]
+    out = {"sino": sino, "angles": ang, "center": np.float64(cen)}
+    r, t = rec.generate_mapping_coordinate(97 + 48, nrow, 97 + 48, 97 + 48)
+    out["map_r"], out["map_theta"] = r, t
+    f = rec.dfi_reconstruction
+    out["dfi_default"] = f(sino.copy(), cen, apply_log=False)
+    out["dfi_angles"] = f(sino.copy(), cen, angles=ang, apply_log=False)
+    off = ang + 0.1
+    out["dfi_angles_offset"] = f(sino.copy(), cen, angles=off,
+                                 apply_log=False)
+    out["dfi_angles_desc"] = f(sino[::-1].copy(), cen, angles=ang[::-1],
+                               apply_log=False)
+    ang360 = np.linspace(0.0, 2 * np.pi, 2 * nrow - 1)
+    s360 = np.concatenate([sino, sino[-2::-1, ::-1]], axis=0)
+    out["sino360"] = s360
+    out["dfi_360"] = f(s360.copy(), cen, angles=ang360, apply_log=False)
+    out["dfi_r0_nofilter"] = f(sino.copy(), cen, ratio=0.0, filter_name=None,
+                               apply_log=False)
+    out["dfi_reflect_pad05"] = f(sino.copy(), cen, ratio=None,
+                                 pad_mode="reflect", pad_rate=0.5,
+                                 apply_log=False)
+    odd = sino[:, :95].copy()
+    out["sino_odd"] = odd
+    out["dfi_odd"] = f(odd.copy(), 46.8, apply_log=False)
+    trans = np.exp(-sino).astype(np.float32)
+    trans[10, 20] = 0.0
+    out["trans"] = trans
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        out["dfi_log"] = f(trans.copy(), cen)
+    out["dfi_log_warned"] = np.array(
+        any("logarithm" in str(w.message) for w in caught))
+    s3 = np.stack([sino, 0.5 * sino], axis=1)
+    out["dfi_3d"] = f(s3.copy(), cen, apply_log=False, ncore=1)
+    np.savez_compressed(os.path.join(HERE, "golden_dfi.npz"), **out)
+
+
 GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
               "recon": make_recon, "unittest": make_reference_test_fixture,
               "center": make_center, "vertical": make_vertical,
-              "conversion": make_conversion}
+              "conversion": make_conversion, "dfi": make_dfi}
 
 if __name__ == "__main__":
     # python make_golden.py [name ...]  (default: every fixture)

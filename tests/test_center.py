@@ -346,4 +346,4 @@ def test_errors(cuda):
     with pytest.raises(NotImplementedError):
         R._find_center_based_slice_metric(np.ones((10, 16), np.float32),
                                           7, 9, 1, apply_log=False,
-                                          method="dfi")
+                                          method="gridrec")

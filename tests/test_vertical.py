@@ -93,14 +93,14 @@ def test_oracle_reconstructions(golden):
 
 
 @pytest.mark.parametrize("mode", PAD_MODES)
-def test_fp64_row_padding_matches_numpy(mode):
+def test_row_padding_matches_numpy(mode):
     import torch
-    from algotom_b200.rec import vertrec as VR
+    from algotom_b200.rec.padding import pad_rows
     rng = np.random.default_rng(1)
     for n in (1, 2, 3, 7, 8):
         x = rng.standard_normal((3, n))
         for pad in (0, 1, 4, 19):
-            got = VR._pad_rows64(torch.from_numpy(x), pad, mode).numpy()
+            got = pad_rows(torch.from_numpy(x), pad, mode).numpy()
             ref = np.pad(x, ((0, 0), (pad, pad)), mode=mode)
             if mode == "mean":  # summation order differs from NumPy's
                 assert np.allclose(got, ref, rtol=1e-15, atol=1e-15)
