@@ -61,7 +61,7 @@ def _args():
                     help="detector rows of the vertical workload")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
-                             "center", "vertical", "halfacq"],
+                             "center", "vertical", "halfacq", "dfi"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
@@ -72,7 +72,8 @@ def _args():
                          "center: centre search over 128 candidates; "
                          "vertical: vertical slices from 1801 projections; "
                          "halfacq: a 360-degree offset-axis slice extended "
-                         "and reconstructed")
+                         "and reconstructed; dfi: direct Fourier inversion "
+                         "of one slice")
     return ap.parse_args()
 
 
@@ -915,8 +916,71 @@ def run_halfacq(args):
         "gpu_launches": 3 * args.steps}), flush=True)
 
 
+def run_dfi(args):
+    """DFI of one benchmark slice (1801 angles x 2560 det, centre 1278.3):
+    padded to 2561 + 2 x 640 = 3841 columns, row transform, quintic
+    regridding of the 1801 x 3841 polar spectrum onto 3841^2, inverse 2-D
+    transform, device-resident input.  ``value``: slices/s.  CPU baseline:
+    the same steps through scipy.ndimage's compiled spline routines and
+    NumPy's FFT, as the reference calls them (one slice, one core); its
+    output is also the accuracy reference."""
+    import torch
+    from algotom_b200 import phantom
+    from algotom_b200.rec import reconstruction as R
+    dev = torch.device("cuda", 0)
+    ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
+    s, _, _ = phantom.ellipse_sinogram(2000, NROW, NCOL, CENTER,
+                                       photons=PHOTONS, angles=ang)
+    sd = torch.as_tensor(s, device=dev)
+
+    def step():
+        return R.dfi_reconstruction(sd, CENTER, apply_log=False)
+
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(0)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), \
+        torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        r = step()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t = e0.elapsed_time(e1) / 1e3 / args.steps
+    acc = cpu = None
+    if not args.no_oracle:
+        from oracle import dfi_oracle as DO
+        from oracle import fbp_oracle as O
+        t0 = time.perf_counter()
+        ref = DO.dfi_reconstruction_scipy(s, CENTER)
+        t_cpu = time.perf_counter() - t0
+        acc = {"rel_l2_vs_scipy_port": O.rel_l2(r.cpu().numpy(), ref)}
+        cpu = {"value": 1.0 / t_cpu, "unit": "slices/s", "cores": 1,
+               "kind": "port",
+               "sample": "one 1801 x 2560 slice through scipy.ndimage "
+                         "(shift, map_coordinates order 5) and NumPy FFTs, "
+                         "%.1f s" % t_cpu}
+    print(json.dumps({
+        "metric": "DFI slices/s at 2560 det", "value": 1.0 / t,
+        "unit": "slices/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded 12-ellipse phantom)",
+        "config": {"workload": "DFI of one 1801 x 2560 slice, padded to "
+                               "3841, regridded to 3841^2"},
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
+        # shift, pad gather, spline prefilter x 2, regrid, plus library FFTs
+        "gpu_launches": 4 * args.steps}), flush=True)
+
+
 def main():
     args = _args()
+    if args.workload == "dfi":
+        run_dfi(args)
+        return
     if args.workload == "halfacq":
         run_halfacq(args)
         return

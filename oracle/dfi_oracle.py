@@ -212,3 +212,34 @@ def dfi_reconstruction(sinogram, center, angles=None, ratio=1.0,
             ratio = min(center, ncol - center) / (0.5 * ncol)
         rec = rec * O.make_circle_mask(ncol, ratio)
     return rec
+
+
+def dfi_reconstruction_scipy(sinogram, center, ratio=1.0, filter_name="hann",
+                             pad_rate=0.25, pad_mode="edge"):
+    """The same steps (no angle handling, no -log) through scipy.ndimage's
+    compiled spline routines and NumPy's FFT, as the reference calls them:
+    the timed CPU baseline at full size, where the pure-Python restatement
+    above would take minutes."""
+    import scipy.ndimage as ndi
+    sino = np.asarray(sinogram, dtype=np.float32)
+    nrow, ncol = sino.shape
+    if ncol % 2 == 0:
+        sino = np.pad(sino, ((0, 0), (0, 1)), mode="edge")
+    ncol1 = sino.shape[-1]
+    pad = int(pad_rate * ncol1)
+    sino = ndi.shift(sino, (0, (ncol1 - 1) / 2.0 - center), mode="nearest")
+    sino = np.pad(sino, ((0, 0), (pad, pad)), mode=pad_mode)
+    nrow, ncol2 = sino.shape
+    mask = O.make_circle_mask(ncol2, 1.0)
+    r_mat, theta_mat = mapping_coordinates(ncol2, nrow, ncol2, ncol2)
+    f = np.fft.fftshift(np.fft.fft(np.fft.ifftshift(sino, axes=1)), axes=1)
+    if filter_name is not None:
+        f = f * O.make_smoothing_window(filter_name, ncol2)[None, :]
+    coords = np.vstack((theta_mat.ravel(), r_mat.ravel()))
+    reg = ndi.map_coordinates(f, coords, order=5, mode="reflect").reshape(
+        r_mat.shape) * mask
+    rec = np.real(np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(reg))))
+    rec = rec[pad:ncol + pad, pad:ncol + pad]
+    if ratio is not None:
+        rec = rec * O.make_circle_mask(ncol, ratio)
+    return rec
