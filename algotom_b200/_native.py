@@ -98,7 +98,7 @@ _SIGS = {
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _c_i64, _vp]),
     "atb_spline_prefilter": (ctypes.c_int, [
-        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        _vp, _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, ctypes.c_int, _vp]),
     "atb_dfi_regrid": (ctypes.c_int, [
         _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),

@@ -16,7 +16,8 @@ inversion runs on the device:
    before ``-log``;
 3. every row is transformed (library FFT, FP64) and windowed;
 4. the polar spectrum is turned into quintic B-spline coefficients along
-   both axes (``atb_spline_prefilter``) and regridded onto the Cartesian
+   both axes (``atb_spline_prefilter``, the prefilter's impulse response as
+   a parallel FIR) and regridded onto the Cartesian
    frequency grid with the unit-circle mask (``atb_dfi_regrid``);
 5. an inverse 2-D transform (library FFT, FP64), crop and circle mask.
 
@@ -57,17 +58,19 @@ def generate_mapping_coordinate(width_sino, height_sino, width_rec,
 
 def _prefilter(t, axis, order, boundary):
     """B-spline coefficients of a contiguous float64 / complex128 2-D CUDA
-    tensor along ``axis``, in place (boundary 0: half-sample symmetric,
-    1: whole-sample symmetric)."""
+    tensor along ``axis``, in a new tensor (boundary 0: half-sample
+    symmetric, 1: whole-sample symmetric)."""
     h, w = t.shape
     ncomp = 2 if t.is_complex() else 1
     if axis == 1:
         lines, line_stride, es, n = h, w * ncomp, ncomp, w
     else:
         lines, line_stride, es, n = w, ncomp, w * ncomp, h
-    nat.call("atb_spline_prefilter", t.data_ptr(), line_stride, es, lines,
-             ncomp, n, order, boundary, R._stream_ptr(t.device))
-    return t
+    out = torch.empty_like(t)
+    nat.call("atb_spline_prefilter", t.data_ptr(), out.data_ptr(),
+             line_stride, es, lines, ncomp, n, order, boundary,
+             R._stream_ptr(t.device))
+    return out
 
 
 def _bspline3(u):
@@ -139,9 +142,7 @@ def _dfi_slice(s, window):
                                          dim=1), dim=1)
     if window is not None:
         f = f * window
-    f = f.contiguous()
-    _prefilter(f, 0, 5, 0)
-    _prefilter(f, 1, 5, 0)
+    f = _prefilter(_prefilter(f.contiguous(), 0, 5, 0), 1, 5, 0)
     reg = torch.empty((w, w), dtype=torch.complex128, device=s.device)
     nat.call("atb_dfi_regrid", f.data_ptr(), nrow, w, reg.data_ptr(),
              R._stream_ptr(s.device))

@@ -401,20 +401,24 @@ int atb_extend_rows(const float *src, int64_t src_row_stride, int nrow,
 /* ---------------------------------------------------------------------- */
 
 /*
- * B-spline coefficients of order 3 or 5 along many strided lines, in place;
+ * B-spline coefficients of order 3 or 5 along many strided lines;
  * replaces scipy.ndimage.spline_filter1d inside the map_coordinates of
  * dfi_reconstruction (reconstruction.py:776-781, order 5, "reflect") and
  * the shift along angles of __dfi_handle_angles (:746, order 3, "wrap").
+ * Applied as the filter's symmetric impulse response (2 x 48 taps for
+ * order 5, 2 x 32 for order 3), exact to below 1e-17 relative.
  *
- *   data      float64; line L = (outer, comp) starts at
- *             data + (L / ncomp) * line_stride + (L % ncomp), elements
+ *   src, dst  float64, not overlapping; line L = (outer, comp) starts at
+ *             + (L / ncomp) * line_stride + (L % ncomp), elements
  *             elem_stride apart (strides in doubles); ncomp = 2 walks the
- *             real and imaginary parts of interleaved complex data
- *   boundary  0: half-sample symmetric start values (scipy's "reflect";
- *             also "nearest" after 12 edge samples of padding),
+ *             real and imaginary parts of interleaved complex data.  Either
+ *             the elements (elem_stride == ncomp) or the lines
+ *             (line_stride == ncomp) must be contiguous.
+ *   boundary  0: half-sample symmetric extension (scipy's "reflect"; also
+ *             "nearest" after 12 edge samples of padding),
  *             1: whole-sample symmetric (scipy's "mirror" and "wrap")
  */
-int atb_spline_prefilter(double *data, int64_t line_stride,
+int atb_spline_prefilter(const double *src, double *dst, int64_t line_stride,
                          int64_t elem_stride, int nlines, int ncomp, int n,
                          int order, int boundary, void *stream);
 

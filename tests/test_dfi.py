@@ -62,10 +62,19 @@ def test_oracle_matches_reference(golden, name):
 def test_abi_argument_errors():
     lib = nat.load()
     one = 1
-    assert lib.atb_spline_prefilter(None, 8, 1, 2, 1, 8, 5, 0, None) == -1
-    assert lib.atb_spline_prefilter(one, 8, 1, 2, 3, 8, 5, 0, None) == -1
-    assert lib.atb_spline_prefilter(one, 8, 1, 2, 1, 8, 4, 0, None) == -1
-    assert lib.atb_spline_prefilter(one, 8, 1, 2, 1, 8, 5, 2, None) == -1
+    two = 2
+    assert lib.atb_spline_prefilter(None, two, 8, 1, 2, 1, 8, 5, 0,
+                                    None) == -1
+    assert lib.atb_spline_prefilter(one, one, 8, 1, 2, 1, 8, 5, 0,
+                                    None) == -1  # in place
+    assert lib.atb_spline_prefilter(one, two, 8, 1, 2, 3, 8, 5, 0,
+                                    None) == -1
+    assert lib.atb_spline_prefilter(one, two, 8, 1, 2, 1, 8, 4, 0,
+                                    None) == -1
+    assert lib.atb_spline_prefilter(one, two, 8, 1, 2, 1, 8, 5, 2,
+                                    None) == -1
+    assert lib.atb_spline_prefilter(one, two, 8, 3, 2, 1, 8, 5, 0,
+                                    None) == -1  # neither axis contiguous
     assert lib.atb_dfi_regrid(None, 8, 8, one, None) == -1
     assert lib.atb_dfi_regrid(one, 8, 50000, one, None) == -3
     assert b"too large" in lib.atb_last_error()
