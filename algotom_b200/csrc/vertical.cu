@@ -54,15 +54,17 @@ struct VArgs {
   double *part;        // group partials [ngroups][nline][height][npts], or null
 };
 
-// table entry: bin d and fraction f >= 0 (f == 0: the single sample y[d]),
-// or f < 0: no contribution
-struct __align__(8) VPos {
-  int d;
-  float f;
+// table entry of one (point, angle): the two taps d0 <= d1 (equal for a
+// single sample), the fraction f, and live = 1 when the point receives a
+// value (else 0: d0 = d1 = 0 keeps the reads in bounds and the value is
+// discarded by a select, so no NaN or inf sample can leak in)
+struct __align__(16) VPos {
+  int d0, d1;
+  float f, live;
 };
 
 __device__ __forceinline__ VPos make_pos(const VArgs &a, const double2 *pts, int n, int je) {
-  VPos v = {0, -1.0f};
+  VPos v = {0, 0, 0.0f, 0.0f};
   const double2 cs = a.trig[n];
   const double2 xy = pts[je];
   // same expression and rounding order as the reference: (x cos + y sin) + center
@@ -70,26 +72,60 @@ __device__ __forceinline__ VPos make_pos(const VArgs &a, const double2 *pts, int
   const int width1 = a.width - 1;
   if (p >= 0.0 && p <= (double)width1) {
     const double fl = floor(p);
-    v.d = (int)fl;
-    v.f = (float)(p - fl);  // exact difference; 0 when u == d
+    v.d0 = (int)fl;
+    v.f = (float)(p - fl);  // exact difference; 0 when ceil(p) == floor(p)
+    v.d1 = v.f > 0.0f ? v.d0 + 1 : v.d0;
+    v.live = 1.0f;
   } else if (a.edge_pad) {
-    v.d = p < 0.0 ? 0 : width1;
-    v.f = 0.0f;
+    v.d0 = v.d1 = p < 0.0 ? 0 : width1;
+    v.live = 1.0f;
   }
   return v;
 }
 
-// the two samples of entry v in one row (both y[d] when f == 0; nothing
-// read when f < 0)
-__device__ __forceinline__ void taps(const float *row, VPos v, float &y0, float &y1) {
-  y0 = y1 = 0.0f;
-  if (v.f >= 0.0f) {
-    y0 = __ldg(row + v.d);
-    y1 = __ldg(row + (v.f > 0.0f ? v.d + 1 : v.d));
+// the angles [0, nang) of the current table for this thread's rows; kFull:
+// all kRowsPerThread rows exist (no predicates)
+template <bool kFull>
+__device__ __forceinline__ void accumulate(const VPos (*tab)[kPts], int pl, int nang, const float *base,
+                                           long long ps, const int *roff, int nr, float *part) {
+  int an = 0;
+  for (; an + 1 < nang; an += 2, base += 2 * ps) {
+    // both angles' samples are requested before any is used
+    const VPos v0 = tab[an][pl], v1 = tab[an + 1][pl];
+    const float *b1 = base + ps;
+    float y[2][kRowsPerThread][2];
+#pragma unroll
+    for (int r = 0; r < kRowsPerThread; ++r) {
+      if (kFull || r < nr) {
+        y[0][r][0] = __ldg(base + roff[r] + v0.d0);
+        y[0][r][1] = __ldg(base + roff[r] + v0.d1);
+        y[1][r][0] = __ldg(b1 + roff[r] + v1.d0);
+        y[1][r][1] = __ldg(b1 + roff[r] + v1.d1);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRowsPerThread; ++r) {
+      if (kFull || r < nr) {
+        const float a0 = y[0][r][0] + (y[0][r][1] - y[0][r][0]) * v0.f;
+        const float a1 = y[1][r][0] + (y[1][r][1] - y[1][r][0]) * v1.f;
+        part[r] += (v0.live != 0.0f ? a0 : 0.0f) + (v1.live != 0.0f ? a1 : 0.0f);
+      }
+    }
+  }
+  if (an < nang) {
+    const VPos v0 = tab[an][pl];
+#pragma unroll
+    for (int r = 0; r < kRowsPerThread; ++r) {
+      if (kFull || r < nr) {
+        const float y0 = __ldg(base + roff[r] + v0.d0), y1 = __ldg(base + roff[r] + v0.d1);
+        const float a0 = y0 + (y1 - y0) * v0.f;
+        part[r] += v0.live != 0.0f ? a0 : 0.0f;
+      }
+    }
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 3) vbp_kernel(VArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) vbp_kernel(VArgs a) {
   __shared__ VPos tab[kAng][kPts];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int line = blockIdx.x / a.npb, pb = blockIdx.x - line * a.npb;
@@ -113,7 +149,7 @@ __global__ void __launch_bounds__(kThreads, 3) vbp_kernel(VArgs a) {
     __syncthreads();  // the previous table is no longer read
     for (int e = tid; e < kAng * kPts; e += kThreads) {
       const int an = e / kPts, pe = e - an * kPts, je = j0 + pe;
-      tab[an][pe] = (an < nang && je < a.npts) ? make_pos(a, pts, n0 + an, je) : VPos{0, -1.0f};
+      tab[an][pe] = (an < nang && je < a.npts) ? make_pos(a, pts, n0 + an, je) : VPos{0, 0, 0.0f, 0.0f};
     }
     __syncthreads();
     if (j < a.npts && nr > 0) {
@@ -122,39 +158,10 @@ __global__ void __launch_bounds__(kThreads, 3) vbp_kernel(VArgs a) {
 #pragma unroll
       for (int r = 0; r < kRowsPerThread; ++r) part[r] = 0.0f;
       const float *base = a.proj + (long long)n0 * a.ps;
-      int an = 0;
-      for (; an + 1 < nang; an += 2, base += 2 * a.ps) {
-        // both angles' samples are requested before any is used
-        const VPos v0 = tab[an][pl], v1 = tab[an + 1][pl];
-        float y[2][kRowsPerThread][2];
-#pragma unroll
-        for (int r = 0; r < kRowsPerThread; ++r) {
-          if (r < nr) {
-            taps(base + roff[r], v0, y[0][r][0], y[0][r][1]);
-            taps(base + a.ps + roff[r], v1, y[1][r][0], y[1][r][1]);
-          }
-        }
-        const float f0 = fmaxf(v0.f, 0.0f), f1 = fmaxf(v1.f, 0.0f);
-#pragma unroll
-        for (int r = 0; r < kRowsPerThread; ++r) {
-          if (r < nr) {
-            part[r] += y[0][r][0] + (y[0][r][1] - y[0][r][0]) * f0;
-            part[r] += y[1][r][0] + (y[1][r][1] - y[1][r][0]) * f1;
-          }
-        }
-      }
-      if (an < nang) {
-        const VPos v0 = tab[an][pl];
-        const float f0 = fmaxf(v0.f, 0.0f);
-#pragma unroll
-        for (int r = 0; r < kRowsPerThread; ++r) {
-          if (r < nr) {
-            float y0, y1;
-            taps(base + roff[r], v0, y0, y1);
-            part[r] += y0 + (y1 - y0) * f0;
-          }
-        }
-      }
+      if (nr == kRowsPerThread)
+        accumulate<true>(tab, pl, nang, base, a.ps, roff, nr, part);
+      else
+        accumulate<false>(tab, pl, nang, base, a.ps, roff, nr, part);
 #pragma unroll
       for (int r = 0; r < kRowsPerThread; ++r) acc[r] += (double)part[r];
     }
@@ -189,8 +196,8 @@ __global__ void vbp_reduce_kernel(const double *__restrict__ part, int ngroups, 
   }
 }
 
-// angle groups for a launch of `base` CTAs: enough for about four full
-// waves of 3 CTAs per SM, at least one 32-angle table per group
+// angle groups for a launch of `base` CTAs: enough for about 1776 CTAs
+// (six waves of 2 CTAs per SM), at least one 32-angle table per group
 int vbp_groups(int nproj, long long base) {
   const long long want = 4LL * 148 * 3;
   long long g = (want + base - 1) / base;
