@@ -16,8 +16,9 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
            "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
            "atb_backproject_batch_noalloc", "atb_gaussian_rows",
-           "atb_zoom_linear", "atb_image_range", "atb_slice_metric_workspace",
-           "atb_slice_metric", "atb_vertical_backproject",
+           "atb_gaussian_cols", "atb_zoom_linear", "atb_image_range",
+           "atb_slice_metric_workspace", "atb_slice_metric",
+           "atb_slice_entropy64", "atb_vertical_backproject",
            "atb_vertical_workspace", "atb_flat_log", "atb_shift_rows",
            "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid")
 
@@ -74,6 +75,9 @@ _SIGS = {
     "atb_gaussian_rows": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
         _c_i64, _vp]),
+    "atb_gaussian_cols": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+        ctypes.c_int, _vp, _c_i64, _c_i64, _vp]),
     "atb_zoom_linear": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, _c_i64, ctypes.c_int,
         ctypes.c_int, _vp]),
@@ -85,9 +89,12 @@ _SIGS = {
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, ctypes.c_float, ctypes.c_float, _vp, _c_i64, _vp,
         _vp]),
+    "atb_slice_entropy64": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_double, ctypes.c_double, _vp, _c_i64, _vp, _vp]),
     "atb_vertical_backproject": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
-        _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp,
         ctypes.c_int, _vp, _c_i64, _c_i64, _vp, _c_i64, _vp]),
     "atb_vertical_workspace": (_c_i64, [
         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

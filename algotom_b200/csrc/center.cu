@@ -10,6 +10,11 @@
 //   explicitly rounded operations (no contraction), half-sample symmetric
 //   extension, then rounded to float32: the same operations in the same
 //   order as scipy's correlate1d, hence the same float32 results.
+// - atb_gaussian_cols: the same filter down the columns of a batch of
+//   images (gaussian_filter1d along axis 1 of a [n, rows, cols] stack; the
+//   first pass of gaussian_filter(projections, (0, sigma, sigma)) in
+//   vertrec.py:1349), each CTA staging a 32-column strip of rows plus the
+//   halo in shared memory.
 // - atb_zoom_linear: scipy.ndimage.zoom(x, z, order=1, mode="nearest")
 //   (reconstruction.py:1427): sample k of an axis sits at input coordinate
 //   k (n-1)/(m-1), clamped to [0, n-1]; the four bilinear taps are summed in
@@ -20,6 +25,8 @@
 //   (reconstruction.py:1212-1221 after the normalisation of :1243-1245) or
 //   the edge sharpness (:1224-1229).  Both reductions are deterministic:
 //   integer histogram counts, and FP64 partial sums reduced in a fixed order.
+//   atb_slice_entropy64 is the entropy of float64 images, normalised in FP64
+//   (the vertical-slice search, vertrec.py:1389-1392).
 #include <cmath>
 
 #include "common.cuh"
@@ -27,6 +34,10 @@
 namespace {
 
 constexpr int kRowTile = 256;        // output samples per CTA (Gaussian)
+constexpr int kColTile = 32;         // columns per CTA (Gaussian, columns)
+constexpr int kColRows = 64;         // output rows per CTA (Gaussian, columns)
+constexpr int kColThreads = 256;
+constexpr int kMaxColRadius = 700;   // strip + halo: <= 190 KB of shared memory
 constexpr int kMaxGaussRadius = 8192;
 constexpr int kMetricThreads = 256;
 constexpr int kMetricBlocks = 256;   // partial sums per image (sharpness)
@@ -45,8 +56,8 @@ __global__ void __launch_bounds__(kRowTile) gaussian_rows_kernel(const float *__
   extern __shared__ __align__(16) unsigned char smem[];
   double *ws = reinterpret_cast<double *>(smem);            // [radius + 1]
   float *xs = reinterpret_cast<float *>(ws + radius + 1);   // [kRowTile + 2 radius]
-  const int row = blockIdx.y;
-  const int c0 = blockIdx.x * kRowTile;
+  const long long row = blockIdx.x;
+  const int c0 = blockIdx.y * kRowTile;
   const float *x = src + (long long)row * srs;
   for (int j = threadIdx.x; j <= radius; j += kRowTile) ws[j] = w[j];
   const int span = kRowTile + 2 * radius;
@@ -59,7 +70,40 @@ __global__ void __launch_bounds__(kRowTile) gaussian_rows_kernel(const float *__
   double acc = __dmul_rn((double)xc[0], ws[0]);
   for (int j = 1; j <= radius; ++j)
     acc = __dadd_rn(acc, __dmul_rn(__dadd_rn((double)xc[j], (double)xc[-j]), ws[j]));
-  dst[(long long)row * drs + c] = __double2float_rn(acc);
+  dst[row * drs + c] = __double2float_rn(acc);
+}
+
+// Column pass: CTA (x, y, z) filters columns [32 x, 32 x + 32) of rows
+// [64 y, 64 y + 64) of image z; threads (lane = column, warp = row phase)
+// read the strip with its halo row by row (coalesced), then each output
+// takes the symmetric sum down its column in shared memory.
+__global__ void __launch_bounds__(kColThreads)
+    gaussian_cols_kernel(const float *__restrict__ src, long long sis, long long srs, int nrow, int ncol,
+                         const double *__restrict__ w, int radius, float *__restrict__ dst, long long dis,
+                         long long drs) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *ws = reinterpret_cast<double *>(smem);           // [radius + 1]
+  float *xs = reinterpret_cast<float *>(ws + radius + 1);  // [kColRows + 2 radius][kColTile]
+  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+  const int c = blockIdx.x * kColTile + lane;
+  const int r0 = blockIdx.y * kColRows;
+  const float *img = src + blockIdx.z * sis;
+  for (int j = threadIdx.x; j <= radius; j += kColThreads) ws[j] = w[j];
+  const int span = kColRows + 2 * radius;
+  for (int j = wy; j < span; j += kColThreads / 32)
+    xs[j * kColTile + lane] = c < ncol ? img[reflect_index((long long)r0 - radius + j, nrow) * srs + c] : 0.0f;
+  __syncthreads();
+  if (c >= ncol) return;
+  float *out = dst + blockIdx.z * dis;
+  for (int k = wy; k < kColRows; k += kColThreads / 32) {
+    const int r = r0 + k;
+    if (r >= nrow) break;
+    const float *xc = xs + (radius + k) * kColTile + lane;
+    double acc = __dmul_rn((double)xc[0], ws[0]);
+    for (int j = 1; j <= radius; ++j)
+      acc = __dadd_rn(acc, __dmul_rn(__dadd_rn((double)xc[j * kColTile], (double)xc[-j * kColTile]), ws[j]));
+    out[r * drs + c] = __double2float_rn(acc);
+  }
 }
 
 struct ZoomAxis {
@@ -159,14 +203,22 @@ __device__ __forceinline__ int level_u8(float v, float nmin, float range) {
 }
 
 // counts[img][256] += histogram of this CTA's share of image blockIdx.y
-__global__ void __launch_bounds__(kMetricThreads) histogram_kernel(const float *__restrict__ imgs, long long is,
-                                                                   long long rs, int rows, int cols, float nmin,
-                                                                   float nmax, int *counts) {
+// the same in FP64 (float64 images normalised by float64 bounds)
+__device__ __forceinline__ int level_u8(double v, double nmin, double range) {
+  double r = __ddiv_rn(__dsub_rn(v, nmin), range);
+  r = fmin(fmax(r, 0.0), 1.0);
+  return (int)__dmul_rn(r, 255.0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMetricThreads) histogram_kernel(const T *__restrict__ imgs, long long is,
+                                                                   long long rs, int rows, int cols, T nmin,
+                                                                   T nmax, int *counts) {
   __shared__ int h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
-  const float *img = imgs + blockIdx.y * is;
-  const float range = __fsub_rn(nmax, nmin);
+  const T *img = imgs + blockIdx.y * is;
+  const T range = nmax - nmin;  // one rounded subtraction in T
   const long long n = (long long)rows * cols;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(i / cols), c = (int)(i - (long long)r * cols);
@@ -252,16 +304,44 @@ extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int n
   if (!src || !dst || !weights) return atb::fail(ATB_EINVAL, "atb_gaussian_rows: null pointer");
   if (nrow < 1 || ncol < 1 || radius < 0)
     return atb::fail(ATB_EINVAL, "atb_gaussian_rows: bad shape nrow=%d ncol=%d radius=%d", nrow, ncol, radius);
-  if (nrow > 65535 || radius > kMaxGaussRadius)
-    return atb::fail(ATB_ERANGE, "atb_gaussian_rows: nrow=%d or radius=%d too large", nrow, radius);
+  if (ncol > 65535 * kRowTile || radius > kMaxGaussRadius)
+    return atb::fail(ATB_ERANGE, "atb_gaussian_rows: ncol=%d or radius=%d too large", ncol, radius);
   if (src == dst) return atb::fail(ATB_EINVAL, "atb_gaussian_rows: in-place filtering is not supported");
   const size_t smem = sizeof(double) * (radius + 1) + sizeof(float) * (kRowTile + 2 * (size_t)radius);
   int rc = atb::ensure_smem(gaussian_rows_kernel, smem, "atb_gaussian_rows");
   if (rc != ATB_OK) return rc;
-  dim3 grid((ncol + kRowTile - 1) / kRowTile, nrow);
+  dim3 grid(nrow, (ncol + kRowTile - 1) / kRowTile);
   gaussian_rows_kernel<<<grid, kRowTile, smem, atb::as_stream(stream)>>>(src, src_row_stride, ncol, weights, radius,
                                                                            dst, dst_row_stride);
   return atb::check_launch("atb_gaussian_rows");
+}
+
+extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64_t src_row_stride, int nimg,
+                                 int nrow, int ncol, const double *weights, int radius, float *dst,
+                                 int64_t dst_img_stride, int64_t dst_row_stride, void *stream) {
+  if (!src || !dst || !weights) return atb::fail(ATB_EINVAL, "atb_gaussian_cols: null pointer");
+  if (nimg < 1 || nrow < 1 || ncol < 1 || radius < 0)
+    return atb::fail(ATB_EINVAL, "atb_gaussian_cols: bad shape nimg=%d nrow=%d ncol=%d radius=%d", nimg, nrow,
+                     ncol, radius);
+  if (src == dst) return atb::fail(ATB_EINVAL, "atb_gaussian_cols: in-place filtering is not supported");
+  if ((int64_t)nrow * src_row_stride > 2147483647LL || (int64_t)nrow * dst_row_stride > 2147483647LL)
+    return atb::fail(ATB_ERANGE, "atb_gaussian_cols: image of %d rows too large", nrow);
+  if (radius > kMaxColRadius) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: radius=%d too large", radius);
+  const size_t smem = sizeof(double) * (radius + 1) + sizeof(float) * kColTile * (kColRows + 2 * (size_t)radius);
+  int rc = atb::ensure_smem(gaussian_cols_kernel, smem, "atb_gaussian_cols");
+  if (rc != ATB_OK) return rc;
+  const int gx = (ncol + kColTile - 1) / kColTile, gy = (nrow + kColRows - 1) / kColRows;
+  if (gy > 65535) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: nrow=%d too large", nrow);
+  cudaStream_t st = atb::as_stream(stream);
+  for (int z0 = 0; z0 < nimg; z0 += 65535) {
+    const int nz = nimg - z0 < 65535 ? nimg - z0 : 65535;
+    gaussian_cols_kernel<<<dim3(gx, gy, nz), kColThreads, smem, st>>>(
+        src + z0 * src_img_stride, src_img_stride, src_row_stride, nrow, ncol, weights, radius,
+        dst + z0 * dst_img_stride, dst_img_stride, dst_row_stride);
+    rc = atb::check_launch("atb_gaussian_cols");
+    if (rc != ATB_OK) return rc;
+  }
+  return ATB_OK;
 }
 
 extern "C" int atb_zoom_linear(const float *src, int64_t src_row_stride, int in_rows, int in_cols, float *dst,
@@ -316,8 +396,8 @@ extern "C" int atb_slice_metric(const float *imgs, int64_t img_stride, int64_t r
     int *counts = static_cast<int *>(work);
     cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * 256 * (size_t)nimg, st);
     if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_slice_metric: %s", cudaGetErrorString(e));
-    histogram_kernel<<<dim3(nblk, nimg), kMetricThreads, 0, st>>>(imgs, img_stride, row_stride, rows, cols, nmin,
-                                                                  nmax, counts);
+    histogram_kernel<float><<<dim3(nblk, nimg), kMetricThreads, 0, st>>>(imgs, img_stride, row_stride, rows, cols,
+                                                                         nmin, nmax, counts);
     int rc = atb::check_launch("atb_slice_metric");
     if (rc != ATB_OK) return rc;
     entropy_kernel<<<nimg, kMetricThreads, 0, st>>>(counts, out);
@@ -335,4 +415,26 @@ extern "C" int atb_slice_metric(const float *imgs, int64_t img_stride, int64_t r
     return atb::check_launch("atb_slice_metric");
   }
   return atb::fail(ATB_EINVAL, "atb_slice_metric: unknown metric %d", metric);
+}
+
+extern "C" int atb_slice_entropy64(const double *imgs, int64_t img_stride, int64_t row_stride, int nimg, int rows,
+                                   int cols, double nmin, double nmax, void *work, int64_t work_bytes, double *out,
+                                   void *stream) {
+  if (!imgs || !work || !out) return atb::fail(ATB_EINVAL, "atb_slice_entropy64: null pointer");
+  if (nimg < 1 || rows < 1 || cols < 1)
+    return atb::fail(ATB_EINVAL, "atb_slice_entropy64: bad shape nimg=%d rows=%d cols=%d", nimg, rows, cols);
+  if (nimg > 65535) return atb::fail(ATB_ERANGE, "atb_slice_entropy64: nimg=%d too large", nimg);
+  if (work_bytes < atb_slice_metric_workspace(nimg, rows, cols, ATB_METRIC_ENTROPY))
+    return atb::fail(ATB_EINVAL, "atb_slice_entropy64: workspace of %lld bytes is too small", (long long)work_bytes);
+  cudaStream_t st = atb::as_stream(stream);
+  const int nblk = metric_blocks((long long)rows * cols);
+  int *counts = static_cast<int *>(work);
+  cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * 256 * (size_t)nimg, st);
+  if (e != cudaSuccess) return atb::fail(ATB_ECUDA, "atb_slice_entropy64: %s", cudaGetErrorString(e));
+  histogram_kernel<double><<<dim3(nblk, nimg), kMetricThreads, 0, st>>>(imgs, img_stride, row_stride, rows, cols,
+                                                                        nmin, nmax, counts);
+  int rc = atb::check_launch("atb_slice_entropy64");
+  if (rc != ATB_OK) return rc;
+  entropy_kernel<<<nimg, kMetricThreads, 0, st>>>(counts, out);
+  return atb::check_launch("atb_slice_entropy64");
 }

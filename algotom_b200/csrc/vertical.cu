@@ -47,6 +47,7 @@ struct VArgs {
   long long pls;          // point stride between lines
   int npts, nline, npb;   // points per line, lines, point blocks per line
   double center;
+  const double *line_centers;  // per-line centre, or null (all `center`)
   int edge_pad;
   double *acc;
   long long als, ars;  // accumulator line / row strides
@@ -63,12 +64,12 @@ struct __align__(16) VPos {
   float f, live;
 };
 
-__device__ __forceinline__ VPos make_pos(const VArgs &a, const double2 *pts, int n, int je) {
+__device__ __forceinline__ VPos make_pos(const VArgs &a, const double2 *pts, int n, int je, double center) {
   VPos v = {0, 0, 0.0f, 0.0f};
   const double2 cs = a.trig[n];
   const double2 xy = pts[je];
   // same expression and rounding order as the reference: (x cos + y sin) + center
-  const double p = __dadd_rn(__dadd_rn(__dmul_rn(xy.x, cs.x), __dmul_rn(xy.y, cs.y)), a.center);
+  const double p = __dadd_rn(__dadd_rn(__dmul_rn(xy.x, cs.x), __dmul_rn(xy.y, cs.y)), center);
   const int width1 = a.width - 1;
   if (p >= 0.0 && p <= (double)width1) {
     const double fl = floor(p);
@@ -135,6 +136,7 @@ __global__ void __launch_bounds__(kThreads, 2) vbp_kernel(VArgs a) {
   const int r0 = blockIdx.y * kRows + (warp >> 1) * kRowsPerThread;
   const int nr = min(kRowsPerThread, a.height - r0);  // live rows (may be <= 0)
   const double2 *pts = a.points + line * a.pls;
+  const double center = a.line_centers ? a.line_centers[line] : a.center;
   const int g0 = blockIdx.z * a.apg, g1 = min(a.nproj, g0 + a.apg);
   // 32-bit row offsets: one projection holds fewer than 2^31 samples
   int roff[kRowsPerThread];
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, 2) vbp_kernel(VArgs a) {
     __syncthreads();  // the previous table is no longer read
     for (int e = tid; e < kAng * kPts; e += kThreads) {
       const int an = e / kPts, pe = e - an * kPts, je = j0 + pe;
-      tab[an][pe] = (an < nang && je < a.npts) ? make_pos(a, pts, n0 + an, je) : VPos{0, 0, 0.0f, 0.0f};
+      tab[an][pe] = (an < nang && je < a.npts) ? make_pos(a, pts, n0 + an, je, center) : VPos{0, 0, 0.0f, 0.0f};
     }
     __syncthreads();
     if (j < a.npts && nr > 0) {
@@ -246,8 +248,9 @@ extern "C" int64_t atb_vertical_workspace(int nproj, int height, int npts, int n
 
 extern "C" int atb_vertical_backproject(const float *proj, int64_t proj_stride, int64_t row_stride, int nproj,
                                         int height, int width, const double *trig, const double *points,
-                                        int64_t line_stride, int npts, int nline, double center, int edge_pad,
-                                        double *acc, int64_t acc_line_stride, int64_t acc_row_stride, void *work,
+                                        int64_t line_stride, int npts, int nline, double center,
+                                        const double *line_centers, int edge_pad, double *acc,
+                                        int64_t acc_line_stride, int64_t acc_row_stride, void *work,
                                         int64_t work_bytes, void *stream) {
   if (!proj || !trig || !points || !acc) return atb::fail(ATB_EINVAL, "atb_vertical_backproject: null pointer");
   if (nproj < 1 || height < 1 || width < 1 || npts < 1 || nline < 1)
@@ -266,7 +269,7 @@ extern "C" int atb_vertical_backproject(const float *proj, int64_t proj_stride, 
   a.trig = reinterpret_cast<const double2 *>(trig);
   a.points = reinterpret_cast<const double2 *>(points);
   a.pls = line_stride; a.npts = npts; a.nline = nline; a.npb = npb;
-  a.center = center; a.edge_pad = edge_pad ? 1 : 0;
+  a.center = center; a.line_centers = line_centers; a.edge_pad = edge_pad ? 1 : 0;
   a.acc = acc; a.als = acc_line_stride; a.ars = acc_row_stride;
   // split the angles over CTAs when the caller's scratch holds the partials
   const long long elems = (long long)nline * height * npts;

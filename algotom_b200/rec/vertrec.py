@@ -36,6 +36,7 @@ import torch
 from .. import _native as nat
 from . import reconstruction as R
 from . import windows as win
+from .center import _gaussian_weights, slice_metrics
 from .padding import pad_rows
 
 _WARN_FULL = ("!!! Applying logarithm is enabled but there are values <= 0.0"
@@ -133,15 +134,20 @@ def _points(x_mat, y_mat, width, device, round32):
 def _backproject(proj, trig, pts, center, edge_pad, acc):
     """acc [nline, height, npts] += vertical back-projection of the float32
     CUDA slab ``proj`` [n, height, width] (last axis contiguous), with
-    scratch for the split of the angles over CTAs when the output is small."""
+    scratch for the split of the angles over CTAs when the output is small.
+    ``center``: a number, or a float64 CUDA tensor with one centre per
+    line."""
     n, height, width = proj.shape
     nline, npts = pts.shape[0], pts.shape[1]
     nbytes = nat.call("atb_vertical_workspace", n, height, npts, nline)
     work = torch.empty(int(nbytes), dtype=torch.uint8, device=proj.device) \
         if nbytes > 0 else None
+    per_line = isinstance(center, torch.Tensor)
     nat.call("atb_vertical_backproject", proj.data_ptr(), proj.stride(0),
              proj.stride(1), n, height, width, trig.data_ptr(),
-             pts.data_ptr(), npts, npts, nline, float(center),
+             pts.data_ptr(), npts, npts, nline,
+             0.0 if per_line else float(center),
+             center.data_ptr() if per_line else None,
              int(bool(edge_pad)), acc.data_ptr(), acc.stride(0),
              acc.stride(1), work.data_ptr() if work is not None else None,
              int(nbytes), R._stream_ptr(proj.device))
@@ -445,12 +451,35 @@ def _fields(flat_field, dark_field, height0, width0, top, bot, left, right):
     return np.float32(dark), np.float32(flat_dark)
 
 
+def _gaussian_slab(x, wts, tmp, out):
+    """``gaussian_filter(x, (0, sigma, sigma))`` of a float32 CUDA slab
+    [n, height, width] (last axis contiguous) into ``out``: down the
+    columns into ``tmp``, then along the rows; float32 between the passes,
+    as scipy."""
+    n, height, width = x.shape
+    r = wts.numel() - 1
+    st = R._stream_ptr(x.device)
+    nat.call("atb_gaussian_cols", x.data_ptr(), x.stride(0), x.stride(1), n,
+             height, width, wts.data_ptr(), r, tmp.data_ptr(), tmp.stride(0),
+             tmp.stride(1), st)
+    nat.call("atb_gaussian_rows", tmp.data_ptr(), width, n * height, width,
+             wts.data_ptr(), r, out.data_ptr(), width, st)
+
+
 def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
                  dark_field, chunk_size, ramp_filter, filter_name, pad,
                  pad_mode, apply_log, gpu, show_progress, masking,
-                 round_points):
+                 round_points, line_centers=None, sigma=0.0,
+                 log_warning=None, device_out=False):
     """The chunk loop of ``vertrec.py:584-695`` for any set of slices;
-    returns float64 [num_slice, height, width] (NumPy for host input)."""
+    returns float64 [num_slice, height, width] (NumPy for host input unless
+    ``device_out``).
+
+    ``line_centers``: one centre per slice instead of ``center``.
+    ``sigma`` > 0: each projection is smoothed first (the Gaussian of a
+    centre search, ``vertrec.py:1348-1349``).  ``log_warning``: one warning
+    with this text if ``-log`` met values <= 0 anywhere, instead of the
+    reconstructions' per-chunk warnings ("": no warning)."""
     (num_proj0, height0, width0, proj_stop, num_proj, angles, top, bot,
      left, right, width, height) = geo
     proj_start = proj_stop - num_proj
@@ -477,7 +506,15 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
     trig = _trig_plus(angles, dev, gpu)
     pts = _points(x_mat, y_mat, width, dev, gpu or round_points)
     c = float(np.float32(center)) if gpu else float(center)
+    if line_centers is not None:
+        lc = np.asarray(line_centers, dtype=np.float64)
+        if gpu:
+            lc = np.float32(lc).astype(np.float64)
+        c = torch.from_numpy(np.ascontiguousarray(lc)).to(dev)
     nline = pts.shape[0]
+    wts = None
+    if sigma > 0:
+        wts = torch.from_numpy(_gaussian_weights(sigma)).to(dev)
     acc = torch.zeros((nline, height, width), dtype=torch.float64,
                       device=dev)
     log2m = nat.call("atb_filter_log2m", int(width), int(pad))
@@ -492,7 +529,7 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
         spans.append((start, start + num_rest))
     nonpos = torch.zeros(len(spans), dtype=torch.int32, device=dev)
     chunks = _Chunks(projections, top, bot, left, right, dev)
-    preprocess = apply_log or dark is not None
+    preprocess = apply_log or dark is not None or wts is not None
     item = 4 if chunks.pinned is None else chunks.pinned.element_size()
     slabs = _slabs(spans, chunk_size * height * width * item, is_cuda,
                    preprocess or (is_cuda and projections.dtype !=
@@ -512,7 +549,19 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
                 pre = torch.empty((n, height, width), dtype=torch.float32,
                                   device=dev)
                 work[("pre", n)] = pre
+            if wts is not None:
+                tmp = work.get(("tmp", n))
+                if tmp is None:
+                    tmp = torch.empty_like(pre)
+                    work[("tmp", n)] = tmp
+                if code != nat.F32:  # counts to float32 first
+                    _flat_log(raw, code, None, None, False, pre, nonpos[:1])
+                    raw = pre
+                _gaussian_slab(raw, wts, tmp, pre)
+                raw, code = pre, nat.F32
             for k in range(k0, k1):  # one warning counter per chunk
+                if raw is pre and not apply_log and dark is None:
+                    break  # smoothed, nothing else to do
                 a, b = spans[k][0] - s0, spans[k][1] - s0
                 _flat_log(raw[a:b], code, dark, flat_dark, apply_log,
                           pre[a:b], nonpos[k:k + 1])
@@ -542,10 +591,13 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
     del acc
     if apply_log:
         counts = nonpos.cpu().numpy()
+        if log_warning and counts.any():
+            warnings.warn(log_warning)
         for k, (start, stop) in enumerate(spans):
             if counts[k] > 0:
-                warnings.warn(_WARN_FULL if k < num_iter else _WARN_REST)
-                if dark is None:
+                if log_warning is None:
+                    warnings.warn(_WARN_FULL if k < num_iter else _WARN_REST)
+                if dark is None and wts is None:
                     chunks.repair(start, stop)
     if show_progress:
         print("\nDone! Total time elapsed: {0:.2f}".format(time.time() - t0))
@@ -556,7 +608,7 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
         m[pad_left:pad_left + 2 * rad] = 1.0
         ver = ver * m
     ver = (ver * np.pi) / (num_proj - 1)
-    return ver if is_cuda else ver.cpu().numpy()
+    return ver if is_cuda or device_out else ver.cpu().numpy()
 
 
 def _as_dtype(x, np_dtype):
@@ -653,3 +705,156 @@ def vertical_reconstruction_different_angles(projections, slice_indices,
         projections, x_mat, y_mat, center, geo, flat_field, dark_field,
         chunk_size, ramp_filter, filter_name, pad, pad_mode, apply_log, gpu,
         show_progress, masking, round_points=True), np.float32)
+
+
+# --------------------------------------------------------------------------
+# centre search on a vertical slice (vertrec.py:1255-1383)
+# --------------------------------------------------------------------------
+_SEARCH_BYTES = 4 << 30  # FP64 slices reconstructed per pass over the data
+
+
+def _autocorrelation(imgs):
+    """``mean(max(|ifft(|fft(row)|^2)|, axis=1))`` of every float32 image
+    of [n, rows, cols] (``vertrec.py:1255-1261``; library FFT)."""
+    f = torch.fft.fft(imgs, dim=-1)
+    ac = torch.fft.ifft(f.abs() ** 2, dim=-1).abs()
+    return ac.amax(dim=-1).to(torch.float64).mean(dim=-1).cpu().numpy()
+
+
+def _entropy(imgs, nmin, nmax):
+    """Histogram entropy of [n, rows, cols] slices normalised by
+    (nmin, nmax), in the slices' precision."""
+    if imgs.dtype == torch.float32:
+        return slice_metrics(imgs, "entropy", nmin, nmax)
+    imgs = imgs.contiguous()
+    n, rows, cols = imgs.shape
+    nbytes = nat.call("atb_slice_metric_workspace", n, rows, cols,
+                      nat.METRICS["entropy"])
+    work = torch.empty(int(nbytes), dtype=torch.uint8, device=imgs.device)
+    out = torch.empty(n, dtype=torch.float64, device=imgs.device)
+    nat.call("atb_slice_entropy64", imgs.data_ptr(), imgs.stride(0),
+             imgs.stride(1), n, rows, cols, float(nmin), float(nmax),
+             work.data_ptr(), work.numel(), out.data_ptr(),
+             R._stream_ptr(imgs.device))
+    return out.cpu().numpy()
+
+
+def find_center_vertical_slice(projections, slice_index, start, stop,
+                               step=1.0, metric="entropy", alpha=0.0,
+                               angles=None, chunk_size=30,
+                               ramp_filter="after", sigma=3, apply_log=True,
+                               gpu=True, block=(16, 16), ncore=None,
+                               prefer="threads", show_progress=True,
+                               masking=True, return_metric=False,
+                               invert_metric=False, metric_function=None,
+                               **kwargs):
+    """Centre of rotation from metrics of one vertical slice reconstructed
+    at every centre of ``np.arange(start, stop + step, step)``;
+    ``vertrec.py:1264-1383``.
+
+    The projections are smoothed (``sigma``) and ``-log``-ed on the device
+    chunk by chunk, and every candidate centre -- plus the mean centre that
+    sets the entropy's normalisation -- is a line of the same vertical
+    back-projection launch, so the data are read once for all of them
+    (in passes of about 4 GB of FP64 slices when there are many).  Metrics:
+    ``"entropy"``, ``"sharpness"`` (device kernels), ``"autocorrelation"``
+    (library FFT) or ``metric_function(recon, **kwargs)`` on each slice as a
+    NumPy array.  Returns the centre of the smallest metric, or
+    ``(list_center, list_metric)`` with ``return_metric``.
+    """
+    if (metric != "entropy" and metric != "sharpness"
+            and metric != "autocorrelation" and metric_function is None):
+        msg = "Please select one of three options: 'entropy', 'sharpness', " \
+              "'autocorrelation'; or provide a custom method."
+        raise ValueError(msg)
+    if ramp_filter is None:
+        ramp_filter = "after"
+    list_center = np.arange(start, stop + step, step)
+    list_metric = np.zeros_like(list_center)
+    num_metric = len(list_metric)
+    (num_proj, height, width) = projections.shape
+    if angles is None:
+        angles = np.deg2rad(np.linspace(0.0, 180.0, num_proj))
+    use_entropy = metric_function is None and metric == "entropy"
+    mean_center = np.mean(list_center) if use_entropy else None
+    # the reconstructions' own checks, for every centre they would get
+    geo = None
+    for cen in ([mean_center] if use_entropy else []) + list(list_center):
+        geo = _check_common(projections, cen, angles, (0, 0, 0, 0), 0, -1,
+                            ramp_filter)
+    if slice_index < 0 or slice_index > (width - 1):
+        raise ValueError("Index (relative to the cropped image) is out of "
+                         "range {})".format((0, width - 1)))
+    pad = min(int(0.15 * width), 150)
+    xlist, ylist = _get_points_single_line(slice_index, alpha, width)
+    out_dtype = torch.float64 if ramp_filter == "after" else torch.float32
+    mask = None
+    if masking:
+        rad = int(min(np.min(list_center), width - np.min(list_center)))
+        pad_left = (width - 2 * rad) // 2
+        pad_right = width - 2 * rad - pad_left
+        mask = np.pad(np.ones(2 * rad, dtype=np.float32),
+                      (pad_left, pad_right), mode="constant")
+    log_text = ("!!! Applying logarithm is enabled but there are values "
+                "<= 0.0 in the data !!!")
+    centers = ([mean_center] if use_entropy else []) + list(list_center)
+    per_pass = max(1, int(_SEARCH_BYTES // (8 * height * width)))
+    nmin = nmax = None
+    if show_progress:
+        t0 = time.time()
+    done = 0
+    for g0 in range(0, len(centers), per_pass):
+        group = centers[g0:g0 + per_pass]
+        xs = np.tile(np.asarray(xlist), (len(group), 1))
+        ys = np.tile(np.asarray(ylist), (len(group), 1))
+        recs = _reconstruct(
+            projections, xs, ys, group[0], geo, None, None, chunk_size,
+            ramp_filter, "hann", pad, "edge", apply_log, gpu, False, False,
+            round_points=False, line_centers=group, sigma=sigma,
+            log_warning=log_text if g0 == 0 else "", device_out=True)
+        recs = recs.to(out_dtype)
+        if use_entropy and g0 == 0:
+            first = recs[0]
+            if out_dtype == torch.float32:
+                nmin = np.float32(first.min().item())
+                nmax = np.float32(first.max().item())
+            else:
+                nmin, nmax = first.min().item(), first.max().item()
+            recs = recs[1:]
+        if mask is not None:
+            recs = recs * torch.from_numpy(mask).to(recs.device).to(
+                out_dtype)
+        k = len(recs)
+        if k == 0:
+            continue
+        if metric_function is not None:
+            host = recs.cpu().numpy()
+            values = [metric_function(host[i], **kwargs) for i in range(k)]
+        elif metric == "entropy":
+            values = _entropy(recs, nmin, nmax)
+        elif metric == "autocorrelation":
+            values = _autocorrelation(recs.to(torch.float32))
+        else:
+            values = slice_metrics(recs.to(torch.float32), "sharpness")
+        for i in range(k):
+            list_metric[done + i] = values[i]
+            if show_progress:
+                elapsed_time = time.time() - t0
+                percent_complete = 100.0 * (done + i + 1) / num_metric
+                sys.stdout.write(
+                    f"\rReconstructed image using the center: "
+                    f"{list_center[done + i]}. "
+                    f"Progress: {percent_complete:.0f}% - "
+                    f"Time elapsed: {elapsed_time:.2f} seconds")
+        done += k
+        del recs
+    if invert_metric:
+        list_metric = np.max(list_metric) - list_metric
+    min_pos = np.argmin(list_metric)
+    center = list_center[min_pos]
+    if show_progress:
+        print("\nDone! Optimal center: {0}.".format(center))
+    if return_metric is True:
+        return list_center, list_metric
+    else:
+        return center

@@ -61,7 +61,8 @@ def _args():
                     help="detector rows of the vertical workload")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
-                             "center", "vertical", "halfacq", "dfi"],
+                             "center", "vertical", "vcenter", "halfacq",
+                             "dfi"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
@@ -71,6 +72,7 @@ def _args():
                          "a CUDA graph; single: one 1024^2 x 900 slice; "
                          "center: centre search over 128 candidates; "
                          "vertical: vertical slices from 1801 projections; "
+                         "vcenter: centre search on a vertical slice; "
                          "halfacq: a 360-degree offset-axis slice extended "
                          "and reconstructed; dfi: direct Fourier inversion "
                          "of one slice")
@@ -827,6 +829,133 @@ def run_vertical(args):
         "gpu_launches": args.steps}), flush=True)
 
 
+def run_vcenter(args):
+    """Centre search on a vertical slice (``find_center_vertical_slice``)
+    over a projection stack of 1801 x rows x 2560 float32 (device-resident,
+    9.4 GB at 512 rows): Gaussian smoothing (sigma 3) of every projection,
+    41 candidate centres 0.5 px apart plus the mean centre as lines of one
+    vertical back-projection per chunk slab, FP64 "after" ramp filter,
+    entropy of every candidate slice.  The metric counts the pixel-angle
+    updates of the candidate slices.  e2e: from a pinned host array.
+    Accuracy: the search's metrics against a sequential check -- one
+    ``vertical_reconstruction`` per sampled candidate on the smoothed
+    projections and the entropy computed on the host with NumPy.  CPU
+    baseline: the FP64 oracle's vertical back-projection on 4 rows."""
+    import torch
+    from algotom_b200 import _native as nat
+    from algotom_b200.rec import vertrec as VR
+    dev = torch.device("cuda", 0)
+    height = args.rows
+    proj, ang = make_sinograms(height, dev)  # attenuation [1801][rows][2560]
+    torch.cuda.synchronize()
+    start, stop, step = CENTER - 10.0, CENTER + 10.0, 0.5
+    ncand = len(np.arange(start, stop + step, step))
+    kw = dict(angles=ang, apply_log=False, show_progress=False,
+              return_metric=True)
+
+    def search(src):
+        return VR.find_center_vertical_slice(src, NCOL // 2, start, stop,
+                                             step=step, **kw)
+
+    def timed(src, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            r = search(src)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / n, r
+
+    for _ in range(args.warmup):
+        search(proj)
+    sampler = ClockSampler(0)
+    sampler.start()
+    t, (cs, ms) = timed(proj, args.steps)
+    clocks = sampler.stop()
+    nbytes = proj.numel() * 4
+    t_e2e = None
+    if not args.no_e2e:
+        host = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+        host.copy_(proj)
+        search(host.numpy())
+        t_e2e, _ = timed(host.numpy(), max(1, args.steps // 2))
+        del host
+    upd = ncand * NROW * height * NCOL
+    # per slab of chunks: two Gaussian passes, the back-projection (+ the
+    # reduction of its angle groups when it splits them); then the entropy
+    # histogram and its reduction
+    nchunk = -(-NROW // 30)
+    nslab = len(VR._slabs([None] * nchunk, 30 * height * NCOL * 4, True,
+                          True))
+    per_slab = 30 * max(1, (1 << 29) // (30 * height * NCOL * 4))
+    split = nat.call("atb_vertical_workspace", min(NROW, per_slab), height,
+                     NCOL, ncand + 1) > 0
+    launches = nslab * (3 + int(split)) + 2
+    acc = cpu = None
+    if not args.no_oracle:
+        # sequential check: smoothed projections, one reconstruction per
+        # sampled candidate, the reference's entropy on the host
+        w = torch.from_numpy(VR._gaussian_weights(3)).to(dev)
+        sm, tmp = torch.empty_like(proj), torch.empty_like(proj)
+        VR._gaussian_slab(proj, w, tmp, sm)
+        del tmp
+        one = dict(angles=ang, apply_log=False, show_progress=False,
+                   pad=min(int(0.15 * NCOL), 150))
+        first = VR.vertical_reconstruction(sm, NCOL // 2, np.mean(cs),
+                                           **one).cpu().numpy()
+        nmin, nmax = first.min(), first.max()
+        rad = int(min(np.min(cs), NCOL - np.min(cs)))
+        mask = np.zeros(NCOL)
+        mask[(NCOL - 2 * rad) // 2:(NCOL - 2 * rad) // 2 + 2 * rad] = 1.0
+        errs = []
+        for i in (0, ncand // 2, ncand - 1):
+            r = VR.vertical_reconstruction(sm, NCOL // 2, cs[i],
+                                           **one).cpu().numpy() * mask
+            lv = np.uint8(np.clip((r - nmin) / (nmax - nmin), 0, 1) * 255)
+            h = 1.0 + np.bincount(lv.ravel(), minlength=256)
+            b = np.convolve(h, np.ones(7), mode="valid")
+            e = -np.sum(b * np.log2(b))
+            errs.append(abs(ms[i] - e) / abs(e))
+        del sm
+        acc = {"metric_rel_err_vs_sequential": float(max(errs)),
+               "candidates_checked": 3}
+        from oracle import vertical_oracle as VO
+        rows = sorted({0, height // 5, (3 * height) // 5, height - 1})
+        sub = proj[:, rows, :].cpu().numpy()
+        xs, ys = VO.points_single_line(NCOL // 2, 0.0, NCOL)
+        t0 = time.perf_counter()
+        VO.vertical_back_projection(sub, ang, xs, ys, CENTER, True)
+        t_cpu = time.perf_counter() - t0
+        cpu = {"value": len(rows) * NROW * NCOL / t_cpu, "unit": "updates/s",
+               "cores": 1, "kind": "port",
+               "sample": "FP64 NumPy vertical back-projection of %d detector "
+                         "rows for one centre, %.1f s" % (len(rows), t_cpu)}
+    pk, src = _peaks()
+    print(json.dumps({
+        "metric": "vertical centre-search pixel-angle updates/s at 2560 det",
+        "value": upd / t, "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded 12-ellipse phantoms)",
+        "config": {"workload": "find_center_vertical_slice, %d candidates, "
+                               "entropy, sigma 3, over 1801 projections of "
+                               "%d x 2560 (device-resident)" % (ncand, height),
+                   "l2": "inputs larger than L2 (%.1f GB)" % (nbytes / 1e9)},
+        "best_center": float(cs[np.argmin(ms)]),
+        "roofline": {"bound": "smem", "achieved": upd / t, "unit":
+                     "updates/s", "note": "whole search per step; the "
+                     "back-projection's own roofline is the vertical "
+                     "workload's", "peak_source": src},
+        "e2e": None if t_e2e is None else {
+            "value": upd / t_e2e, "unit": "updates/s",
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": ncand * 8,
+            "ms_per_step": t_e2e * 1e3},
+        "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
+        "gpu_launches": launches * args.steps}), flush=True)
+
+
 def run_halfacq(args):
     """Half-acquisition slice: a 360-degree sinogram of 3601 angles x 2560
     detector pixels whose rotation axis sits at 2300.4 (offset), extended on
@@ -986,6 +1115,9 @@ def main():
         return
     if args.workload == "vertical":
         run_vertical(args)
+        return
+    if args.workload == "vcenter":
+        run_vcenter(args)
         return
     if args.workload == "center":
         run_center(args)

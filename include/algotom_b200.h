@@ -265,11 +265,29 @@ int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems,
  *
  *   weights   device float64 [radius + 1]: the half kernel w[0..radius] of
  *             the unit-sum sampled Gaussian, radius = int(4 sigma + 0.5)
- *   dst       must not overlap src; radius <= 8192, nrow <= 65535
+ *   dst       must not overlap src; radius <= 8192, ncol <= 65535 * 256
  */
 int atb_gaussian_rows(const float *src, int64_t src_row_stride, int nrow,
                       int ncol, const double *weights, int radius,
                       float *dst, int64_t dst_row_stride, void *stream);
+
+/*
+ * The same filter down the columns of nimg float32 images
+ * (gaussian_filter1d along axis 1 of a [nimg, nrow, ncol] stack), the first
+ * pass of the projection smoothing gaussian_filter(projections,
+ * (0, sigma, sigma)) before a vertical-slice centre search
+ * (vertrec.py:1348-1349; the second pass is atb_gaussian_rows).  Same
+ * float32 results as scipy.
+ *
+ *   weights   as atb_gaussian_rows; radius <= 700 (the strip with its halo
+ *             fits in shared memory)
+ *   dst       must not overlap src; nrow * row_stride < 2^31
+ */
+int atb_gaussian_cols(const float *src, int64_t src_img_stride,
+                      int64_t src_row_stride, int nimg, int nrow, int ncol,
+                      const double *weights, int radius, float *dst,
+                      int64_t dst_img_stride, int64_t dst_row_stride,
+                      void *stream);
 
 /*
  * scipy.ndimage.zoom(x, zoom, order=1, mode="nearest") of a float32 image
@@ -310,6 +328,18 @@ int atb_slice_metric(const float *imgs, int64_t img_stride,
                      int metric, float nmin, float nmax, void *work,
                      int64_t work_bytes, double *out, void *stream);
 
+/*
+ * The histogram entropy of float64 images, normalised in FP64: the metric
+ * of find_center_vertical_slice (vertrec.py:1389-1392) on slices that the
+ * "after" ramp filter leaves in float64.  Arguments as atb_slice_metric
+ * (work: atb_slice_metric_workspace(nimg, rows, cols, ATB_METRIC_ENTROPY)
+ * bytes).
+ */
+int atb_slice_entropy64(const double *imgs, int64_t img_stride,
+                        int64_t row_stride, int nimg, int rows, int cols,
+                        double nmin, double nmax, void *work,
+                        int64_t work_bytes, double *out, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Vertical slices (algotom/rec/vertrec.py)                               */
 /* ---------------------------------------------------------------------- */
@@ -332,6 +362,9 @@ int atb_slice_metric(const float *imgs, int64_t img_stride,
  *   trig    float64 [nproj][2] = (cos a, sin a)  (note: +a, not -a)
  *   points  float64 [nline][npts][2] = (x, y), line_stride between lines
  *           (in points)
+ *   line_centers  device float64 [nline]: a centre per line (candidate
+ *           centres of one slice, find_center_vertical_slice), or NULL:
+ *           every line uses `center`
  *   acc     float64 [nline][height][npts], added to (not overwritten)
  *   work    device scratch of up to atb_vertical_workspace() bytes, or
  *           NULL: with it, the angles are also split over CTAs when the
@@ -342,7 +375,8 @@ int atb_vertical_backproject(const float *proj, int64_t proj_stride,
                              int64_t row_stride, int nproj, int height,
                              int width, const double *trig,
                              const double *points, int64_t line_stride,
-                             int npts, int nline, double center, int edge_pad,
+                             int npts, int nline, double center,
+                             const double *line_centers, int edge_pad,
                              double *acc, int64_t acc_line_stride,
                              int64_t acc_row_stride, void *work,
                              int64_t work_bytes, void *stream);

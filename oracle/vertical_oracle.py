@@ -140,3 +140,93 @@ def vertical_reconstruction(projections, x_mat, y_mat, center, angles=None,
         m[pad_left:pad_left + 2 * rad] = 1.0
         out = out * m
     return out * np.pi / (num_proj - 1)
+
+
+def smooth_projections(projections, sigma):
+    """``gaussian_filter(projections, (0, sigma, sigma))`` of float32
+    projections: the height pass, then the width pass, float32 between them
+    (vertrec.py:1348-1349)."""
+    from .center_oracle import gaussian_filter_rows
+    out = np.empty(projections.shape, np.float32)
+    for n, p in enumerate(np.asarray(projections, np.float32)):
+        tmp = gaussian_filter_rows(np.ascontiguousarray(p.T), sigma).T
+        out[n] = gaussian_filter_rows(np.ascontiguousarray(tmp), sigma)
+    return out
+
+
+def autocorrelation(img):
+    """``mean(max(|ifft(|fft(row)|^2)|, axis=1))`` (vertrec.py:1255-1261),
+    FP64."""
+    f = np.fft.fft(np.asarray(img, np.float32).astype(np.float64))
+    return float(np.mean(np.max(np.abs(np.fft.ifft(np.abs(f) ** 2)),
+                                axis=1)))
+
+
+def find_center_vertical_slice(projections, slice_index, start, stop,
+                               step=1.0, metric="entropy", alpha=0.0,
+                               angles=None, chunk_size=30,
+                               ramp_filter="after", sigma=3, apply_log=True,
+                               masking=True, invert_metric=False,
+                               metric_function=None, **kwargs):
+    """(list_center, list_metric) of ``find_center_vertical_slice``
+    (vertrec.py:1264-1383): smoothing, ``-log`` (values <= 0 set to 1),
+    one FP64 vertical reconstruction per centre (hann window, edge padding
+    of min(0.15 width, 150)), the mask of the smallest centre, and the
+    entropy (normalised by the range of the slice at the mean centre, in
+    float64 after the "after" ramp filter and float32 otherwise),
+    sharpness or autocorrelation metric, or ``metric_function(slice,
+    **kwargs)``."""
+    from . import center_oracle as C
+    if ramp_filter is None:
+        ramp_filter = "after"
+    list_center = np.arange(start, stop + step, step)
+    list_metric = np.zeros_like(list_center)
+    num_proj, height, width = projections.shape
+    if angles is None:
+        angles = np.deg2rad(np.linspace(0.0, 180.0, num_proj))
+    proj = np.asarray(projections, np.float32)
+    if sigma > 0:
+        proj = smooth_projections(proj, sigma)
+    proj = proj.astype(np.float64)
+    if apply_log:
+        proj = -np.log(np.where(proj <= 0.0, 1.0, proj))
+    xs, ys = points_single_line(slice_index, alpha, width)
+    pad = min(int(0.15 * width), 150)
+    out_dt = np.float64 if ramp_filter == "after" else np.float32
+
+    def recon(center):
+        r = vertical_reconstruction(proj, xs[None], ys[None], center,
+                                    angles=angles, ramp_filter=ramp_filter,
+                                    filter_name="hann", pad=pad,
+                                    pad_mode="edge", apply_log=False)[0]
+        return r.astype(out_dt)
+
+    mask = None
+    if masking:
+        rad = int(min(np.min(list_center), width - np.min(list_center)))
+        pad_left = (width - 2 * rad) // 2
+        mask = np.zeros(width, np.float32)
+        mask[pad_left:pad_left + 2 * rad] = 1.0
+    if metric_function is None and metric == "entropy":
+        first = recon(np.mean(list_center))
+        nmin, nmax = first.min(), first.max()
+    for i, center in enumerate(list_center):
+        r = recon(center)
+        if mask is not None:
+            r = r * mask.astype(out_dt)
+        if metric_function is not None:
+            list_metric[i] = metric_function(r, **kwargs)
+        elif metric == "entropy":
+            if out_dt == np.float32:
+                levels = C.normalise_u8(r, nmin, nmax)
+            else:
+                levels = np.uint8(np.clip((r - nmin) / (nmax - nmin), 0, 1)
+                                  * 255)
+            list_metric[i] = C.histogram_entropy(levels)
+        elif metric == "sharpness":
+            list_metric[i] = C.edge_sharpness(r)
+        else:
+            list_metric[i] = autocorrelation(r)
+    if invert_metric:
+        list_metric = np.max(list_metric) - list_metric
+    return list_center, list_metric

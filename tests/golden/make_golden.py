@@ -320,6 +320,97 @@ def make_vertical():
     np.savez_compressed(os.path.join(HERE, "golden_vertical.npz"), **out)
 
 
+def make_vcenter():
+    """Centre search on a vertical slice (find_center_vertical_slice,
+    algotom/rec/vertrec.py:1264-1383), CPU path, and the projection
+    smoothing it starts with."""
+    import scipy.ndimage as ndi
+    import algotom.rec.vertrec as vrec
+    nproj, height, width, cen = 73, 10, 64, 31.7
+    ang = np.deg2rad(np.linspace(0.0, 180.0, nproj))
+    att = np.zeros((nproj, height, width), np.float32)
+    for i in range(height):
+        att[:, i, :] = phantom.ellipse_sinogram(60 + i, nproj, width, cen,
+                                                photons=None, angles=ang)[0]
+    trans = np.exp(-att).astype(np.float32)
+    rng = np.random.default_rng(11)
+    tall = rng.random((3, 70, 40)).astype(np.float32)
+    out = {"trans": trans, "angles": ang, "tall": tall}
+    for sg in (3, 1.5, 0.7):
+        out[_key("smooth", sg)] = ndi.gaussian_filter(trans, (0, sg, sg))
+        out[_key("smooth_tall", sg)] = ndi.gaussian_filter(tall, (0, sg, sg))
+    common = dict(gpu=False, show_progress=False, ncore=1, return_metric=True)
+    cases = {
+        "entropy": dict(),
+        "sharpness": dict(metric="sharpness"),
+        "autocorr": dict(metric="autocorrelation"),
+        "entropy_before": dict(ramp_filter="before", sigma=1.5),
+        "sharp_nomask": dict(metric="sharpness", masking=False, sigma=0,
+                             alpha=30.0, slice_index=20),
+        "entropy_invert": dict(invert_metric=True, chunk_size=16, sigma=0.7),
+        "autocorr_angles": dict(metric="autocorrelation", alpha=60.0,
+                                slice_index=40, angles=ang, chunk_size=None),
+    }
+    for name, kw in cases.items():
+        kw = dict(kw)
+        idx = kw.pop("slice_index", 32)
+        cs, ms = vrec.find_center_vertical_slice(
+            trans.copy(), idx, 28.0, 35.0, step=0.5, **kw, **common)
+        out[_key("vc", name, "centers")] = cs
+        out[_key("vc", name, "metrics")] = ms
+    cs, ms = vrec.find_center_vertical_slice(trans.copy(), 32, 28, 35,
+                                             step=1, metric="sharpness",
+                                             **common)
+    out["vc_int_centers"], out["vc_int_metrics"] = cs, ms
+    out["vc_best"] = vrec.find_center_vertical_slice(
+        trans.copy(), 32, 28.0, 35.0, step=0.5, gpu=False,
+        show_progress=False, ncore=1)
+    bad = trans.copy()
+    bad[5, 3, 7] = 0.0
+    bad[40, 8, 20] = -1.0
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        cs, ms = vrec.find_center_vertical_slice(
+            bad, 32, 29.0, 34.0, step=1.0, sigma=0, metric="sharpness",
+            **common)
+    out["vc_log_metrics"] = ms
+    out["vc_log_warnings"] = np.array([str(w.message) for w in caught
+                                       if "logarithm" in str(w.message)])
+    out["vc_log_mutated"] = bad
+    # the reference's own search test data (tests/test_rec/test_vertrec.py:
+    # 52-81, 498-539): a 3-D phantom of three cut squares, projected by
+    # rotation over 180 degrees; centre 30
+    import algotom.util.utility as util
+    w, h = 61, 40
+    mat = util.make_circle_mask(w, 0.8)
+    for rad, i_s, j_s in ((10, 30, 20), (5, 20, 30), (5, 20, 50)):
+        mat[i_s:i_s + rad, j_s:j_s + rad] = 0
+    mat = ndi.gaussian_filter(mat, 1)
+    vol = np.zeros((h, w, w), dtype=np.float32)
+    vol[1:] = mat
+    ang360 = np.linspace(0.0, 360.0, 91, dtype=np.float32)
+    projs = np.zeros((91, h, w), dtype=np.float32)
+    for i, a in enumerate(ang360):
+        projs[i] = np.sum(ndi.rotate(vol, -a, axes=(1, 2), order=1,
+                                     reshape=False), axis=1)
+    projs = projs[:46] + 1
+    out["cube_projs"] = projs
+    for metric in ("autocorrelation", "entropy", "sharpness"):
+        cs, ms = vrec.find_center_vertical_slice(
+            projs.copy(), w // 2, 25, 39, step=1.0, metric=metric,
+            invert_metric=True, masking=False, **common)
+        out[_key("cube", metric, "centers")] = cs
+        out[_key("cube", metric, "metrics")] = ms
+
+    def get_negative(mat, n=2):
+        return np.abs(np.mean(mat[mat < 0.0])) ** n
+    cs, ms = vrec.find_center_vertical_slice(
+        projs.copy(), w // 2, 25, 39, step=1.0, invert_metric=True,
+        metric_function=get_negative, n=2, **common)
+    out["cube__custom__centers"], out["cube__custom__metrics"] = cs, ms
+    np.savez_compressed(os.path.join(HERE, "golden_vcenter.npz"), **out)
+
+
 def make_conversion():
     """360-degree conversions (algotom/prep/conversion.py:43-454) and the
     scipy sub-pixel shift they call."""
@@ -407,6 +498,7 @@ def make_dfi():
 GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
               "recon": make_recon, "unittest": make_reference_test_fixture,
               "center": make_center, "vertical": make_vertical,
+              "vcenter": make_vcenter,
               "conversion": make_conversion, "dfi": make_dfi}
 
 if __name__ == "__main__":

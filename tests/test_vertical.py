@@ -122,17 +122,17 @@ def test_abi_argument_errors():
     lib = nat.load()
     one = 1
     assert lib.atb_vertical_backproject(None, 8, 8, 2, 2, 8, one, one, 8, 8,
-                                        1, 3.0, 0, one, 8, 8, None, 0,
+                                        1, 3.0, None, 0, one, 8, 8, None, 0,
                                         None) == -1
     assert lib.atb_vertical_backproject(one, 8, 8, 0, 2, 8, one, one, 8, 8,
-                                        1, 3.0, 0, one, 8, 8, None, 0,
+                                        1, 3.0, None, 0, one, 8, 8, None, 0,
                                         None) == -1
     assert lib.atb_vertical_backproject(one, 8, 8, 2, 2, 8, one, one, 8, 8,
-                                        1, float("nan"), 0, one, 8, 8, None,
-                                        0, None) == -1
+                                        1, float("nan"), None, 0, one, 8, 8,
+                                        None, 0, None) == -1
     assert lib.atb_vertical_backproject(one, 1 << 31, 1 << 30, 2, 4, 8, one,
-                                        one, 8, 8, 1, 3.0, 0, one, 8, 8,
-                                        None, 0, None) == -3
+                                        one, 8, 8, 1, 3.0, None, 0, one, 8,
+                                        8, None, 0, None) == -3
     # a small output asks for scratch to split the angles, a large one not
     assert lib.atb_vertical_workspace(1801, 64, 2560, 1) > 0
     assert lib.atb_vertical_workspace(1801, 2048, 2560, 64) == 0
