@@ -38,52 +38,58 @@ constexpr int kColTile = 32;         // columns per CTA (Gaussian, columns)
 constexpr int kColRows = 64;         // output rows per CTA (Gaussian, columns)
 constexpr int kColThreads = 256;
 constexpr int kMaxColRadius = 700;   // strip + halo: <= 190 KB of shared memory
+constexpr int kColRadius64 = 300;    // FP64 strip + halo: <= 172 KB
 constexpr int kMaxGaussRadius = 8192;
 constexpr int kMetricThreads = 256;
 constexpr int kMetricBlocks = 256;   // partial sums per image (sharpness)
 static_assert(kMetricThreads == 256, "one thread per histogram bin");
 
 __device__ __forceinline__ int reflect_index(long long i, int n) {
+  if (i >= 0 && i < n) return (int)i;  // inside: no 64-bit remainder
   const long long period = 2LL * n;
   long long r = i % period;
   if (r < 0) r += period;
   return (int)(r >= n ? period - 1 - r : r);
 }
 
+// Row pass: CTA (row, tile) filters 256 samples of one row.  The strip and
+// its halo are staged once as FP64 (the conversion is exact), so the taps
+// read doubles from shared memory.
 __global__ void __launch_bounds__(kRowTile) gaussian_rows_kernel(const float *__restrict__ src, long long srs,
                                                                  int ncol, const double *__restrict__ w, int radius,
                                                                  float *__restrict__ dst, long long drs) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double *ws = reinterpret_cast<double *>(smem);            // [radius + 1]
-  float *xs = reinterpret_cast<float *>(ws + radius + 1);   // [kRowTile + 2 radius]
+  double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
+  double *xs = ws + radius + 1;                   // [kRowTile + 2 radius]
   const long long row = blockIdx.x;
   const int c0 = blockIdx.y * kRowTile;
-  const float *x = src + (long long)row * srs;
+  const float *x = src + row * srs;
   for (int j = threadIdx.x; j <= radius; j += kRowTile) ws[j] = w[j];
   const int span = kRowTile + 2 * radius;
   for (int j = threadIdx.x; j < span; j += kRowTile)
-    xs[j] = x[reflect_index((long long)c0 - radius + j, ncol)];
+    xs[j] = (double)x[reflect_index((long long)c0 - radius + j, ncol)];
   __syncthreads();
   const int c = c0 + threadIdx.x;
   if (c >= ncol) return;
-  const float *xc = xs + radius + threadIdx.x;
-  double acc = __dmul_rn((double)xc[0], ws[0]);
-  for (int j = 1; j <= radius; ++j)
-    acc = __dadd_rn(acc, __dmul_rn(__dadd_rn((double)xc[j], (double)xc[-j]), ws[j]));
+  const double *xc = xs + radius + threadIdx.x;
+  double acc = __dmul_rn(xc[0], ws[0]);
+  for (int j = 1; j <= radius; ++j) acc = __dadd_rn(acc, __dmul_rn(__dadd_rn(xc[j], xc[-j]), ws[j]));
   dst[row * drs + c] = __double2float_rn(acc);
 }
 
 // Column pass: CTA (x, y, z) filters columns [32 x, 32 x + 32) of rows
 // [64 y, 64 y + 64) of image z; threads (lane = column, warp = row phase)
-// read the strip with its halo row by row (coalesced), then each output
-// takes the symmetric sum down its column in shared memory.
+// read the strip with its halo row by row (coalesced) into shared memory
+// as S (FP64 for radii up to kColRadius64: converted once, not per tap),
+// then each output takes the symmetric sum down its column.
+template <typename S>
 __global__ void __launch_bounds__(kColThreads)
     gaussian_cols_kernel(const float *__restrict__ src, long long sis, long long srs, int nrow, int ncol,
                          const double *__restrict__ w, int radius, float *__restrict__ dst, long long dis,
                          long long drs) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double *ws = reinterpret_cast<double *>(smem);           // [radius + 1]
-  float *xs = reinterpret_cast<float *>(ws + radius + 1);  // [kColRows + 2 radius][kColTile]
+  double *ws = reinterpret_cast<double *>(smem);   // [radius + 1]
+  S *xs = reinterpret_cast<S *>(ws + radius + 1);  // [kColRows + 2 radius][kColTile]
   const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
   const int c = blockIdx.x * kColTile + lane;
   const int r0 = blockIdx.y * kColRows;
@@ -91,14 +97,14 @@ __global__ void __launch_bounds__(kColThreads)
   for (int j = threadIdx.x; j <= radius; j += kColThreads) ws[j] = w[j];
   const int span = kColRows + 2 * radius;
   for (int j = wy; j < span; j += kColThreads / 32)
-    xs[j * kColTile + lane] = c < ncol ? img[reflect_index((long long)r0 - radius + j, nrow) * srs + c] : 0.0f;
+    xs[j * kColTile + lane] = c < ncol ? (S)img[reflect_index((long long)r0 - radius + j, nrow) * srs + c] : (S)0;
   __syncthreads();
   if (c >= ncol) return;
   float *out = dst + blockIdx.z * dis;
   for (int k = wy; k < kColRows; k += kColThreads / 32) {
     const int r = r0 + k;
     if (r >= nrow) break;
-    const float *xc = xs + (radius + k) * kColTile + lane;
+    const S *xc = xs + (radius + k) * kColTile + lane;
     double acc = __dmul_rn((double)xc[0], ws[0]);
     for (int j = 1; j <= radius; ++j)
       acc = __dadd_rn(acc, __dmul_rn(__dadd_rn((double)xc[j * kColTile], (double)xc[-j * kColTile]), ws[j]));
@@ -307,7 +313,7 @@ extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int n
   if (ncol > 65535 * kRowTile || radius > kMaxGaussRadius)
     return atb::fail(ATB_ERANGE, "atb_gaussian_rows: ncol=%d or radius=%d too large", ncol, radius);
   if (src == dst) return atb::fail(ATB_EINVAL, "atb_gaussian_rows: in-place filtering is not supported");
-  const size_t smem = sizeof(double) * (radius + 1) + sizeof(float) * (kRowTile + 2 * (size_t)radius);
+  const size_t smem = sizeof(double) * (radius + 1) + sizeof(double) * (kRowTile + 2 * (size_t)radius);
   int rc = atb::ensure_smem(gaussian_rows_kernel, smem, "atb_gaussian_rows");
   if (rc != ATB_OK) return rc;
   dim3 grid(nrow, (ncol + kRowTile - 1) / kRowTile);
@@ -327,17 +333,28 @@ extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64
   if ((int64_t)nrow * src_row_stride > 2147483647LL || (int64_t)nrow * dst_row_stride > 2147483647LL)
     return atb::fail(ATB_ERANGE, "atb_gaussian_cols: image of %d rows too large", nrow);
   if (radius > kMaxColRadius) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: radius=%d too large", radius);
-  const size_t smem = sizeof(double) * (radius + 1) + sizeof(float) * kColTile * (kColRows + 2 * (size_t)radius);
-  int rc = atb::ensure_smem(gaussian_cols_kernel, smem, "atb_gaussian_cols");
+  const bool s64 = radius <= kColRadius64;
+  const size_t smem = sizeof(double) * (radius + 1) +
+                      (s64 ? sizeof(double) : sizeof(float)) * kColTile * (kColRows + 2 * (size_t)radius);
+  int rc = s64 ? atb::ensure_smem(gaussian_cols_kernel<double>, smem, "atb_gaussian_cols")
+               : atb::ensure_smem(gaussian_cols_kernel<float>, smem, "atb_gaussian_cols");
   if (rc != ATB_OK) return rc;
   const int gx = (ncol + kColTile - 1) / kColTile, gy = (nrow + kColRows - 1) / kColRows;
   if (gy > 65535) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: nrow=%d too large", nrow);
   cudaStream_t st = atb::as_stream(stream);
   for (int z0 = 0; z0 < nimg; z0 += 65535) {
     const int nz = nimg - z0 < 65535 ? nimg - z0 : 65535;
-    gaussian_cols_kernel<<<dim3(gx, gy, nz), kColThreads, smem, st>>>(
-        src + z0 * src_img_stride, src_img_stride, src_row_stride, nrow, ncol, weights, radius,
-        dst + z0 * dst_img_stride, dst_img_stride, dst_row_stride);
+    const dim3 grid(gx, gy, nz);
+    const float *s0 = src + z0 * src_img_stride;
+    float *d0 = dst + z0 * dst_img_stride;
+    if (s64)
+      gaussian_cols_kernel<double><<<grid, kColThreads, smem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol,
+                                                                    weights, radius, d0, dst_img_stride,
+                                                                    dst_row_stride);
+    else
+      gaussian_cols_kernel<float><<<grid, kColThreads, smem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol,
+                                                                   weights, radius, d0, dst_img_stride,
+                                                                   dst_row_stride);
     rc = atb::check_launch("atb_gaussian_cols");
     if (rc != ATB_OK) return rc;
   }

@@ -76,6 +76,7 @@ Taps make_taps(int order) {
 // index of sample i of a line of n under the symmetric extension
 // (boundary 0: half-sample "reflect", 1: whole-sample "mirror")
 __device__ __forceinline__ int sym_index(int i, int n, int boundary) {
+  if (i >= 0 && i < n) return i;  // inside: no remainder
   if (boundary == 0) {
     const int p = 2 * n;
     int r = i % p;
@@ -139,6 +140,7 @@ __device__ __forceinline__ double bspline5(double u) {
 
 // half-sample symmetric index
 __device__ __forceinline__ int reflect_index(int i, int n) {
+  if (i >= 0 && i < n) return i;
   const int p = 2 * n;
   int r = i % p;
   if (r < 0) r += p;
