@@ -175,7 +175,7 @@ def test_recon_2d_vs_reference(cuda, golden, name):
     fn = R.fbp_reconstruction if name == "fbp" else R.bpf_reconstruction
     dtypes = eval(str(g["dtypes"]))
     sino, ang = g["sino"], g["angles"]
-    tol = TOL if name == "fbp" else 2e-5
+    tol = TOL
     for ratio in (1.0, 0.0, None):
         key = "%s__2d__%s" % (name, ratio)
         got = fn(sino.copy(), 47.5, angles=ang, ratio=ratio, apply_log=False)
@@ -200,7 +200,7 @@ def test_recon_2d_vs_reference(cuda, golden, name):
 def test_recon_3d_vs_reference(cuda, golden, name):
     g = golden("recon")
     fn = R.fbp_reconstruction if name == "fbp" else R.bpf_reconstruction
-    tol = TOL if name == "fbp" else 2e-5
+    tol = TOL
     got = fn(g["s3"].copy(), 47.5, angles=g["angles"], ratio=0.0,
              apply_log=False, ncore=1)
     assert got.shape == (96, 3, 96) and got.dtype == np.float32
@@ -220,7 +220,7 @@ def test_reference_unittests_ported(cuda, golden):
                     (R.bpf_reconstruction, "bpf_180")):
         rec1 = fn(s180.copy(), 32, apply_log=False, gpu=True)
         assert np.max(np.abs(mat - rec1)) <= 0.1
-        assert O.rel_l2(rec1, g[key]) < 2e-5
+        assert O.rel_l2(rec1, g[key]) < TOL
         rec2 = fn(s360.copy(), 32, angles=np.deg2rad(ang_deg),
                   apply_log=False, gpu=True)
         assert np.max(np.abs(mat - rec2)) <= 0.1
