@@ -112,6 +112,123 @@ __global__ void __launch_bounds__(kColThreads)
   }
 }
 
+// Register-window forms for radii up to KR (4, 8, 12 or 16; sigma <= 3.9):
+// the strip is staged as float32 by asynchronous copies (all in flight at
+// once), and each thread computes kWinOut consecutive outputs of one line
+// from a window of kWinOut + 2 radius samples widened to FP64 in registers,
+// so a sample is read from shared memory once per thread instead of once
+// per tap (the forms above read 2 radius + 1 samples per output and are
+// bound by shared memory).  Same operations in the same order as above:
+// bit-identical.
+constexpr int kWinOut = 8;     // outputs per thread
+constexpr int kLineTile = 32;  // lines per CTA (one per lane)
+constexpr int kSegs = 8;       // warps per CTA, each kWinOut outputs per line
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+}
+
+template <int KR>
+__device__ __forceinline__ void window_filter(const float *xs, int stride, const double *ws, int radius,
+                                              double (&acc)[kWinOut]) {
+  // xs points at the staged sample of this thread's first output minus
+  // `radius` (window element m sits at xs[(m - KR + radius) * stride]);
+  // each sample is widened to FP64 once (exact)
+  double win[kWinOut + 2 * KR];
+#pragma unroll
+  for (int m = 0; m < kWinOut + 2 * KR; ++m)
+    win[m] = (m >= KR - radius && m < kWinOut + KR + radius) ? (double)xs[(m - KR + radius) * stride] : 0.0;
+#pragma unroll
+  for (int i = 0; i < kWinOut; ++i) acc[i] = __dmul_rn(win[KR + i], ws[0]);
+#pragma unroll
+  for (int j = 1; j <= KR; ++j) {
+    if (j <= radius) {
+      const double wj = ws[j];
+#pragma unroll
+      for (int i = 0; i < kWinOut; ++i)
+        acc[i] = __dadd_rn(acc[i], __dmul_rn(__dadd_rn(win[KR + i + j], win[KR + i - j]), wj));
+    }
+  }
+}
+
+// rows: CTA = 32 rows (lane) x 64 columns (8 warps x 8); the tile plus halo
+// is staged row-major with an odd pitch (conflict-free per-lane rows), the
+// results go through shared memory for coalesced stores
+template <int KR>
+__global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3 : 2)) gaussian_rows_win_kernel(
+    const float *__restrict__ src, long long srs, long long nrow, int ncol, const double *__restrict__ w,
+    int radius, float *__restrict__ dst, long long drs) {
+  constexpr int kCols = kSegs * kWinOut;  // 64
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
+  const int span = kCols + 2 * radius, pitch = span | 1;
+  float *xs = reinterpret_cast<float *>(ws + radius + 1);  // [32][pitch]
+  float *ot = xs + kLineTile * pitch;                       // [32][kCols + 1]
+  const int tid = threadIdx.x, lane = tid & 31, seg = tid >> 5;
+  const long long row0 = (long long)blockIdx.x * kLineTile;
+  const int c0 = blockIdx.y * kCols;
+  for (int j = tid; j <= radius; j += kLineTile * kSegs) ws[j] = w[j];
+  // the whole strip in flight at once: one asynchronous copy per sample
+  for (int e = tid; e < kLineTile * span; e += kLineTile * kSegs) {
+    const int rr = e / span, cc = e - rr * span;
+    const long long row = row0 + rr;
+    if (row < nrow)
+      cp_async4(xs + rr * pitch + cc, src + row * srs + reflect_index((long long)c0 - radius + cc, ncol));
+    else
+      xs[rr * pitch + cc] = 0.0f;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  double acc[kWinOut];
+  window_filter<KR>(xs + lane * pitch + seg * kWinOut, 1, ws, radius, acc);
+#pragma unroll
+  for (int i = 0; i < kWinOut; ++i) ot[lane * (kCols + 1) + seg * kWinOut + i] = __double2float_rn(acc[i]);
+  __syncthreads();
+  for (int e = tid; e < kLineTile * kCols; e += kLineTile * kSegs) {
+    const int rr = e / kCols, cc = e - rr * kCols;
+    const long long row = row0 + rr;
+    if (row < nrow && c0 + cc < ncol) dst[row * drs + c0 + cc] = ot[rr * (kCols + 1) + cc];
+  }
+}
+
+// columns: CTA = 32 columns (lane) x 64 rows (8 warps x 8) of one image;
+// the strip plus halo is staged as in gaussian_cols_kernel
+template <int KR>
+__global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3 : 2)) gaussian_cols_win_kernel(
+    const float *__restrict__ src, long long sis, long long srs, int nrow, int ncol, const double *__restrict__ w,
+    int radius, float *__restrict__ dst, long long dis, long long drs) {
+  constexpr int kRowsT = kSegs * kWinOut;  // 64
+  extern __shared__ __align__(16) unsigned char smem[];
+  double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
+  float *xs = reinterpret_cast<float *>(ws + radius + 1);  // [kRowsT + 2 radius][32]
+  const int tid = threadIdx.x, lane = tid & 31, seg = tid >> 5;
+  const int c = blockIdx.x * kLineTile + lane;
+  const int r0 = blockIdx.y * kRowsT;
+  const float *img = src + blockIdx.z * sis;
+  for (int j = tid; j <= radius; j += kLineTile * kSegs) ws[j] = w[j];
+  const int span = kRowsT + 2 * radius;
+  for (int j = seg; j < span; j += kSegs) {
+    if (c < ncol)
+      cp_async4(xs + j * kLineTile + lane, img + reflect_index((long long)r0 - radius + j, nrow) * srs + c);
+    else
+      xs[j * kLineTile + lane] = 0.0f;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int k0 = seg * kWinOut;
+  if (c >= ncol || r0 + k0 >= nrow) return;
+  double acc[kWinOut];
+  window_filter<KR>(xs + k0 * kLineTile + lane, kLineTile, ws, radius, acc);
+  float *out = dst + blockIdx.z * dis;
+#pragma unroll
+  for (int i = 0; i < kWinOut; ++i)
+    if (r0 + k0 + i < nrow) out[(long long)(r0 + k0 + i) * drs + c] = __double2float_rn(acc[i]);
+}
+
 struct ZoomAxis {
   int i0, i1;
   double w0, w1;
@@ -313,12 +430,31 @@ extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int n
   if (ncol > 65535 * kRowTile || radius > kMaxGaussRadius)
     return atb::fail(ATB_ERANGE, "atb_gaussian_rows: ncol=%d or radius=%d too large", ncol, radius);
   if (src == dst) return atb::fail(ATB_EINVAL, "atb_gaussian_rows: in-place filtering is not supported");
+  cudaStream_t st = atb::as_stream(stream);
+  if (radius <= 16) {
+    const int span = kSegs * kWinOut + 2 * radius;
+    const size_t wsmem = sizeof(double) * (radius + 1) + sizeof(float) * kLineTile * (span | 1) +
+                         sizeof(float) * kLineTile * (kSegs * kWinOut + 1);
+    const dim3 wgrid((nrow + kLineTile - 1) / kLineTile, (ncol + kSegs * kWinOut - 1) / (kSegs * kWinOut));
+    if (wgrid.y > 65535) return atb::fail(ATB_ERANGE, "atb_gaussian_rows: ncol=%d too large", ncol);
+    auto launch = [&](auto kern) {
+      int rc = atb::ensure_smem(kern, wsmem, "atb_gaussian_rows");
+      if (rc != ATB_OK) return rc;
+      kern<<<wgrid, kLineTile * kSegs, wsmem, st>>>(src, src_row_stride, nrow, ncol, weights, radius, dst,
+                                                    dst_row_stride);
+      return atb::check_launch("atb_gaussian_rows");
+    };
+    if (radius <= 4) return launch(gaussian_rows_win_kernel<4>);
+    if (radius <= 8) return launch(gaussian_rows_win_kernel<8>);
+    if (radius <= 12) return launch(gaussian_rows_win_kernel<12>);
+    return launch(gaussian_rows_win_kernel<16>);
+  }
   const size_t smem = sizeof(double) * (radius + 1) + sizeof(double) * (kRowTile + 2 * (size_t)radius);
   int rc = atb::ensure_smem(gaussian_rows_kernel, smem, "atb_gaussian_rows");
   if (rc != ATB_OK) return rc;
   dim3 grid(nrow, (ncol + kRowTile - 1) / kRowTile);
-  gaussian_rows_kernel<<<grid, kRowTile, smem, atb::as_stream(stream)>>>(src, src_row_stride, ncol, weights, radius,
-                                                                           dst, dst_row_stride);
+  gaussian_rows_kernel<<<grid, kRowTile, smem, st>>>(src, src_row_stride, ncol, weights, radius, dst,
+                                                      dst_row_stride);
   return atb::check_launch("atb_gaussian_rows");
 }
 
@@ -333,6 +469,28 @@ extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64
   if ((int64_t)nrow * src_row_stride > 2147483647LL || (int64_t)nrow * dst_row_stride > 2147483647LL)
     return atb::fail(ATB_ERANGE, "atb_gaussian_cols: image of %d rows too large", nrow);
   if (radius > kMaxColRadius) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: radius=%d too large", radius);
+  if (radius <= 16) {
+    const size_t wsmem = sizeof(double) * (radius + 1) + sizeof(float) * kLineTile * (kSegs * kWinOut + 2 * radius);
+    auto kern = radius <= 4 ? gaussian_cols_win_kernel<4>
+                : radius <= 8 ? gaussian_cols_win_kernel<8>
+                : radius <= 12 ? gaussian_cols_win_kernel<12> : gaussian_cols_win_kernel<16>;
+    int rc = atb::ensure_smem(kern, wsmem, "atb_gaussian_cols");
+    if (rc != ATB_OK) return rc;
+    const int gx = (ncol + kLineTile - 1) / kLineTile, gy = (nrow + kSegs * kWinOut - 1) / (kSegs * kWinOut);
+    if (gy > 65535) return atb::fail(ATB_ERANGE, "atb_gaussian_cols: nrow=%d too large", nrow);
+    cudaStream_t st = atb::as_stream(stream);
+    for (int z0 = 0; z0 < nimg; z0 += 65535) {
+      const int nz = nimg - z0 < 65535 ? nimg - z0 : 65535;
+      const dim3 grid(gx, gy, nz);
+      const float *s0 = src + z0 * src_img_stride;
+      float *d0 = dst + z0 * dst_img_stride;
+      kern<<<grid, kLineTile * kSegs, wsmem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol, weights, radius,
+                                                   d0, dst_img_stride, dst_row_stride);
+      rc = atb::check_launch("atb_gaussian_cols");
+      if (rc != ATB_OK) return rc;
+    }
+    return ATB_OK;
+  }
   const bool s64 = radius <= kColRadius64;
   const size_t smem = sizeof(double) * (radius + 1) +
                       (s64 ? sizeof(double) : sizeof(float)) * kColTile * (kColRows + 2 * (size_t)radius);

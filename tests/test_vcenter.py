@@ -145,6 +145,22 @@ def test_device_smoothing_bit_exact(cuda, golden, sigma):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("sigma", (0.7, 2, 3, 4, 5))
+def test_device_smoothing_tiles_and_radii(cuda, sigma):
+    """Both forms of each Gaussian pass (register windows up to radius 16,
+    shared-memory taps beyond) over several tiles, against the oracle,
+    which is bit-exact with scipy."""
+    import torch
+    from algotom_b200.rec import vertrec as VR
+    x = np.random.default_rng(5).random((3, 150, 203)).astype(np.float32)
+    t = torch.as_tensor(x, device=cuda)
+    w = torch.from_numpy(VR._gaussian_weights(sigma)).to(cuda)
+    tmp, out = torch.empty_like(t), torch.empty_like(t)
+    VR._gaussian_slab(t, w, tmp, out)
+    assert np.array_equal(out.cpu().numpy(), V.smooth_projections(x, sigma))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_search_matches_reference(cuda, golden, name):
     from algotom_b200.rec import vertrec as VR
