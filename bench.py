@@ -434,6 +434,24 @@ def run_batch(args):
     e1.record()
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / args.steps
+    # the persistent back-projection alone, on the stream it launches on
+    from algotom_b200 import _native as nat
+    from algotom_b200.rec import reconstruction as R
+    st = torch.cuda.current_stream(dev)
+    b0, b1 = torch.cuda.Event(enable_timing=True), \
+        torch.cuda.Event(enable_timing=True)
+    b0.record(st)
+    for _ in range(args.steps):
+        nat.call("atb_backproject_batch", bf.items_dev.data_ptr(), bf.n,
+                 bf.units_dev.data_ptr(), bf.nunits, bf.counter.data_ptr(), 0,
+                 bf.variant, R._stream_ptr(dev))
+    b1.record(st)
+    torch.cuda.synchronize()
+    t_bp = b0.elapsed_time(b1) / 1e3 / args.steps
+    peaks, src = _peaks()
+    f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    smem_peak = SMEM_BYTES_PER_CLK_PER_SM * N_SM * f_clk / 1e9
+    smem_achieved = SMEM_BYTES_PER_UPDATE * bf.updates / t_bp / 1e9
     err = None
     if not args.no_oracle:
         from oracle import fbp_oracle as O
@@ -451,6 +469,15 @@ def run_batch(args):
                                "under a CUDA graph", "items": len(geo),
                    "tile_variant": bf.variant, "units": bf.nunits,
                    "updates": bf.updates},
+        "roofline": {"bound": "smem", "kernel": "bp_batch_kernel",
+                     "achieved": smem_achieved, "peak": smem_peak,
+                     "unit": "GB/s", "frac": smem_achieved / smem_peak,
+                     "bytes_per_update": SMEM_BYTES_PER_UPDATE,
+                     "updates_per_s": bf.updates / t_bp,
+                     "ms_per_launch": t_bp * 1e3,
+                     "peak_source": "shared-memory delivery, 128 B/clk x 148 "
+                                    "SM x sm_max_mhz (%s)" % src},
+        "gpu_launches": (bf.n + 1) * args.steps + args.steps,
         "accuracy": err}), flush=True)
 
 
