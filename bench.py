@@ -747,6 +747,42 @@ def run_center(args):
         "gpu_launches": 8 * args.steps}), flush=True)
 
 
+def _profile_figure(prefix, key):
+    """A figure `key: value` from a committed ncu summary profiles/<prefix>*.md."""
+    d = os.path.join(ROOT, "profiles")
+    try:
+        names = sorted(os.listdir(d))
+    except OSError:
+        return None
+    for n in names:
+        if n.startswith(prefix) and n.endswith(".md"):
+            m = re.search(key + r":\s*([0-9.eE+-]+)",
+                          open(os.path.join(d, n)).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+def _vertical_bytes(xs, ys, ang, center, width, height):
+    """Algorithmic DRAM bytes of one vertical back-projection launch: per
+    angle the detector bins the slice's points touch (a contiguous run, for
+    unit-spaced points, plus an edge bin where points are clamped), read
+    once for every detector row, and the FP64 accumulator read and written
+    (float32-rounded geometry, as the default gpu=True path)."""
+    r32 = lambda v: np.float32(v).astype(np.float64)  # noqa: E731
+    a = r32(ang)
+    p = (r32(xs)[None, :] * np.cos(a)[:, None] +
+         r32(ys)[None, :] * np.sin(a)[:, None] + float(np.float32(center)))
+    w1 = width - 1
+    inr = (p >= 0) & (p <= w1)
+    d0 = np.where(inr, np.floor(p), np.inf).min(axis=1)
+    d1 = np.where(inr, np.ceil(p), -np.inf).max(axis=1)
+    bins = np.where(np.isfinite(d0), d1 - d0 + 1, 0)
+    bins = bins + ((p < 0).any(axis=1) & (d0 > 0)) + \
+        ((p > w1).any(axis=1) & (d1 < w1))
+    return float(bins.sum()) * height * 4 + height * len(xs) * 16.0
+
+
 def run_vertical(args):
     """Vertical slices from a projection stack of 1801 x 512 x 2560 float32
     (the benchmark's 512 slices read as projections, 9.4 GB, device-
@@ -787,14 +823,32 @@ def run_vertical(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / n
 
+    # the back-projection launch alone (atb_vertical_backproject and its
+    # angle-group reduction) for the slice of `single`
+    xs1, ys1 = VR._get_points_single_line(NCOL // 2, 30.0, NCOL)
+    trig1 = VR._trig_plus(ang, dev, True)
+    pts1 = VR._points(xs1, ys1, NCOL, dev, True)
+    acc1 = torch.zeros((1, height, NCOL), dtype=torch.float64, device=dev)
+
+    def kernel_only(src):
+        VR._backproject(src, trig1, pts1, float(np.float32(CENTER)), True,
+                        acc1)
+        return None
+
     for _ in range(args.warmup):
         single(proj)
         multi(proj)
+        kernel_only(proj)
     sampler = ClockSampler(0)
     sampler.start()
     t1 = timed(single, proj, args.steps)
     t64 = timed(multi, proj, args.steps)
+    t_bp = timed(kernel_only, proj, args.steps)
     clocks = sampler.stop()
+    alg_bytes = _vertical_bytes(np.asarray(xs1, np.float64),
+                                np.asarray(ys1, np.float64), ang, CENTER,
+                                NCOL, height)
+    per_row = _profile_figure("vertical_slice", "dram_bytes_per_row_single")
     t_e2e = None
     nbytes = proj.numel() * 4
     if not args.no_e2e:
@@ -838,10 +892,16 @@ def run_vertical(args):
                                "projections of %d x 2560 (device-resident)"
                                % height,
                    "l2": "inputs larger than L2 (9.4 GB)"},
-        "roofline": {"bound": "hbm", "achieved": nbytes / t1 / 1e9,
+        "roofline": {"bound": "hbm", "kernel": "vbp_kernel",
+                     "achieved": alg_bytes / t_bp / 1e9,
                      "peak": hbm, "unit": "GB/s",
-                     "frac": nbytes / t1 / 1e9 / hbm, "traffic": None,
-                     "bytes": "projections read once per step",
+                     "frac": alg_bytes / t_bp / 1e9 / hbm,
+                     "traffic": None if per_row is None else per_row * height,
+                     "algorithmic_bytes": alg_bytes,
+                     "bytes": "detector bins the slice touches (%.2f of the "
+                              "projections), read once per row, + the FP64 "
+                              "accumulator" % (alg_bytes / nbytes),
+                     "ms_per_launch": t_bp * 1e3,
                      "peak_source": src},
         "multiple_64": {"value": 64 * upd1 / t64, "unit": "updates/s",
                         "ms_per_step": t64 * 1e3},
@@ -851,9 +911,10 @@ def run_vertical(args):
             "d2h_bytes_per_step": height * NCOL * 8,
             "ms_per_step": t_e2e * 1e3},
         "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
-        # one vertical back-projection launch per step (the FP64 filter
-        # after it is library FFT work)
-        "gpu_launches": args.steps}), flush=True)
+        # per step: the single slice (back-projection + angle-group
+        # reduction; the FP64 filter after it is library FFT work), the 64
+        # slices (one back-projection) and the kernel-only launch pair
+        "gpu_launches": 5 * args.steps}), flush=True)
 
 
 def run_vcenter(args):
