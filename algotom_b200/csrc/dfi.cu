@@ -119,6 +119,64 @@ __global__ void __launch_bounds__(kFirThreads)
   dst[outer * line_stride + comp + (long long)i * es] = acc;
 }
 
+// Tiled forms: the strip a CTA filters, plus its 2 x ntaps halo (symmetric
+// extension resolved while staging), is staged in shared memory once, so
+// each output's 2 ntaps + 1 reads hit shared memory instead of L2 (the
+// untiled kernel above reads every tap through the cache hierarchy).  Same
+// taps and summation order: the same results bit for bit.
+constexpr int kFirLines = 32;   // lines per CTA (filter axis strided)
+constexpr int kFirRows = 64;    // outputs per line per CTA (filter axis strided)
+constexpr int kFirSeg = 128;    // positions per CTA (filter axis contiguous)
+
+// filter axis strided, lines contiguous: element (i, l) at src[i * es + l],
+// l < nl; CTA = 32 consecutive l x 64 consecutive i
+__global__ void __launch_bounds__(kFirThreads)
+    prefilter_cols_kernel(const double *__restrict__ src, double *__restrict__ dst, long long es, int nl, int n,
+                          int boundary, Taps taps) {
+  extern __shared__ double xs[];  // [kFirRows + 2 ntaps][kFirLines]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = blockIdx.x * kFirLines + lane;
+  const int i0 = blockIdx.y * kFirRows;
+  const int nt = taps.ntaps, span = kFirRows + 2 * nt;
+  for (int q = warp; q < span; q += kFirThreads / 32)
+    xs[q * kFirLines + lane] = l < nl ? src[(long long)sym_index(i0 - nt + q, n, boundary) * es + l] : 0.0;
+  __syncthreads();
+  if (l >= nl) return;
+  for (int k0 = warp; k0 < kFirRows; k0 += kFirThreads / 32) {
+    const int i = i0 + k0;
+    if (i >= n) break;
+    const double *c = xs + (nt + k0) * kFirLines + lane;
+    double acc = taps.h[0] * c[0];
+    for (int k = 1; k <= nt; ++k) acc += taps.h[k] * (c[-k * kFirLines] + c[k * kFirLines]);
+    dst[(long long)i * es + l] = acc;
+  }
+}
+
+// filter axis contiguous: element (line, i, comp) at
+// src[line * ls + i * ncomp + comp]; CTA = one line x 128 positions
+__global__ void __launch_bounds__(kFirThreads)
+    prefilter_rows_kernel(const double *__restrict__ src, double *__restrict__ dst, long long ls, int ncomp, int n,
+                          int boundary, Taps taps) {
+  extern __shared__ double xs[];  // [(kFirSeg + 2 ntaps) * ncomp]
+  const long long line = blockIdx.y;
+  const int i0 = blockIdx.x * kFirSeg;
+  const int nt = taps.ntaps, span = (kFirSeg + 2 * nt) * ncomp;
+  const double *in = src + line * ls;
+  for (int e = threadIdx.x; e < span; e += kFirThreads) {
+    const int q = e / ncomp, comp = e - q * ncomp;
+    xs[e] = in[(long long)sym_index(i0 - nt + q, n, boundary) * ncomp + comp];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kFirSeg * ncomp; e += kFirThreads) {
+    const int q = e / ncomp, comp = e - q * ncomp, i = i0 + q;
+    if (i >= n) break;
+    const double *c = xs + (nt + q) * ncomp + comp;
+    double acc = taps.h[0] * c[0];
+    for (int k = 1; k <= nt; ++k) acc += taps.h[k] * (c[-k * ncomp] + c[k * ncomp]);
+    dst[line * ls + (long long)i * ncomp + comp] = acc;
+  }
+}
+
 // centred quintic B-spline
 __device__ __forceinline__ double bspline5(double u) {
   const double a = fabs(u);
@@ -210,11 +268,32 @@ extern "C" int atb_spline_prefilter(const double *src, double *dst, int64_t line
   if (elem_stride != ncomp && line_stride != ncomp)
     return atb::fail(ATB_EINVAL, "atb_spline_prefilter: lines or elements must be contiguous");
   static const Taps taps3 = make_taps(3), taps5 = make_taps(5);
+  const Taps &taps = order == 5 ? taps5 : taps3;
+  cudaStream_t st = atb::as_stream(stream);
+  if (line_stride == ncomp && (long long)nlines * ncomp <= 2147483647LL && (n + kFirRows - 1) / kFirRows <= 65535) {
+    // lines contiguous: tiles of 32 lines x 64 positions
+    const int nl = nlines * ncomp;
+    const size_t smem = sizeof(double) * kFirLines * (kFirRows + 2 * taps.ntaps);
+    int rc = atb::ensure_smem(prefilter_cols_kernel, smem, "atb_spline_prefilter");
+    if (rc != ATB_OK) return rc;
+    const dim3 grid((nl + kFirLines - 1) / kFirLines, (n + kFirRows - 1) / kFirRows);
+    prefilter_cols_kernel<<<grid, kFirThreads, smem, st>>>(src, dst, elem_stride, nl, n, boundary, taps);
+    return atb::check_launch("atb_spline_prefilter");
+  }
+  if (elem_stride == ncomp && nlines <= 65535) {
+    // elements contiguous: one line segment of 128 positions per CTA
+    const size_t smem = sizeof(double) * ncomp * (kFirSeg + 2 * taps.ntaps);
+    int rc = atb::ensure_smem(prefilter_rows_kernel, smem, "atb_spline_prefilter");
+    if (rc != ATB_OK) return rc;
+    const dim3 grid((n + kFirSeg - 1) / kFirSeg, nlines);
+    prefilter_rows_kernel<<<grid, kFirThreads, smem, st>>>(src, dst, line_stride, ncomp, n, boundary, taps);
+    return atb::check_launch("atb_spline_prefilter");
+  }
   const long long total = (long long)nlines * ncomp * n;
   const long long blocks = (total + kFirThreads - 1) / kFirThreads;
   if (blocks > 2147483647LL) return atb::fail(ATB_ERANGE, "atb_spline_prefilter: too many samples");
-  prefilter_kernel<<<(int)blocks, kFirThreads, 0, atb::as_stream(stream)>>>(
-      src, dst, line_stride, elem_stride, nlines, ncomp, n, boundary, order == 5 ? taps5 : taps3);
+  prefilter_kernel<<<(int)blocks, kFirThreads, 0, st>>>(src, dst, line_stride, elem_stride, nlines, ncomp, n,
+                                                         boundary, taps);
   return atb::check_launch("atb_spline_prefilter");
 }
 
