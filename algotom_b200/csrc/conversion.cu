@@ -6,12 +6,13 @@
 // -log'ed in float32, as the reference's NumPy float32 arithmetic does) is
 // staged in shared memory as FP64 with 12 copies of each end sample on
 // either side; a sub-pixel shift then follows scipy.ndimage.shift(x, (0, s),
-// order 3, mode "nearest"), the published cubic B-spline method: one thread
-// turns the padded row into spline coefficients with the recursive filter
-// of pole z = sqrt(3) - 2 (gain (1 - z)(1 - 1/z); causal start value of the
-// half-sample symmetric extension; anti-causal start z / (z - 1) c[n-1]),
-// and every thread samples the spline at x - s with the cubic B-spline
-// weights, coefficient indices clamped to the padded row.  (Along the angle
+// order 3, mode "nearest"), the published cubic B-spline method: the padded
+// row becomes spline coefficients through the prefilter of pole
+// z = sqrt(3) - 2 on its half-sample symmetric extension, applied as the
+// 65-tap FIR of its impulse response (spline_fir.cuh; every thread one
+// coefficient, exact to 1e-17 relative where the recursion is a serial chain
+// through the row), and every thread samples the spline at x - s with the
+// cubic B-spline weights, coefficient indices clamped to the padded row.  (Along the angle
 // axis the shift is zero and a cubic spline sampled at its knots returns its
 // samples, so rows are independent.)  The shifted row is rounded to float32
 // as scipy's output is.  extend_sinogram then scales the overlap columns by
@@ -20,8 +21,13 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "spline_fir.cuh"
 
 namespace {
+
+using atb::spline::make_taps;
+using atb::spline::sym_index;
+using atb::spline::Taps;
 
 constexpr int kPad = 12;       // end samples replicated on each side
 constexpr int kThreads = 256;
@@ -38,44 +44,30 @@ struct RowArgs {
   long long drs;
 };
 
-// cubic B-spline coefficients of c[0..n-1] in place (one thread); every
-// product and sum rounded on its own (no contraction), as NumPy does
-__device__ void spline_coefficients(double *c, int n) {
-  const double z = sqrt(3.0) - 2.0;
-  const double gain = __dmul_rn(1.0 - z, 1.0 - 1.0 / z);
-  for (int i = 0; i < n; ++i) c[i] = __dmul_rn(c[i], gain);
-  if (n == 1) return;
-  const double z_n = pow(z, (double)n);
-  const double c0 = c[0];
-  double z_i = z;
-  double s = __dadd_rn(c[0], __dmul_rn(z_n, c[n - 1]));
-  for (int i = 1; i < n; ++i) {
-    s = __dadd_rn(s, __dmul_rn(z_i, __dadd_rn(c[i], __dmul_rn(z_n, c[n - 1 - i]))));
-    z_i = __dmul_rn(z_i, z);
-  }
-  c[0] = __dadd_rn(__dmul_rn(s, z / (1.0 - __dmul_rn(z_n, z_n))), c0);
-  for (int i = 1; i < n; ++i) c[i] = __dadd_rn(c[i], __dmul_rn(z, c[i - 1]));
-  c[n - 1] = __dmul_rn(c[n - 1], z / (z - 1.0));
-  for (int i = n - 2; i >= 0; --i) c[i] = __dmul_rn(z, __dsub_rn(c[i + 1], c[i]));
-}
-
-__global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a) {
+__global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.ncol, big = n + 2 * kPad;
-  double *c = reinterpret_cast<double *>(smem);   // [big]
-  float *y = reinterpret_cast<float *>(c + big);  // [n] the (shifted) row
+  double *c = reinterpret_cast<double *>(smem);  // [big] spline coefficients
+  float *x = reinterpret_cast<float *>(c + big);  // [big] the padded row
+  float *y;                                       // [n] the (shifted) row
   const int row = blockIdx.x;
   const float *src = a.src + row * a.srs;
   for (int k = threadIdx.x; k < big; k += kThreads) {
     const int col = min(max(k - kPad, 0), n - 1);
     float v = src[a.flip ? n - 1 - col : col];
     if (a.apply_log) v = -logf(v);
-    c[k] = (double)v;
+    x[k] = v;
   }
   __syncthreads();
   if (a.shift != 0.0) {
-    if (threadIdx.x == 0) spline_coefficients(c, big);
+    for (int k = threadIdx.x; k < big; k += kThreads) {
+      double acc = taps.h[0] * (double)x[k];
+      for (int m = 1; m <= taps.ntaps; ++m)
+        acc += taps.h[m] * ((double)x[sym_index(k - m, big, 0)] + (double)x[sym_index(k + m, big, 0)]);
+      c[k] = acc;
+    }
     __syncthreads();
+    y = x;  // the padded row is no longer read
     for (int k = threadIdx.x; k < n; k += kThreads) {
       const double cc = __dadd_rn(__dsub_rn((double)k, a.shift), (double)kPad);
       const double f = floor(cc), t = __dsub_rn(cc, f), u = __dsub_rn(1.0, t);
@@ -94,7 +86,8 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a) {
       y[k] = __double2float_rn(v);
     }
   } else {
-    for (int k = threadIdx.x; k < n; k += kThreads) y[k] = (float)c[k + kPad];
+    y = reinterpret_cast<float *>(c);  // no coefficients needed
+    for (int k = threadIdx.x; k < n; k += kThreads) y[k] = x[k + kPad];
   }
   __syncthreads();
   float *dst = a.dst + row * a.drs;
@@ -127,10 +120,11 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a) {
 }
 
 int launch_rows(const RowArgs &a, const char *what, void *stream) {
-  const size_t smem = sizeof(double) * (a.ncol + 2 * kPad) + sizeof(float) * a.ncol;
+  static const Taps taps = make_taps(3);
+  const size_t smem = (sizeof(double) + sizeof(float)) * (a.ncol + 2 * kPad);
   int rc = atb::ensure_smem(row_kernel, smem, what);
   if (rc != ATB_OK) return rc;
-  row_kernel<<<a.nrow, kThreads, smem, atb::as_stream(stream)>>>(a);
+  row_kernel<<<a.nrow, kThreads, smem, atb::as_stream(stream)>>>(a, taps);
   return atb::check_launch(what);
 }
 
