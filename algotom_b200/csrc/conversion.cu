@@ -4,8 +4,8 @@
 //
 // One CTA per sinogram row.  The row (optionally mirrored left-right and
 // -log'ed in float32, as the reference's NumPy float32 arithmetic does) is
-// staged in shared memory as FP64 with 12 copies of each end sample on
-// either side; a sub-pixel shift then follows scipy.ndimage.shift(x, (0, s),
+// staged in shared memory with 12 copies of each end sample on either side;
+// a sub-pixel shift then follows scipy.ndimage.shift(x, (0, s),
 // order 3, mode "nearest"), the published cubic B-spline method: the padded
 // row becomes spline coefficients through the prefilter of pole
 // z = sqrt(3) - 2 on its half-sample symmetric extension, applied as the
