@@ -332,3 +332,95 @@ def find_center_based_slice_metric(sinogram, start, stop, step=0.5,
     else:
         center = coarse_center
     return center
+
+
+def _reconstruct_slice(sinogram, center, method, angles, ratio, filter_name,
+                       apply_log, gpu, ncore):
+    """One slice by ``method``; ``reconstruction.py:1177-1208``.  The
+    ``astra`` and ``gridrec`` back-ends wrap external packages and raise
+    ``NotImplementedError`` here."""
+    if method == "fbp":
+        return R.fbp_reconstruction(sinogram, center, angles=angles,
+                                    ratio=ratio, filter_name=filter_name,
+                                    apply_log=apply_log, gpu=gpu, ncore=ncore)
+    if method == "bpf":
+        return R.bpf_reconstruction(sinogram, center, angles=angles,
+                                    ratio=ratio, filter_name=filter_name,
+                                    apply_log=apply_log, gpu=gpu, ncore=ncore)
+    if method in ("astra", "gridrec"):
+        raise NotImplementedError(
+            "method %r: this library reconstructs with 'fbp', 'bpf' or "
+            "'dfi'" % (method,))
+    from .dfi import dfi_reconstruction
+    return dfi_reconstruction(sinogram, center, angles=angles, ratio=ratio,
+                              filter_name=filter_name, apply_log=apply_log,
+                              ncore=ncore)
+
+
+def find_center_visual_slices(sinogram, output, start, stop, step=1,
+                              zoom=0.5, method="fbp", gpu=False, angles=None,
+                              ratio=1.0, filter_name="hann", apply_log=True,
+                              ncore=None, display=False):
+    """Reconstructions of a sinogram at candidate centres written as TIFF
+    files ``center_<c>.tif`` into a new ``Find_center_<nnn>`` folder under
+    ``output``, for choosing the centre by eye; ``reconstruction.py:
+    1461-1533``.  The (zoomed) sinogram is filtered or ``-log``-ed once and
+    every candidate is a work item of one persistent back-projection launch
+    (``fbp`` / ``bpf``; ``dfi`` reconstructs candidate by candidate).
+    Returns the folder path (with a trailing ``/``)."""
+    import scipy.ndimage as ndi
+    from ._files import make_folder_name, save_image
+    output_name = make_folder_name(output, name_prefix="Find_center",
+                                   zero_prefix=3)
+    output_base = output + "/" + output_name + "/"
+    (nrow, ncol) = sinogram.shape
+    step = np.clip(step, 0.05, ncol - 1)
+    start = np.clip(start, 0, ncol - 1)
+    stop = np.clip(stop + step, start + step, ncol - 1)
+    t, _ = R._to_device(sinogram)
+    if t.dtype != torch.float32:
+        t = t.to(torch.float32)
+    if zoom != 1.0:
+        t = zoom_image(t, zoom)
+        start, stop, step = start * zoom, stop * zoom, step * zoom
+        list_center = np.arange(start, stop, step)
+        if angles is not None:
+            # the angle table is host setup: scipy's own 1-D zoom
+            a = angles.detach().cpu().numpy() if isinstance(
+                angles, torch.Tensor) else np.asarray(angles)
+            angles = ndi.zoom(np.tile(a, (1, 1)), (1.0, zoom))[0]
+        sino = t
+    else:
+        list_center = np.arange(start, stop, step)
+        sino = sinogram
+    out_dtype = np.float32 if method == "fbp" else np.float64
+    if method == "dfi":
+        # DFI takes the logarithm after its sub-pixel centring shift, so
+        # each candidate gets the transmission data (and its own warning)
+        def chunks():
+            for c in list_center:
+                yield [c], _reconstruct_slice(
+                    sino, c, method, angles, ratio, filter_name, apply_log,
+                    gpu, ncore)[None]
+    else:
+        # -log once, with the reference's warning and in-place repair of
+        # the array being reconstructed (the caller's own only without zoom)
+        sino = _prepare(sino, 0, apply_log)
+        source = _Source(sino, angles, method, filter_name)
+        ncol1 = sino.shape[1]
+        per_chunk = max(1, int(_CHUNK_BYTES // (4 * ncol1 * ncol1)))
+
+        def chunks():
+            for k0 in range(0, len(list_center), per_chunk):
+                cs = list_center[k0:k0 + per_chunk]
+                yield cs, source.reconstruct(cs, ratio)
+    for cs, imgs in chunks():
+        imgs = imgs.cpu().numpy() if isinstance(imgs, torch.Tensor) else \
+            np.asarray(imgs)
+        for center, img in zip(cs, imgs):
+            file_name = "center_{0:.2f}".format(center / zoom) + ".tif"
+            save_image(output_base + file_name, img.astype(out_dtype))
+            if display:
+                print("Done: {}".format(output_base + file_name))
+    return output_base
+

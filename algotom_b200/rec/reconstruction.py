@@ -541,7 +541,8 @@ def bpf_reconstruction(sinogram, center, angles=None, ratio=1.0,
 # centre search by slice metrics (reconstruction.py:1254-1458), kept in this
 # module's namespace like the reference's
 from .center import (find_center_based_slice_metric,  # noqa: E402,F401
-                     _find_center_based_slice_metric)
+                     _find_center_based_slice_metric, _reconstruct_slice,
+                     find_center_visual_slices)
 
 # direct Fourier inversion (reconstruction.py:687-907)
 from .dfi import (dfi_reconstruction,  # noqa: E402,F401

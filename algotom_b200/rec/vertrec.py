@@ -739,6 +739,50 @@ def _entropy(imgs, nmin, nmax):
     return out.cpu().numpy()
 
 
+def _candidate_slices(projections, slice_index, centers, alpha, angles,
+                      chunk_size, ramp_filter, sigma, apply_log, gpu):
+    """Yield ``(first, slices)`` for consecutive groups of ``centers``: the
+    vertical slice at ``slice_index`` / ``alpha`` reconstructed at each
+    centre as the searches' ``vertical_reconstruction`` calls make it (hann
+    window, pad min(0.15 width, 150), edge mode, no mask, ``-log`` in the
+    smoothing pass), every centre of a group a line of the same launch;
+    float64 CUDA tensors after the "after" ramp filter, float32 otherwise.
+    The reconstructions' own argument checks run first, for every centre."""
+    (num_proj, height, width) = projections.shape
+    geo = None
+    for cen in centers:
+        geo = _check_common(projections, cen, angles, (0, 0, 0, 0), 0, -1,
+                            ramp_filter)
+    if slice_index < 0 or slice_index > (width - 1):
+        raise ValueError("Index (relative to the cropped image) is out of "
+                         "range {})".format((0, width - 1)))
+    pad = min(int(0.15 * width), 150)
+    xlist, ylist = _get_points_single_line(slice_index, alpha, width)
+    out_dtype = torch.float64 if ramp_filter == "after" else torch.float32
+    log_text = ("!!! Applying logarithm is enabled but there are values "
+                "<= 0.0 in the data !!!")
+    per_pass = max(1, int(_SEARCH_BYTES // (8 * height * width)))
+    for g0 in range(0, len(centers), per_pass):
+        group = centers[g0:g0 + per_pass]
+        xs = np.tile(np.asarray(xlist), (len(group), 1))
+        ys = np.tile(np.asarray(ylist), (len(group), 1))
+        recs = _reconstruct(
+            projections, xs, ys, group[0], geo, None, None, chunk_size,
+            ramp_filter, "hann", pad, "edge", apply_log, gpu, False, False,
+            round_points=False, line_centers=group, sigma=sigma,
+            log_warning=log_text if g0 == 0 else "", device_out=True)
+        yield g0, recs.to(out_dtype)
+
+
+def _search_mask(list_center, width):
+    """The mask of the smallest candidate centre (vertrec.py:1355-1361)."""
+    rad = int(min(np.min(list_center), width - np.min(list_center)))
+    pad_left = (width - 2 * rad) // 2
+    pad_right = width - 2 * rad - pad_left
+    return np.pad(np.ones(2 * rad, dtype=np.float32), (pad_left, pad_right),
+                  mode="constant")
+
+
 def find_center_vertical_slice(projections, slice_index, start, stop,
                                step=1.0, metric="entropy", alpha=0.0,
                                angles=None, chunk_size=30,
@@ -776,46 +820,19 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
     if angles is None:
         angles = np.deg2rad(np.linspace(0.0, 180.0, num_proj))
     use_entropy = metric_function is None and metric == "entropy"
-    mean_center = np.mean(list_center) if use_entropy else None
-    # the reconstructions' own checks, for every centre they would get
-    geo = None
-    for cen in ([mean_center] if use_entropy else []) + list(list_center):
-        geo = _check_common(projections, cen, angles, (0, 0, 0, 0), 0, -1,
-                            ramp_filter)
-    if slice_index < 0 or slice_index > (width - 1):
-        raise ValueError("Index (relative to the cropped image) is out of "
-                         "range {})".format((0, width - 1)))
-    pad = min(int(0.15 * width), 150)
-    xlist, ylist = _get_points_single_line(slice_index, alpha, width)
-    out_dtype = torch.float64 if ramp_filter == "after" else torch.float32
-    mask = None
-    if masking:
-        rad = int(min(np.min(list_center), width - np.min(list_center)))
-        pad_left = (width - 2 * rad) // 2
-        pad_right = width - 2 * rad - pad_left
-        mask = np.pad(np.ones(2 * rad, dtype=np.float32),
-                      (pad_left, pad_right), mode="constant")
-    log_text = ("!!! Applying logarithm is enabled but there are values "
-                "<= 0.0 in the data !!!")
-    centers = ([mean_center] if use_entropy else []) + list(list_center)
-    per_pass = max(1, int(_SEARCH_BYTES // (8 * height * width)))
+    centers = ([np.mean(list_center)] if use_entropy else []) + \
+        list(list_center)
+    mask = _search_mask(list_center, width) if masking else None
     nmin = nmax = None
     if show_progress:
         t0 = time.time()
     done = 0
-    for g0 in range(0, len(centers), per_pass):
-        group = centers[g0:g0 + per_pass]
-        xs = np.tile(np.asarray(xlist), (len(group), 1))
-        ys = np.tile(np.asarray(ylist), (len(group), 1))
-        recs = _reconstruct(
-            projections, xs, ys, group[0], geo, None, None, chunk_size,
-            ramp_filter, "hann", pad, "edge", apply_log, gpu, False, False,
-            round_points=False, line_centers=group, sigma=sigma,
-            log_warning=log_text if g0 == 0 else "", device_out=True)
-        recs = recs.to(out_dtype)
+    for g0, recs in _candidate_slices(projections, slice_index, centers,
+                                      alpha, angles, chunk_size, ramp_filter,
+                                      sigma, apply_log, gpu):
         if use_entropy and g0 == 0:
             first = recs[0]
-            if out_dtype == torch.float32:
+            if recs.dtype == torch.float32:
                 nmin = np.float32(first.min().item())
                 nmax = np.float32(first.max().item())
             else:
@@ -823,7 +840,7 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
             recs = recs[1:]
         if mask is not None:
             recs = recs * torch.from_numpy(mask).to(recs.device).to(
-                out_dtype)
+                recs.dtype)
         k = len(recs)
         if k == 0:
             continue
@@ -858,3 +875,49 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
         return list_center, list_metric
     else:
         return center
+
+
+def find_center_visual_vertical_slices(projections, output_folder,
+                                       slice_index, start, stop, step=1.0,
+                                       alpha=0.0, angles=None, chunk_size=30,
+                                       ramp_filter="after", apply_log=True,
+                                       gpu=True, block=(16, 16), ncore=None,
+                                       prefer="processes", display=True,
+                                       masking=True):
+    """The vertical slice reconstructed at every centre of
+    ``np.arange(start, stop + step, step)`` written as TIFF files
+    ``center_<c>.tif`` into a new ``Find_center_<nnn>`` folder under
+    ``output_folder``, for choosing the centre by eye;
+    ``vertrec.py:1431-1535``.  ``-log`` runs chunk by chunk on the device
+    (with the reference's warning and in-place repair), and every candidate
+    is a line of the same vertical back-projection launch.  Returns the
+    folder path (with a trailing ``/``)."""
+    from ._files import make_folder_name, save_image
+    output_name = make_folder_name(output_folder, name_prefix="Find_center",
+                                   zero_prefix=3)
+    output_base = output_folder + "/" + output_name + "/"
+    list_center = np.arange(start, stop + step, step)
+    (num_proj, height, width) = projections.shape
+    if angles is None:
+        angles = np.deg2rad(np.linspace(0.0, 180.0, num_proj))
+    if ramp_filter is None:
+        ramp_filter = "after"
+    mask = _search_mask(list_center, width) if masking else None
+    if display:
+        t0 = time.time()
+    for g0, recs in _candidate_slices(projections, slice_index,
+                                      list(list_center), alpha, angles,
+                                      chunk_size, ramp_filter, 0, apply_log,
+                                      gpu):
+        host = recs.cpu().numpy()
+        for i, recon in enumerate(host):
+            if mask is not None:
+                recon = recon * mask
+            center = list_center[g0 + i]
+            file_name = "center_{0:.2f}".format(center) + ".tif"
+            save_image(output_base + file_name, recon)
+            if display:
+                print("Done: {0}. Time elapsed {1:.2f}".format(
+                    output_base + file_name, time.time() - t0))
+    return output_base
+

@@ -453,6 +453,73 @@ def make_conversion():
     np.savez_compressed(os.path.join(HERE, "golden_conversion.npz"), **out)
 
 
+def make_visual():
+    """The visual centre searches (reconstruction.py:1461-1533,
+    vertrec.py:1431-1535), CPU path: the file names each writes and the
+    images read back from them."""
+    import shutil
+    import tempfile
+    from PIL import Image
+    import algotom.rec.vertrec as vrec
+
+    def read_folder(base):
+        names = sorted(os.listdir(base))
+        imgs = [np.array(Image.open(os.path.join(base, n))) for n in names]
+        return np.array(names), np.stack(imgs)
+
+    n, nrow, cen = 96, 91, 46.3
+    sino, ang, _ = phantom.ellipse_sinogram(41, nrow, n, cen, photons=2e4)
+    trans = np.exp(-sino).astype(np.float32)
+    out = {"trans": trans, "angles": ang}
+    cases = {
+        "fbp_zoom": dict(start=42.0, stop=50.0, step=1.5, zoom=0.5),
+        "fbp_angles": dict(start=44.0, stop=48.0, step=1.0, zoom=1.0,
+                           angles=ang, ratio=0.0),
+        "bpf": dict(start=45.0, stop=47.0, step=0.5, zoom=1.0,
+                    method="bpf"),
+        "dfi_zoom": dict(start=44.0, stop=47.0, step=1.0, zoom=0.5,
+                         method="dfi", filter_name=None),
+    }
+    tmp = tempfile.mkdtemp()
+    try:
+        for name, kw in cases.items():
+            base = rec.find_center_visual_slices(trans.copy(), tmp, **kw,
+                                                 gpu=False, ncore=1)
+            out[_key("vis", name, "folder")] = np.array(
+                os.path.basename(base.rstrip("/")))
+            out[_key("vis", name, "names")], out[_key("vis", name, "imgs")] = \
+                read_folder(base)
+        w, h = 61, 40
+        mat = util.make_circle_mask(w, 0.8)
+        for rad, i_s, j_s in ((10, 30, 20), (5, 20, 30), (5, 20, 50)):
+            mat[i_s:i_s + rad, j_s:j_s + rad] = 0
+        mat = ndi.gaussian_filter(mat, 1)
+        vol = np.zeros((h, w, w), dtype=np.float32)
+        vol[1:] = mat
+        ang360 = np.linspace(0.0, 360.0, 91, dtype=np.float32)
+        projs = np.zeros((91, h, w), dtype=np.float32)
+        for i, a in enumerate(ang360):
+            projs[i] = np.sum(ndi.rotate(vol, -a, axes=(1, 2), order=1,
+                                         reshape=False), axis=1)
+        projs = projs[:46] + 1
+        out["cube_projs"] = projs
+        vcases = {
+            "after": dict(start=28.0, stop=31.0, step=1.0),
+            "before_nomask": dict(start=29.0, stop=30.5, step=0.5,
+                                  ramp_filter="before", masking=False,
+                                  alpha=30.0),
+        }
+        for name, kw in vcases.items():
+            base = vrec.find_center_visual_vertical_slices(
+                projs.copy(), tmp, w // 2, **kw, gpu=False, ncore=1,
+                display=False)
+            out[_key("vvis", name, "names")], out[_key("vvis", name, "imgs")] \
+                = read_folder(base)
+    finally:
+        shutil.rmtree(tmp)
+    np.savez_compressed(os.path.join(HERE, "golden_visual.npz"), **out)
+
+
 def make_dfi():
     """DFI reconstruction (reconstruction.py:687-907)."""
     nrow, ncol, cen = 181, 96, 47.3
@@ -498,7 +565,7 @@ def make_dfi():
 GENERATORS = {"windows": make_windows, "filter": make_filter, "bp": make_bp,
               "recon": make_recon, "unittest": make_reference_test_fixture,
               "center": make_center, "vertical": make_vertical,
-              "vcenter": make_vcenter,
+              "vcenter": make_vcenter, "visual": make_visual,
               "conversion": make_conversion, "dfi": make_dfi}
 
 if __name__ == "__main__":
