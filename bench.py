@@ -57,6 +57,8 @@ def _args():
     ap.add_argument("--storage", default="float32",
                     choices=["float32", "float16", "bfloat16"],
                     help="element type of the filtered sinogram (stack)")
+    ap.add_argument("--items", type=int, default=64,
+                    help="sinograms of the batch workload")
     ap.add_argument("--rows", type=int, default=512,
                     help="detector rows of the vertical workload")
     ap.add_argument("--workload", default="stack",
@@ -411,7 +413,7 @@ def run_batch(args):
     from algotom_b200 import phantom
     from algotom_b200.rec import batch as B
     dev = torch.device("cuda", 0)
-    geo = B.uneven_batch_geometry()
+    geo = B.uneven_batch_geometry(n_items=args.items)
     sinos = []
     for k, g in enumerate(geo):
         s, _, _ = phantom.ellipse_sinogram(3000 + k, g["nrow"], g["ncol"],
@@ -465,8 +467,9 @@ def run_batch(args):
         "value": bf.updates / t, "unit": "updates/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "64 uneven sinograms, one persistent launch "
-                               "under a CUDA graph", "items": len(geo),
+        "config": {"workload": "%d uneven sinograms, one persistent launch "
+                               "under a CUDA graph" % len(geo),
+                   "items": len(geo),
                    "tile_variant": bf.variant, "units": bf.nunits,
                    "updates": bf.updates},
         "roofline": {"bound": "smem", "kernel": "bp_batch_kernel",
