@@ -460,7 +460,14 @@ def run_batch(args):
         k = min(range(len(geo)), key=lambda i: geo[i]["ncol"])
         ref = O.fbp_reconstruction(sinos[k].cpu().numpy(), geo[k]["center"],
                                    angles=geo[k]["angles"], apply_log=False)
-        err = {"rel_l2": O.rel_l2(bf.outputs[k].cpu().numpy(), ref),
+        from algotom_b200.rec import reconstruction as RR
+        single = RR.fbp_reconstruction(sinos[k], geo[k]["center"],
+                                       angles=geo[k]["angles"],
+                                       apply_log=False)
+        got = bf.outputs[k].cpu().numpy()
+        err = {"rel_l2": O.rel_l2(got, ref),
+               "rel_l2_vs_single_slice_path": O.rel_l2(got,
+                                                       single.cpu().numpy()),
                "item": k, "ncol": geo[k]["ncol"]}
     print(json.dumps({
         "metric": "batched uneven FBP pixel-angle updates/s",
