@@ -18,7 +18,8 @@
 //   scaled to the sinogram's rows), then the quintic B-spline interpolation
 //   of the complex row spectra at that point with half-sample symmetric
 //   taps (map_coordinates(order=5, mode="reflect")), times the unit circle
-//   mask of make_circle_mask(W, 1.0).  FP64 throughout.
+//   mask of make_circle_mask(W, 1.0), written in ifftshift order (ready for
+//   the inverse transform).  FP64 throughout.
 #include <cmath>
 
 #include "common.cuh"
@@ -152,10 +153,13 @@ __global__ void __launch_bounds__(kGridThreads)
   const long long e = blockIdx.x * (long long)kGridThreads + threadIdx.x;
   if (e >= (long long)w * w) return;
   const int i = (int)(e / w), j = (int)(e - (long long)i * w);
+  // written where ifftshift puts it: (i - w // 2, j - w // 2) mod w
+  const long long oi = (i + w - w / 2) % w, oj = (j + w - w / 2) % w;
+  double2 *o = out + oi * w + oj;
   // circle mask of make_circle_mask(w, 1.0): integer grid centred at w // 2
   const long long cm = w / 2, dx = j - cm, dy = i - cm;
   if (dx * dx + dy * dy > cm * cm) {
-    out[e] = make_double2(0.0, 0.0);
+    *o = make_double2(0.0, 0.0);
     return;
   }
   // generate_mapping_coordinate (height_rec = width_rec = width_sino = w)
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(kGridThreads)
     re += wr[a] * sr;
     im += wr[a] * si;
   }
-  out[e] = make_double2(re, im);
+  *o = make_double2(re, im);
 }
 
 }  // namespace

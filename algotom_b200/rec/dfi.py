@@ -133,9 +133,11 @@ def _circle_mask(width, ratio, device):
         torch.float64)
 
 
-def _dfi_slice(s, window):
+def _dfi_slice(s, window, pad, ncol):
     """Steps 3-5 for one prepared float32 [nrow, ncol2] CUDA sinogram;
-    returns the float64 [ncol2, ncol2] image before the crop."""
+    returns the float64 [ncol, ncol] image (cropped at ``pad``).  The
+    regridding writes its grid in ifftshift order and the final fftshift
+    and crop are one index gather, so the 2-D shifts cost no extra pass."""
     nrow, w = s.shape
     x = s.to(torch.float64)
     f = torch.fft.fftshift(torch.fft.fft(torch.fft.ifftshift(x, dim=1),
@@ -146,7 +148,11 @@ def _dfi_slice(s, window):
     reg = torch.empty((w, w), dtype=torch.complex128, device=s.device)
     nat.call("atb_dfi_regrid", f.data_ptr(), nrow, w, reg.data_ptr(),
              R._stream_ptr(s.device))
-    return torch.fft.fftshift(torch.fft.ifft2(torch.fft.ifftshift(reg))).real
+    y = torch.fft.ifft2(reg).real
+    # fftshift(y)[k] = y[(k - w // 2) mod w], rows and columns pad..pad+ncol
+    idx = torch.remainder(torch.arange(pad, pad + ncol, device=s.device)
+                          - w // 2, w)
+    return y.index_select(0, idx).index_select(1, idx)
 
 
 def dfi_reconstruction(sinogram, center, angles=None, ratio=1.0,
@@ -200,7 +206,7 @@ def dfi_reconstruction(sinogram, center, angles=None, ratio=1.0,
         mask = _circle_mask(ncol, ratio, t.device)
     out = []
     for s in stack:
-        r = _dfi_slice(s, window)[pad:ncol + pad, pad:ncol + pad]
+        r = _dfi_slice(s, window, pad, ncol)
         out.append(r * mask if mask is not None else r)
     rec = torch.stack(out, dim=1) if len(out) > 1 or input_3d else out[0]
     dtype = torch.float64 if filter_name is not None else torch.float32

@@ -465,7 +465,9 @@ int atb_spline_prefilter(const double *src, double *dst, int64_t line_stride,
  *   coef   complex128 [nrow][width]: quintic B-spline coefficients of the
  *          centred row spectra (atb_spline_prefilter, order 5, boundary 0,
  *          along both axes)
- *   out    complex128 [width][width], natural (not shifted) order
+ *   out    complex128 [width][width] in ifftshift order: frequency grid
+ *          point (i, j) at ((i - width/2) mod width, (j - width/2) mod
+ *          width), ready for the inverse 2-D transform
  */
 int atb_dfi_regrid(const double *coef, int nrow, int width, double *out,
                    void *stream);
