@@ -142,10 +142,24 @@ __device__ __forceinline__ void fft_stage(float2 *x, int log2m, int logNs, const
     if (b < nb && j < Q) {
       const int k = j & (Ns - 1);
       if (k) {
+        // w^(r k) for r = 1 .. R-1: the powers 1, 2, 4, 8 of w^k from the
+        // tables, each other one the product of those of its set bits (at
+        // most three roundings), against 2 (R - 1) table reads per butterfly
+        auto tw = [&](int c) {
+          const int t = (c * k) << tsh;
+          return cmul(ta[t >> L], tb[t & lmask]);
+        };
+        const float2 w1 = tw(1);
+        const float2 w2 = R >= 4 ? tw(2) : w1;
+        const float2 w4 = R >= 8 ? tw(4) : w1;
+        const float2 w8 = R >= 16 ? tw(8) : w1;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const int t = (r * k) << tsh;
-          v[b][r] = cmul(v[b][r], cmul(ta[t >> L], tb[t & lmask]));
+          float2 w = (r & 1) ? w1 : ((r & 2) ? w2 : ((r & 4) ? w4 : w8));
+          if ((r & 1) && (r & 2)) w = cmul(w, w2);
+          if ((r & 3) && (r & 4)) w = cmul(w, w4);
+          if ((r & 7) && (r & 8)) w = cmul(w, w8);
+          v[b][r] = cmul(v[b][r], w);
         }
       }
       dft<R>(v[b]);
