@@ -66,13 +66,28 @@ def _to_device(x, device=None):
     return t, is_np
 
 
+_trig_cache = {}
+
+
 def _trig(angles, device):
-    """(cos(-a), sin(-a)) in FP64 of the float32-rounded angles."""
-    a = np.float32(np.asarray(angles, dtype=np.float64)).astype(np.float64)
+    """(cos(-a), sin(-a)) in FP64 of the float32-rounded angles, as a
+    device table kept for reuse: a repeated angle set costs neither the host
+    trigonometry nor a host-to-device copy (which, from pageable memory,
+    would also wait for the work already queued on the stream)."""
+    a = np.float32(np.asarray(angles, dtype=np.float64))
+    key = (a.tobytes(), str(device))
+    t = _trig_cache.get(key)
+    if t is not None:
+        return t
+    a = a.astype(np.float64)
     if not np.all(np.isfinite(a)):
         raise ValueError("angles must be finite")
     tab = np.stack([np.cos(-a), np.sin(-a)], axis=1)
-    return torch.from_numpy(np.ascontiguousarray(tab)).to(device)
+    t = torch.from_numpy(np.ascontiguousarray(tab)).to(device)
+    if len(_trig_cache) >= 16:
+        _trig_cache.clear()
+    _trig_cache[key] = t
+    return t
 
 
 def _twiddle(log2m, device):
