@@ -64,7 +64,7 @@ def _args():
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "batch", "single", "bpf", "volume",
                              "center", "vertical", "vcenter", "halfacq",
-                             "dfi"],
+                             "dfi", "reference_gpu"],
                     help="stack: the 256-slice benchmark (default); bpf: the "
                          "same data through bpf_reconstruction; volume: 2160 "
                          "slices streamed slab by slab with float32 / float16 "
@@ -75,6 +75,8 @@ def _args():
                          "center: centre search over 128 candidates; "
                          "vertical: vertical slices from 1801 projections; "
                          "vcenter: centre search on a vertical slice; "
+                         "reference_gpu: algotom's own Numba CUDA path "
+                         "(from baseline/_ref) on the same data; "
                          "halfacq: a 360-degree offset-axis slice extended "
                          "and reconstructed; dfi: direct Fourier inversion "
                          "of one slice")
@@ -1054,6 +1056,82 @@ def run_vcenter(args):
         "gpu_launches": launches * args.steps}), flush=True)
 
 
+def run_reference_gpu(args):
+    """The reference's own GPU path (Numba CUDA), unmodified, imported from a
+    pip install of algotom under baseline/_ref (``pip install --target
+    baseline/_ref``; not part of this repository): ``back_projection_gpu``
+    on one 1024^2 x 900 slice, ``back_projection_gpu_chunk`` and
+    ``fbp_reconstruction(gpu=True)`` on the first ``--slices`` (default 16)
+    slices of the stacked benchmark.  Host arrays in and out, as its API
+    takes them (its kernels copy to and from the device on every call); the
+    filter of its fbp_reconstruction runs on the host.  Prints an
+    ``unavailable`` line when the install or Numba's CUDA target is
+    missing."""
+    import types
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    try:
+        for m in ("pywt", "h5py"):  # imported by algotom, unused on this path
+            sys.modules.setdefault(m, types.ModuleType(m))
+        os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
+        sys.path.insert(0, ref)
+        from numba import cuda
+        if not cuda.is_available():
+            raise RuntimeError("Numba's CUDA target is not available")
+        import algotom.rec.reconstruction as rec
+        if not os.path.abspath(rec.__file__).startswith(ref):
+            raise RuntimeError("algotom not found under baseline/_ref")
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference-gpu",
+                          "unavailable": "%s: %s" % (type(e).__name__, e)}))
+        return
+    from algotom_b200 import phantom
+
+    def timed(fn, n):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        return (time.perf_counter() - t0) / n
+
+    s1, a1, _ = phantom.ellipse_sinogram(1000, 900, 1024, 511.5, photons=1e4)
+    s1 = np.float32(s1)
+    u1 = 1024 * 1024 * 900
+    t_bp1 = timed(lambda: rec.back_projection_gpu(s1, a1, 511.5),
+                  max(1, args.steps))
+    t_fbp1 = timed(lambda: rec.fbp_reconstruction(s1, 511.5, angles=a1,
+                                                  apply_log=False, gpu=True),
+                   max(1, args.steps))
+    nsl = args.slices if args.slices != NSLICE else 16
+    ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
+    st = np.empty((NROW, nsl, NCOL), np.float32)
+    for k in range(nsl):
+        st[:, k, :] = phantom.ellipse_sinogram(2000 + k, NROW, NCOL, CENTER,
+                                               photons=PHOTONS,
+                                               angles=ang)[0]
+    u2 = nsl * NCOL * NCOL * NROW
+    t_bp2 = timed(lambda: rec.back_projection_gpu_chunk(st, ang, CENTER), 1)
+    t_fbp2 = timed(lambda: rec.fbp_reconstruction(st, CENTER, angles=ang,
+                                                  apply_log=False, gpu=True),
+                   1)
+    print(json.dumps({
+        "impl": "reference-gpu",
+        "metric": METRIC, "value": u2 / t_fbp2, "unit": "updates/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded 12-ellipse phantoms)",
+        "config": {"workload": "algotom's fbp_reconstruction(gpu=True) on %d "
+                               "of the 256 slices (1801 x 2560), host arrays "
+                               "in and out" % nsl},
+        "seconds": {"fbp_reconstruction_gpu_stack": t_fbp2,
+                    "back_projection_gpu_chunk_stack": t_bp2,
+                    "fbp_reconstruction_gpu_1024": t_fbp1,
+                    "back_projection_gpu_1024": t_bp1},
+        "updates_per_s": {"fbp_reconstruction_gpu_stack": u2 / t_fbp2,
+                          "back_projection_gpu_chunk_stack": u2 / t_bp2,
+                          "fbp_reconstruction_gpu_1024": u1 / t_fbp1,
+                          "back_projection_gpu_1024": u1 / t_bp1}}),
+          flush=True)
+
+
 def run_halfacq(args):
     """Half-acquisition slice: a 360-degree sinogram of 3601 angles x 2560
     detector pixels whose rotation axis sits at 2300.4 (offset), extended on
@@ -1216,6 +1294,9 @@ def main():
         return
     if args.workload == "vcenter":
         run_vcenter(args)
+        return
+    if args.workload == "reference_gpu":
+        run_reference_gpu(args)
         return
     if args.workload == "center":
         run_center(args)
