@@ -1101,6 +1101,17 @@ def run_reference_gpu(args):
     t_fbp1 = timed(lambda: rec.fbp_reconstruction(s1, 511.5, angles=a1,
                                                   apply_log=False, gpu=True),
                    max(1, args.steps))
+    # the same slice through this build and the FP64 oracle
+    from algotom_b200.rec import reconstruction as R
+    from oracle import fbp_oracle as O
+    ref1 = rec.fbp_reconstruction(s1, 511.5, angles=a1, apply_log=False,
+                                  gpu=True)
+    ours1 = R.fbp_reconstruction(s1, 511.5, angles=a1, apply_log=False)
+    fp64 = O.fbp_reconstruction(s1, 511.5, angles=a1, apply_log=False)
+    acc = {"slice": "1024^2 x 900",
+           "reference_gpu_vs_fp64_oracle": O.rel_l2(ref1, fp64),
+           "this_build_vs_fp64_oracle": O.rel_l2(ours1, fp64),
+           "this_build_vs_reference_gpu": O.rel_l2(ours1, ref1)}
     nsl = args.slices if args.slices != NSLICE else 16
     ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
     st = np.empty((NROW, nsl, NCOL), np.float32)
@@ -1125,6 +1136,7 @@ def run_reference_gpu(args):
                     "back_projection_gpu_chunk_stack": t_bp2,
                     "fbp_reconstruction_gpu_1024": t_fbp1,
                     "back_projection_gpu_1024": t_bp1},
+        "accuracy": acc,
         "updates_per_s": {"fbp_reconstruction_gpu_stack": u2 / t_fbp2,
                           "back_projection_gpu_chunk_stack": u2 / t_bp2,
                           "fbp_reconstruction_gpu_1024": u1 / t_fbp1,
