@@ -325,16 +325,37 @@ def _host_tensor(x):
     return torch.from_numpy(a)
 
 
+def _slab_spans(nslice, slab):
+    """(first slice, count) of the slabs of a streamed stack: full slabs of
+    ``slab``, with the first and last ramped (slab/4, slab/4, slab/2) so the
+    copy-in that nothing overlaps before the first kernel and the copy-out
+    after the last one are short."""
+    ramp = [max(1, slab // 4), max(1, slab // 4), max(1, slab // 2)]
+    if nslice < 2 * slab + 2 * sum(ramp):
+        sizes = [slab] * (nslice // slab) + ([nslice % slab]
+                                            if nslice % slab else [])
+    else:
+        mid = nslice - 2 * sum(ramp)
+        sizes = ramp + [slab] * (mid // slab) + \
+            ([mid % slab] if mid % slab else []) + ramp[::-1]
+    spans, k0 = [], 0
+    for n in sizes:
+        spans.append((k0, n))
+        k0 += n
+    return spans
+
+
 def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
                   pad, pad_mode, apply_log, out_host, storage, kahan,
                   slab=SLAB):
     """FBP of a host stack [nrow, nslice, ncol] streamed through the device
-    in slabs of ``slab`` slices: while slab k is filtered and
-    back-projected, slab k+1 is copied in and slab k-1 copied out (one copy
-    stream each way, double-buffered, ordered by events)."""
+    in slabs of up to ``slab`` slices (ramped at both ends): while slab k is
+    filtered and back-projected, slab k+1 is copied in and slab k-1 copied
+    out (one copy stream each way, double-buffered, ordered by events)."""
     nrow, nslice, ncol = host.shape
     dev = _device()
     k_sl = max(1, min(slab, nslice))
+    spans = _slab_spans(nslice, k_sl)
     cmp = torch.cuda.current_stream(dev)
     s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     in_buf = [torch.empty((nrow, k_sl, ncol), dtype=torch.float32, device=dev)
@@ -353,10 +374,8 @@ def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
     hp, op = host.data_ptr(), out_host.data_ptr()
     trig = _trig(angles, dev)
     cmp.synchronize()
-    nslab = (nslice + k_sl - 1) // k_sl
-    for k in range(nslab):
-        b, k0 = k % 2, k * k_sl
-        kk = min(k_sl, nslice - k0)
+    for k, (k0, kk) in enumerate(spans):
+        b = k % 2
         if k >= 2:
             s_in.wait_event(ev_in_free[b])
         nat.call("atb_copy_2d", in_buf[b].data_ptr(), slab_b, hp + k0 * ncol * 4,

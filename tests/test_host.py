@@ -174,3 +174,18 @@ def test_bpf_image_padding_matches_numpy(mode):
             ref = np.stack([np.pad(a, pad, mode=mode) for a in x])
             assert got.shape == ref.shape
             assert np.allclose(got, ref, rtol=1e-14, atol=1e-14), (n, pad)
+
+
+def test_stream_slab_spans_cover_the_stack():
+    """Slabs of a host stack streamed through the device: contiguous, cover
+    every slice once, at most ``slab`` slices, ramped at both ends of long
+    stacks."""
+    from algotom_b200.rec.reconstruction import _slab_spans
+    for n in (1, 5, 31, 32, 33, 64, 79, 100, 128, 256, 257, 2160):
+        for slab in (1, 4, 32):
+            sp = _slab_spans(n, slab)
+            assert sp[0][0] == 0 and sum(c for _, c in sp) == n
+            assert all(0 < c <= slab for _, c in sp)
+            assert all(a + c == b for (a, c), (b, _) in zip(sp, sp[1:]))
+    sizes = [c for _, c in _slab_spans(256, 32)]
+    assert sizes[:3] == [8, 8, 16] and sizes[-3:] == [16, 8, 8]
