@@ -24,8 +24,9 @@
 // writes its FP64 partial sums to caller scratch and a second kernel adds
 // the groups in a fixed order, so results do not depend on scheduling.  The
 // grid runs all (line, point block) CTAs of one row block next to each
-// other, so a row block's projection rows are read from HBM about once per
-// angle group however many lines share them.
+// other, so the lines resident together share a row block's projection
+// rows through L2 (with 64 lines about 8 slices' CTAs fit at once, and the
+// rows are read from HBM about 6 times rather than 64).
 #include <cmath>
 
 #include "common.cuh"
