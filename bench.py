@@ -100,7 +100,13 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        # the samples are summarised into the bench line; the raw file goes
+        # where BENCH_CLOCKS_DIR says (default: the system temp folder)
+        import tempfile
+        base = os.environ.get("BENCH_CLOCKS_DIR",
+                              os.path.join(tempfile.gettempdir(),
+                                           "algotom_b200_bench"))
+        self.path = os.path.join(base, "clocks_rank%d.csv" % gpu_index)
 
     def start(self):
         try:
