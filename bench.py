@@ -151,7 +151,8 @@ class ClockSampler:
 
 def _traffic_per_update():
     """DRAM bytes per update of the back-projection kernel, from the
-    committed ncu summary (profiles/backproject_*.md), if present."""
+    committed ncu summary of the back-projector under profiles/ (its
+    `dram_bytes_per_update:` line), if present."""
     d = os.path.join(ROOT, "profiles")
     try:
         names = sorted(os.listdir(d))
@@ -766,7 +767,8 @@ def run_center(args):
 
 
 def _profile_figure(prefix, key):
-    """A figure `key: value` from a committed ncu summary profiles/<prefix>*.md."""
+    """A figure `key: value` from a committed ncu summary under profiles/
+    whose name starts with `prefix`."""
     d = os.path.join(ROOT, "profiles")
     try:
         names = sorted(os.listdir(d))
