@@ -74,10 +74,10 @@ _SIGS = {
         _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "atb_gaussian_rows": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
-        _c_i64, _vp]),
+        _c_i64, ctypes.c_int, _vp]),
     "atb_gaussian_cols": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
-        ctypes.c_int, _vp, _c_i64, _c_i64, _vp]),
+        ctypes.c_int, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
     "atb_zoom_linear": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, _c_i64, ctypes.c_int,
         ctypes.c_int, _vp]),

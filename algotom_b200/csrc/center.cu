@@ -9,7 +9,9 @@
 //   x[i] w0 + sum_j (x[i+j] + x[i-j]) w_j, left to right in FP64 with
 //   explicitly rounded operations (no contraction), half-sample symmetric
 //   extension, then rounded to float32: the same operations in the same
-//   order as scipy's correlate1d, hence the same float32 results.
+//   order as scipy's correlate1d, hence the same float32 results.  For an
+//   integer input array scipy stores each pass truncated toward zero; the
+//   to_int flag does the same, on the same FP64 sums.
 // - atb_gaussian_cols: the same filter down the columns of a batch of
 //   images (gaussian_filter1d along axis 1 of a [n, rows, cols] stack; the
 //   first pass of gaussian_filter(projections, (0, sigma, sigma)) in
@@ -44,6 +46,12 @@ constexpr int kMetricThreads = 256;
 constexpr int kMetricBlocks = 256;   // partial sums per image (sharpness)
 static_assert(kMetricThreads == 256, "one thread per histogram bin");
 
+// a filtered sample as stored: float32, or (to_int) truncated toward zero
+// as scipy stores a filter's output for an integer input array
+__device__ __forceinline__ float gauss_out(double v, int to_int) {
+  return to_int ? (float)trunc(v) : __double2float_rn(v);
+}
+
 __device__ __forceinline__ int reflect_index(long long i, int n) {
   if (i >= 0 && i < n) return (int)i;  // inside: no 64-bit remainder
   const long long period = 2LL * n;
@@ -57,7 +65,8 @@ __device__ __forceinline__ int reflect_index(long long i, int n) {
 // read doubles from shared memory.
 __global__ void __launch_bounds__(kRowTile) gaussian_rows_kernel(const float *__restrict__ src, long long srs,
                                                                  int ncol, const double *__restrict__ w, int radius,
-                                                                 float *__restrict__ dst, long long drs) {
+                                                                 float *__restrict__ dst, long long drs,
+                                                                 int to_int) {
   extern __shared__ __align__(16) unsigned char smem[];
   double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
   double *xs = ws + radius + 1;                   // [kRowTile + 2 radius]
@@ -74,7 +83,7 @@ __global__ void __launch_bounds__(kRowTile) gaussian_rows_kernel(const float *__
   const double *xc = xs + radius + threadIdx.x;
   double acc = __dmul_rn(xc[0], ws[0]);
   for (int j = 1; j <= radius; ++j) acc = __dadd_rn(acc, __dmul_rn(__dadd_rn(xc[j], xc[-j]), ws[j]));
-  dst[row * drs + c] = __double2float_rn(acc);
+  dst[row * drs + c] = gauss_out(acc, to_int);
 }
 
 // Column pass: CTA (x, y, z) filters columns [32 x, 32 x + 32) of rows
@@ -86,7 +95,7 @@ template <typename S>
 __global__ void __launch_bounds__(kColThreads)
     gaussian_cols_kernel(const float *__restrict__ src, long long sis, long long srs, int nrow, int ncol,
                          const double *__restrict__ w, int radius, float *__restrict__ dst, long long dis,
-                         long long drs) {
+                         long long drs, int to_int) {
   extern __shared__ __align__(16) unsigned char smem[];
   double *ws = reinterpret_cast<double *>(smem);   // [radius + 1]
   S *xs = reinterpret_cast<S *>(ws + radius + 1);  // [kColRows + 2 radius][kColTile]
@@ -108,7 +117,7 @@ __global__ void __launch_bounds__(kColThreads)
     double acc = __dmul_rn((double)xc[0], ws[0]);
     for (int j = 1; j <= radius; ++j)
       acc = __dadd_rn(acc, __dmul_rn(__dadd_rn((double)xc[j * kColTile], (double)xc[-j * kColTile]), ws[j]));
-    out[r * drs + c] = __double2float_rn(acc);
+    out[r * drs + c] = gauss_out(acc, to_int);
   }
 }
 
@@ -161,7 +170,7 @@ __device__ __forceinline__ void window_filter(const float *xs, int stride, const
 template <int KR>
 __global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3 : 2)) gaussian_rows_win_kernel(
     const float *__restrict__ src, long long srs, long long nrow, int ncol, const double *__restrict__ w,
-    int radius, float *__restrict__ dst, long long drs) {
+    int radius, float *__restrict__ dst, long long drs, int to_int) {
   constexpr int kCols = kSegs * kWinOut;  // 64
   extern __shared__ __align__(16) unsigned char smem[];
   double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
@@ -186,7 +195,7 @@ __global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3
   double acc[kWinOut];
   window_filter<KR>(xs + lane * pitch + seg * kWinOut, 1, ws, radius, acc);
 #pragma unroll
-  for (int i = 0; i < kWinOut; ++i) ot[lane * (kCols + 1) + seg * kWinOut + i] = __double2float_rn(acc[i]);
+  for (int i = 0; i < kWinOut; ++i) ot[lane * (kCols + 1) + seg * kWinOut + i] = gauss_out(acc[i], to_int);
   __syncthreads();
   for (int e = tid; e < kLineTile * kCols; e += kLineTile * kSegs) {
     const int rr = e / kCols, cc = e - rr * kCols;
@@ -200,7 +209,7 @@ __global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3
 template <int KR>
 __global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3 : 2)) gaussian_cols_win_kernel(
     const float *__restrict__ src, long long sis, long long srs, int nrow, int ncol, const double *__restrict__ w,
-    int radius, float *__restrict__ dst, long long dis, long long drs) {
+    int radius, float *__restrict__ dst, long long dis, long long drs, int to_int) {
   constexpr int kRowsT = kSegs * kWinOut;  // 64
   extern __shared__ __align__(16) unsigned char smem[];
   double *ws = reinterpret_cast<double *>(smem);  // [radius + 1]
@@ -226,7 +235,7 @@ __global__ void __launch_bounds__(kLineTile * kSegs, KR <= 4 ? 4 : (KR <= 12 ? 3
   float *out = dst + blockIdx.z * dis;
 #pragma unroll
   for (int i = 0; i < kWinOut; ++i)
-    if (r0 + k0 + i < nrow) out[(long long)(r0 + k0 + i) * drs + c] = __double2float_rn(acc[i]);
+    if (r0 + k0 + i < nrow) out[(long long)(r0 + k0 + i) * drs + c] = gauss_out(acc[i], to_int);
 }
 
 struct ZoomAxis {
@@ -423,7 +432,7 @@ int metric_blocks(long long npix) {
 }  // namespace
 
 extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int nrow, int ncol, const double *weights,
-                                 int radius, float *dst, int64_t dst_row_stride, void *stream) {
+                                 int radius, float *dst, int64_t dst_row_stride, int to_int, void *stream) {
   if (!src || !dst || !weights) return atb::fail(ATB_EINVAL, "atb_gaussian_rows: null pointer");
   if (nrow < 1 || ncol < 1 || radius < 0)
     return atb::fail(ATB_EINVAL, "atb_gaussian_rows: bad shape nrow=%d ncol=%d radius=%d", nrow, ncol, radius);
@@ -441,7 +450,7 @@ extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int n
       int rc = atb::ensure_smem(kern, wsmem, "atb_gaussian_rows");
       if (rc != ATB_OK) return rc;
       kern<<<wgrid, kLineTile * kSegs, wsmem, st>>>(src, src_row_stride, nrow, ncol, weights, radius, dst,
-                                                    dst_row_stride);
+                                                    dst_row_stride, to_int);
       return atb::check_launch("atb_gaussian_rows");
     };
     if (radius <= 4) return launch(gaussian_rows_win_kernel<4>);
@@ -454,13 +463,13 @@ extern "C" int atb_gaussian_rows(const float *src, int64_t src_row_stride, int n
   if (rc != ATB_OK) return rc;
   dim3 grid(nrow, (ncol + kRowTile - 1) / kRowTile);
   gaussian_rows_kernel<<<grid, kRowTile, smem, st>>>(src, src_row_stride, ncol, weights, radius, dst,
-                                                      dst_row_stride);
+                                                      dst_row_stride, to_int);
   return atb::check_launch("atb_gaussian_rows");
 }
 
 extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64_t src_row_stride, int nimg,
                                  int nrow, int ncol, const double *weights, int radius, float *dst,
-                                 int64_t dst_img_stride, int64_t dst_row_stride, void *stream) {
+                                 int64_t dst_img_stride, int64_t dst_row_stride, int to_int, void *stream) {
   if (!src || !dst || !weights) return atb::fail(ATB_EINVAL, "atb_gaussian_cols: null pointer");
   if (nimg < 1 || nrow < 1 || ncol < 1 || radius < 0)
     return atb::fail(ATB_EINVAL, "atb_gaussian_cols: bad shape nimg=%d nrow=%d ncol=%d radius=%d", nimg, nrow,
@@ -485,7 +494,7 @@ extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64
       const float *s0 = src + z0 * src_img_stride;
       float *d0 = dst + z0 * dst_img_stride;
       kern<<<grid, kLineTile * kSegs, wsmem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol, weights, radius,
-                                                   d0, dst_img_stride, dst_row_stride);
+                                                   d0, dst_img_stride, dst_row_stride, to_int);
       rc = atb::check_launch("atb_gaussian_cols");
       if (rc != ATB_OK) return rc;
     }
@@ -508,11 +517,11 @@ extern "C" int atb_gaussian_cols(const float *src, int64_t src_img_stride, int64
     if (s64)
       gaussian_cols_kernel<double><<<grid, kColThreads, smem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol,
                                                                     weights, radius, d0, dst_img_stride,
-                                                                    dst_row_stride);
+                                                                    dst_row_stride, to_int);
     else
       gaussian_cols_kernel<float><<<grid, kColThreads, smem, st>>>(s0, src_img_stride, src_row_stride, nrow, ncol,
                                                                    weights, radius, d0, dst_img_stride,
-                                                                   dst_row_stride);
+                                                                   dst_row_stride, to_int);
     rc = atb::check_launch("atb_gaussian_cols");
     if (rc != ATB_OK) return rc;
   }

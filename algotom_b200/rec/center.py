@@ -43,15 +43,30 @@ def _gaussian_weights(sigma, truncate=4.0):
     return np.ascontiguousarray(phi[r:])
 
 
-def gaussian_filter_rows(x, sigma):
+def _integer_input(x):
+    """True when ``x`` (array, tensor or dataset) holds integers: scipy's
+    filters then store their output in that integer type, truncated toward
+    zero."""
+    dt = getattr(x, "dtype", None)
+    if isinstance(dt, torch.dtype):
+        return not (dt.is_floating_point or dt.is_complex or
+                    dt == torch.bool)
+    if dt is None:
+        dt = np.asarray(x).dtype
+    return np.dtype(dt).kind in "iu"
+
+
+def gaussian_filter_rows(x, sigma, to_int=False):
     """``scipy.ndimage.gaussian_filter1d(x, sigma, axis=1)`` of a 2-D float32
-    CUDA tensor (mode "reflect"); returns a new tensor."""
+    CUDA tensor (mode "reflect"); returns a new tensor.  ``to_int``: the
+    values are integer counts and the results are truncated toward zero, as
+    scipy's for an integer array."""
     w = _gaussian_weights(sigma)
     wd = torch.from_numpy(w).to(x.device)
     out = torch.empty(x.shape, dtype=torch.float32, device=x.device)
     nat.call("atb_gaussian_rows", x.data_ptr(), x.stride(0), x.shape[0],
              x.shape[1], wd.data_ptr(), len(w) - 1, out.data_ptr(),
-             out.stride(0), R._stream_ptr(x.device))
+             out.stride(0), int(bool(to_int)), R._stream_ptr(x.device))
     return out
 
 
@@ -216,7 +231,7 @@ def _prepare(sinogram, sigma, apply_log):
         t, _ = R._to_device(sinogram)
         if t.dim() != 2:
             raise ValueError("sinogram must be 2-D")
-        t = gaussian_filter_rows(t, sigma)
+        t = gaussian_filter_rows(t, sigma, _integer_input(sinogram))
         if apply_log:
             R._check_log_input(t)
     else:

@@ -36,7 +36,7 @@ import torch
 from .. import _native as nat
 from . import reconstruction as R
 from . import windows as win
-from .center import _gaussian_weights, slice_metrics
+from .center import _gaussian_weights, _integer_input, slice_metrics
 from .padding import pad_rows
 
 _WARN_FULL = ("!!! Applying logarithm is enabled but there are values <= 0.0"
@@ -451,19 +451,21 @@ def _fields(flat_field, dark_field, height0, width0, top, bot, left, right):
     return np.float32(dark), np.float32(flat_dark)
 
 
-def _gaussian_slab(x, wts, tmp, out):
+def _gaussian_slab(x, wts, tmp, out, to_int=False):
     """``gaussian_filter(x, (0, sigma, sigma))`` of a float32 CUDA slab
     [n, height, width] (last axis contiguous) into ``out``: down the
     columns into ``tmp``, then along the rows; float32 between the passes,
-    as scipy."""
+    as scipy.  ``to_int``: integer counts, each pass truncated toward zero
+    (scipy's result for an integer array)."""
     n, height, width = x.shape
     r = wts.numel() - 1
     st = R._stream_ptr(x.device)
+    ti = int(bool(to_int))
     nat.call("atb_gaussian_cols", x.data_ptr(), x.stride(0), x.stride(1), n,
              height, width, wts.data_ptr(), r, tmp.data_ptr(), tmp.stride(0),
-             tmp.stride(1), st)
+             tmp.stride(1), ti, st)
     nat.call("atb_gaussian_rows", tmp.data_ptr(), width, n * height, width,
-             wts.data_ptr(), r, out.data_ptr(), width, st)
+             wts.data_ptr(), r, out.data_ptr(), width, ti, st)
 
 
 def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
@@ -515,6 +517,7 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
     wts = None
     if sigma > 0:
         wts = torch.from_numpy(_gaussian_weights(sigma)).to(dev)
+        to_int = _integer_input(projections)
     acc = torch.zeros((nline, height, width), dtype=torch.float64,
                       device=dev)
     log2m = nat.call("atb_filter_log2m", int(width), int(pad))
@@ -557,7 +560,7 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
                 if code != nat.F32:  # counts to float32 first
                     _flat_log(raw, code, None, None, False, pre, nonpos[:1])
                     raw = pre
-                _gaussian_slab(raw, wts, tmp, pre)
+                _gaussian_slab(raw, wts, tmp, pre, to_int)
                 raw, code = pre, nat.F32
             for k in range(k0, k1):  # one warning counter per chunk
                 if raw is pre and not apply_log and dark is None:

@@ -266,10 +266,14 @@ int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems,
  *   weights   device float64 [radius + 1]: the half kernel w[0..radius] of
  *             the unit-sum sampled Gaussian, radius = int(4 sigma + 0.5)
  *   dst       must not overlap src; radius <= 8192, ncol <= 65535 * 256
+ *   to_int    nonzero: each output is truncated toward zero, the value scipy
+ *             stores when the input array has an integer dtype (the counts
+ *             are passed as exact float32 integers)
  */
 int atb_gaussian_rows(const float *src, int64_t src_row_stride, int nrow,
                       int ncol, const double *weights, int radius,
-                      float *dst, int64_t dst_row_stride, void *stream);
+                      float *dst, int64_t dst_row_stride, int to_int,
+                      void *stream);
 
 /*
  * The same filter down the columns of nimg float32 images
@@ -282,12 +286,13 @@ int atb_gaussian_rows(const float *src, int64_t src_row_stride, int nrow,
  *   weights   as atb_gaussian_rows; radius <= 700 (the strip with its halo
  *             fits in shared memory)
  *   dst       must not overlap src; nrow * row_stride < 2^31
+ *   to_int    as atb_gaussian_rows
  */
 int atb_gaussian_cols(const float *src, int64_t src_img_stride,
                       int64_t src_row_stride, int nimg, int nrow, int ncol,
                       const double *weights, int radius, float *dst,
                       int64_t dst_img_stride, int64_t dst_row_stride,
-                      void *stream);
+                      int to_int, void *stream);
 
 /*
  * scipy.ndimage.zoom(x, zoom, order=1, mode="nearest") of a float32 image

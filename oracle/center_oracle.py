@@ -51,7 +51,10 @@ def _reflect_index(i, n):
 
 
 def gaussian_filter_rows(x, sigma):
-    """``scipy.ndimage.gaussian_filter1d(x, sigma, axis=1)`` of 2-D float32."""
+    """``scipy.ndimage.gaussian_filter1d(x, sigma, axis=1)`` of 2-D float32,
+    or of an integer array: then the result has the input's integer type,
+    truncated toward zero (the C conversion scipy's correlate1d stores)."""
+    dtype = np.asarray(x).dtype
     x = np.asarray(x, dtype=np.float32).astype(np.float64)
     w = gaussian_weights(sigma)
     n = x.shape[1]
@@ -60,6 +63,8 @@ def gaussian_filter_rows(x, sigma):
     for j in range(1, len(w)):
         acc = acc + (x[:, _reflect_index(idx + j, n)] +
                      x[:, _reflect_index(idx - j, n)]) * w[j]
+    if dtype.kind in "iu":
+        return np.trunc(acc).astype(dtype)
     return acc.astype(np.float32)
 
 
@@ -152,9 +157,12 @@ def slice_metrics(sinogram, start, stop, step=1, metric="entropy",
     if len(centers) == 0:
         raise ValueError("Invalid searching parameters: (start, stop, step)="
                          "{}!!!".format((start, stop, step)))
-    sino = np.asarray(sinogram, dtype=np.float32)
+    sino = np.asarray(sinogram)
+    if sino.dtype.kind not in "iu":
+        sino = sino.astype(np.float32)
     if sigma > 0:
         sino = gaussian_filter_rows(sino, sigma)
+    sino = sino.astype(np.float32)
     if apply_log:
         sino = np.where(sino <= 0.0, np.float32(1.0), sino)
         sino = (-np.log(sino.astype(np.float64))).astype(np.float32)

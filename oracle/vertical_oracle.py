@@ -145,10 +145,14 @@ def vertical_reconstruction(projections, x_mat, y_mat, center, angles=None,
 def smooth_projections(projections, sigma):
     """``gaussian_filter(projections, (0, sigma, sigma))`` of float32
     projections: the height pass, then the width pass, float32 between them
-    (vertrec.py:1348-1349)."""
+    (vertrec.py:1348-1349).  Integer projections keep their type, each pass
+    truncated toward zero, as scipy's."""
     from .center_oracle import gaussian_filter_rows
-    out = np.empty(projections.shape, np.float32)
-    for n, p in enumerate(np.asarray(projections, np.float32)):
+    projections = np.asarray(projections)
+    dtype = projections.dtype if projections.dtype.kind in "iu" \
+        else np.dtype(np.float32)
+    out = np.empty(projections.shape, dtype)
+    for n, p in enumerate(projections.astype(dtype, copy=False)):
         tmp = gaussian_filter_rows(np.ascontiguousarray(p.T), sigma).T
         out[n] = gaussian_filter_rows(np.ascontiguousarray(tmp), sigma)
     return out
@@ -184,10 +188,12 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
     num_proj, height, width = projections.shape
     if angles is None:
         angles = np.deg2rad(np.linspace(0.0, 180.0, num_proj))
-    proj = np.asarray(projections, np.float32)
+    proj = np.asarray(projections)
+    if proj.dtype.kind not in "iu":
+        proj = proj.astype(np.float32)
     if sigma > 0:
         proj = smooth_projections(proj, sigma)
-    proj = proj.astype(np.float64)
+    proj = proj.astype(np.float32).astype(np.float64)
     if apply_log:
         proj = -np.log(np.where(proj <= 0.0, 1.0, proj))
     xs, ys = points_single_line(slice_index, alpha, width)

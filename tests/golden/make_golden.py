@@ -232,6 +232,15 @@ def make_center():
                apply_log=True, gpu=False, ncore=1, return_metric=True)
     out[_key("list", "log", "centers")] = cs
     out[_key("list", "log", "metrics")] = ms
+    # integer counts: scipy smooths them into the same integer type,
+    # truncated toward zero, before the -log
+    counts = np.uint16(trans * 40000.0)
+    out["counts"] = counts
+    out[_key("gauss", "u16", 2)] = ndi.gaussian_filter1d(counts, 2, axis=1)
+    cs, ms = f(counts.copy(), cen - 2, cen + 2, 1.0, angles=ang, sigma=2,
+               apply_log=True, gpu=False, ncore=1, return_metric=True)
+    out[_key("list", "u16", "centers")] = cs
+    out[_key("list", "u16", "metrics")] = ms
     # chosen centres of the two-pass search
     g = rec.find_center_based_slice_metric
     finds = {
@@ -374,6 +383,23 @@ def make_vcenter():
             bad, 32, 29.0, 34.0, step=1.0, sigma=0, metric="sharpness",
             **common)
     out["vc_log_metrics"] = ms
+    # integer counts: each smoothing pass is truncated toward zero.  (Not
+    # with apply_log=False and the "after" filter: the reference's CPU
+    # back-projector then interpolates the uint16 counts in uint16, and a
+    # negative difference wraps around -- slices of ~1e18.)
+    counts = np.uint16(trans * 40000.0)
+    out["counts"] = counts
+    for sg in (3, 1.5):
+        out[_key("smooth_u16", sg)] = ndi.gaussian_filter(counts,
+                                                          (0, sg, sg))
+    for name, kw in (("u16_entropy", dict()),
+                     ("u16_sharp_before_nolog",
+                      dict(metric="sharpness", apply_log=False, sigma=1.5,
+                           ramp_filter="before"))):
+        cs, ms = vrec.find_center_vertical_slice(
+            counts.copy(), 32, 28.0, 35.0, step=0.5, **kw, **common)
+        out[_key("vc", name, "centers")] = cs
+        out[_key("vc", name, "metrics")] = ms
     out["vc_log_warnings"] = np.array([str(w.message) for w in caught
                                        if "logarithm" in str(w.message)])
     out["vc_log_mutated"] = bad

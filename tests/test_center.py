@@ -103,6 +103,21 @@ def test_oracle_log_input(golden):
     assert np.max(np.abs(ms - ref) / np.abs(ref)) < METRIC_RTOL
 
 
+def test_oracle_integer_counts(golden):
+    """uint16 counts: scipy smooths them into uint16, truncated toward
+    zero, and the -log follows in float32."""
+    g = golden("center")
+    cen = float(g["center"])
+    got = C.gaussian_filter_rows(g["counts"], 2)
+    assert got.dtype == np.uint16
+    assert np.array_equal(got, g["gauss__u16__2"])
+    cs, ms = C.slice_metrics(g["counts"], cen - 2, cen + 2, 1.0,
+                             angles=g["angles"], apply_log=True, sigma=2)
+    ref = g["list__u16__metrics"]
+    assert np.array_equal(cs, g["list__u16__centers"])
+    assert np.max(np.abs(ms - ref) / np.abs(ref)) < METRIC_RTOL
+
+
 @pytest.mark.parametrize("name", sorted(FINDS))
 def test_oracle_find_center(golden, name):
     g = golden("center")
@@ -130,10 +145,12 @@ def test_empty_search_range_raises():
 def test_abi_argument_errors():
     lib = nat.load()
     one = 1
-    assert lib.atb_gaussian_rows(None, 8, 4, 8, None, 2, None, 8,
+    assert lib.atb_gaussian_rows(None, 8, 4, 8, None, 2, None, 8, 0,
                                  None) == -1
-    assert lib.atb_gaussian_rows(one, 8, 4, 8, one, 9000, 2, 8, None) == -3
-    assert lib.atb_gaussian_rows(one, 8, 4, 8, one, 2, one, 8, None) == -1
+    assert lib.atb_gaussian_rows(one, 8, 4, 8, one, 9000, 2, 8, 0,
+                                 None) == -3
+    assert lib.atb_gaussian_rows(one, 8, 4, 8, one, 2, one, 8, 1,
+                                 None) == -1
     assert lib.atb_zoom_linear(one, 8, 0, 8, 2, 8, 4, 4, None) == -1
     assert lib.atb_zoom_linear(one, 8, 4, 8, 2, 8, 70000, 4, None) == -3
     assert lib.atb_image_range(one, 8, 0, 8, one, one, None) == -1
@@ -161,6 +178,39 @@ def test_gaussian_rows_bit_exact(cuda, golden, sigma):
     assert np.array_equal(got, g["gauss__%s" % sigma])
     got = CC.gaussian_filter_rows(_dev(g["narrow"]), 2).cpu().numpy()
     assert np.array_equal(got, g["gauss__narrow__2"])
+
+
+@pytest.mark.gpu
+def test_gaussian_rows_integer_counts(cuda, golden):
+    """to_int: each result truncated toward zero, as scipy's uint16."""
+    from algotom_b200.rec import center as CC
+    g = golden("center")
+    x = _dev(g["counts"].astype(np.float32))
+    got = CC.gaussian_filter_rows(x, 2, to_int=True).cpu().numpy()
+    assert np.array_equal(got, g["gauss__u16__2"].astype(np.float32))
+    rng = np.random.default_rng(3)
+    for dt, lo, hi in ((np.uint16, 0, 65536), (np.int16, -3000, 3000)):
+        v = rng.integers(lo, hi, (9, 300)).astype(dt)
+        for sigma in (0.7, 3, 5):  # register windows and shared-memory taps
+            got = CC.gaussian_filter_rows(_dev(v.astype(np.float32)), sigma,
+                                          to_int=True).cpu().numpy()
+            assert np.array_equal(got, C.gaussian_filter_rows(v, sigma)
+                                  .astype(np.float32)), (dt, sigma)
+
+
+@pytest.mark.gpu
+def test_integer_sinogram_search_matches_reference(cuda, golden):
+    from algotom_b200.rec import reconstruction as R
+    g = golden("center")
+    cen = float(g["center"])
+    counts = g["counts"].copy()
+    cs, ms = R._find_center_based_slice_metric(
+        counts, cen - 2, cen + 2, 1.0, angles=g["angles"], sigma=2,
+        apply_log=True, return_metric=True)
+    ref = g["list__u16__metrics"]
+    assert np.array_equal(cs, g["list__u16__centers"])
+    assert np.max(np.abs(ms - ref) / np.abs(ref)) < METRIC_RTOL
+    assert np.array_equal(counts, g["counts"])
 
 
 @pytest.mark.gpu
