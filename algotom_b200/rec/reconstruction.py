@@ -151,14 +151,20 @@ def filter_sinograms(sino3, pad, pad_mode="edge", apply_log=False,
 
 
 def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
-                scale=1.0, out=None, kahan="chunk", trig=None, variant=0):
+                scale=1.0, out=None, kahan="chunk", trig=None, variant=0,
+                staging="tma"):
     """Device back-projection of [nrow, nslice, ncol] -> [ncol, nslice, ncol].
 
     ``sino3`` may be float32, float16 or bfloat16 (last axis contiguous).
     ``trig`` may hold the angle table from :func:`_trig` already on the
     device (saves its host-to-device copy per call).  ``variant`` selects
-    the single-slice tile variant (0: 64 x 64, 1: 32 x 32).
+    the single-slice tile variant (0: 64 x 64, 1: 32 x 32).  ``staging``:
+    "tma" stages the detector windows of 2- and 4-slice CTAs with TMA box
+    loads where the rows are 16-byte aligned, "cp.async" always with
+    cp.async; the results are the same.
     """
+    if staging not in ("tma", "cp.async"):
+        raise ValueError("staging must be 'tma' or 'cp.async'")
     nrow, nslice, ncol = sino3.shape
     dev = sino3.device
     code = {torch.float32: nat.F32, torch.float16: nat.F16,
@@ -172,8 +178,8 @@ def backproject(sino3, angles, center, edge_pad=False, mask_r2=-1.0,
              sino3.stride(1), nrow, nslice, ncol, trig.data_ptr(),
              float(np.float32(center)), int(bool(edge_pad)), float(mask_r2),
              float(scale), out.data_ptr(), out.stride(0), out.stride(1),
-             (1 if kahan == "angle" else 0) | (int(variant) << 2),
-             _stream_ptr(dev))
+             (1 if kahan == "angle" else 0) | (int(variant) << 2) |
+             (16 if staging == "cp.async" else 0), _stream_ptr(dev))
     return out
 
 

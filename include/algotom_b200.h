@@ -143,7 +143,10 @@ int atb_neg_log(const float *src, int64_t src_row_stride,
  *            path; edge_pad must be 0);
  *            bits 2-3: tile variant for single-slice launches: 0 = 64 x 64
  *            pixels on 256 threads, 1 = 32 x 32 on 128 threads (chosen by the
- *            autotuner; stacks of 2 or more slices always use 64 x 32 tiles)
+ *            autotuner; stacks of 2 or more slices always use 64 x 32 tiles);
+ *            bit 4: stage the detector windows with cp.async even where
+ *            TMA box loads are used by default (CTAs of 2 or 4 slices with a
+ *            16-byte aligned base, strides and row length); same results
  */
 int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int64_t sino_slice_stride, int nrow, int nslice, int ncol,
@@ -151,6 +154,15 @@ int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     double mask_r2, float scale, float *out,
                     int64_t out_row_stride, int64_t out_slice_stride,
                     int flags, void *stream);
+
+/*
+ * Status word of the back-projection kernels: bit 0 is set when a CTA gave
+ * up waiting (after about 70 ms) for a TMA window load and left its tile
+ * unwritten.  Returns the word (0 = no such event since the last reset) and
+ * clears it when reset != 0; negative on a CUDA error.  Synchronises with
+ * the device.
+ */
+int atb_backproject_status(int reset);
 
 /*
  * Forward (Radon) projection that is the exact adjoint of atb_backproject
