@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 # every symbol include/algotom_b200.h declares
 EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
-           "atb_backproject_status", "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
+           "atb_backproject_status", "atb_backproject_centers",
+           "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
            "atb_backproject_batch_noalloc", "atb_gaussian_rows",
            "atb_gaussian_cols", "atb_zoom_linear", "atb_image_range",
            "atb_slice_metric_workspace", "atb_slice_metric",
@@ -63,6 +64,10 @@ _SIGS = {
         ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
         ctypes.c_float, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
     "atb_backproject_status": (ctypes.c_int, [ctypes.c_int]),
+    "atb_backproject_centers": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_double,
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+        ctypes.c_float, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
     "atb_radon_adjoint": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
         ctypes.c_double, _vp, _c_i64, _c_i64, _vp]),

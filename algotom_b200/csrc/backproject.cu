@@ -108,6 +108,8 @@ struct BPArgs {
   long long ors, oss;
   int vec16;  // rows 16-byte aligned: stage by TMA (tma) or 16-byte cp.async
   int tma;    // the kernel's tensor map describes sino: stage windows by TMA
+  int spacing;  // centre-group launches: slice m is centre center + m spacing
+                // of the one sinogram (sss = 0)
   int slope;  // back-project the interpolant's slope D_j instead of its value
 };
 
@@ -314,7 +316,18 @@ struct BPCfg {
 // One CTA's work: the TX x TY pixel tile (bx, by) of the slice group bz.
 // Every thread of the CTA must call it (it synchronises).  tmem is the
 // base of the CTA's K::kTmemCols TMEM columns (chunked Kahan only).
-template <typename T, int S, bool kPerAngleKahan, int V = 0>
+// kGroup: the launch's slices are candidate centres center + m spacing of
+// ONE sinogram (a centre search).  Slice m at centre c + m spacing sees the
+// same local positions q as the CTA's first slice on a source row shifted
+// by m spacing bins, so a CTA stages one row segment covering all its
+// slices and builds each slice's pairs from it at that shift; the
+// accumulation is the stacked one.  Edge angles decide the detector range
+// per slice.
+__host__ __device__ constexpr int group_segment(int win, int s, int spacing, int vec) {
+  return ((win + (s - 1) * spacing + 3 * vec - 1) / vec) * vec;
+}
+
+template <typename T, int S, bool kPerAngleKahan, int V = 0, bool kGroup = false>
 __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz, unsigned char *smem,
                                         uint32_t tmem, const CUtensorMap *tmap) {
   using K = BPCfg<T, S, V>;
@@ -340,6 +353,11 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   const bool use_tma = a.tma != 0;
   const int ncol = a.ncol;
   const T *sino = reinterpret_cast<const T *>(a.sino) + slice0 * a.sss;
+  // centre-group launches: this CTA's first centre, the shift between its
+  // slices and the length of the row segment it stages
+  const int gsp = kGroup ? a.spacing : 0;
+  const double ctr = kGroup ? a.center + (double)slice0 * (double)gsp : a.center;
+  const int seglen = kGroup ? group_segment(kWin, S, gsp, K::kVecElems) : kRaw;
 
   // thread -> pixel offsets inside the tile: warp (wx, wy) covers
   // (8 PX) x (4 PY) pixels, lane (lx, ly) an 8 x 4 block replicated PX x PY
@@ -395,12 +413,15 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
       AngleParam p = {0.f, 0.f, 0.f, 0.f, 0.f, 0, 0.0, 0.0};
       if (i < a.nrow) {
         const double2 cs = a.trig[i];
-        const double P0 = ((double)x0 - ic) * cs.x + ((double)y0 - ic) * cs.y + a.center;
+        const double P0 = ((double)x0 - ic) * cs.x + ((double)y0 - ic) * cs.y + ctr;
         const double ec = (double)(TX - 1) * cs.x, es = (double)(TY - 1) * cs.y;
         // non-finite trig (rejected by the host) is skipped, never indexed
         if (isfinite(P0) && isfinite(ec) && isfinite(es)) {
           const double pmin = P0 + fmin(0.0, ec) + fmin(0.0, es);
           const double pmax = P0 + fmax(0.0, ec) + fmax(0.0, es);
+          // highest position of any slice (a centre group's last slice sits
+          // (S - 1) spacing bins further)
+          const double pmax_all = pmax + (double)((S - 1) * gsp);
           lo = (int)floor(pmin) - 1;
           p.qbase = (float)(P0 - (double)(lo + kHalf));
           p.c = (float)cs.x;
@@ -415,8 +436,8 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
             // slope mode is continuous (edges smoothed over one bin)
             if (pmin > (double)ncol + 1e-2 || pmax < -1.0 - 1e-2) flag = 1;
           } else if (!a.edge_pad) {
-            if (pmin > (double)(ncol - 1) + 1e-2 || pmax < -1e-2) flag = 1;
-            else if (pmin < 1e-2 || pmax > (double)(ncol - 1) - 1e-2) flag = 2;
+            if (pmin > (double)(ncol - 1) + 1e-2 || pmax_all < -1e-2) flag = 1;
+            else if (pmin < 1e-2 || pmax_all > (double)(ncol - 1) - 1e-2) flag = 2;
           }
         }
       }
@@ -454,8 +475,9 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
         const int lo = lo_s[buf][tid];
         const int base = (lo / kV - (lo % kV < 0)) * kV;  // a 16-byte multiple, as TMA requires
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&raw_bar[buf], (unsigned)K::kBoxBytes);
-        tma_load_3d(raw + ((size_t)buf * kChunk + tid) * K::kRawSlot, tmap, base, slice0, it, &raw_bar[buf]);
+        mbar_arrive_expect_tx(&raw_bar[buf], (unsigned)(kGroup ? seglen * (int)sizeof(T) : K::kBoxBytes));
+        tma_load_3d(raw + ((size_t)buf * kChunk + tid) * K::kRawSlot, tmap, base, kGroup ? 0 : slice0, it,
+                    &raw_bar[buf]);
       } else {
         mbar_arrive(&raw_bar[buf]);
       }
@@ -468,24 +490,27 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
       if (use_tma) {
         // the window arrives by TMA
       } else if (vec16) {
-        constexpr int kVec = kRaw / kV;
-        for (int idx = s_jl; idx < S * kVec; idx += kTPA) {
+        // rows of S slices, or a centre group's one row segment
+        const int kVec = seglen / kV, nrows = kGroup ? 1 : nsl;
+        for (int idx = s_jl; idx < (kGroup ? 1 : S) * kVec; idx += kTPA) {
           const int ks = idx / kVec, v = idx - ks * kVec;
           const int d = base + kV * v;
-          if (ks < nsl && d >= 0 && d < ncol)  // ncol % kV == 0: a vector is in or out
+          if (ks < nrows && d >= 0 && d < ncol)  // ncol % kV == 0: a vector is in or out
             cp_async16(rb + ks * kRaw + kV * v, src + ks * sss + d);
         }
       } else if constexpr (sizeof(T) == 4) {
-        for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
-          const int ks = idx / kRaw, v = idx - ks * kRaw;
+        const int nrows = kGroup ? 1 : nsl;
+        for (int idx = s_jl; idx < (kGroup ? 1 : S) * seglen; idx += kTPA) {
+          const int ks = idx / seglen, v = idx - ks * seglen;
           const int d = base + v;
-          if (ks < nsl && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
+          if (ks < nrows && d >= 0 && d < ncol) cp_async4(rb + ks * kRaw + v, src + ks * sss + d);
         }
       } else {
-        for (int idx = s_jl; idx < S * kRaw; idx += kTPA) {
-          const int ks = idx / kRaw, v = idx - ks * kRaw;
+        const int nrows = kGroup ? 1 : nsl;
+        for (int idx = s_jl; idx < (kGroup ? 1 : S) * seglen; idx += kTPA) {
+          const int ks = idx / seglen, v = idx - ks * seglen;
           const int d = base + v;
-          if (ks < nsl && d >= 0 && d < ncol) rb[ks * kRaw + v] = src[ks * sss + d];
+          if (ks < nrows && d >= 0 && d < ncol) rb[ks * kRaw + v] = src[ks * sss + d];
         }
       }
       if ((edge_pad || slope) && s_jl < nsl) {
@@ -506,27 +531,31 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     const int base = (lo / kV - (lo % kV < 0)) * kV;
     // every d and d+1 of the window inside [0, ncol-1] with d <= ncol-2
     // (slope mode: also clear of the smoothed edges at bins 0 and ncol-2)
-    const bool interior = slope ? (lo >= 1 && lo + kWin <= ncol1 - 1) : (lo >= 0 && lo + kWin <= ncol1);
+    const int span = (S - 1) * gsp;  // a centre group's last slice reads span bins further
+    const bool interior =
+        slope ? (lo >= 1 && lo + kWin <= ncol1 - 1) : (lo >= 0 && lo + kWin + span <= ncol1);
     const T *rb = raw + ((size_t)buf * kChunk + s_ai) * K::kRawSlot;
     // detector sample x (0 <= x <= ncol-1) of slice ks
     auto val = [&](int ks, int x) -> float {
       const int r = x - base;
-      if (r >= 0 && r < kRaw) return atb::to_float(rb[ks * kRaw + r]);
+      if (r >= 0 && r < seglen) return atb::to_float(rb[(kGroup ? 0 : ks * kRaw) + r]);
       return edge_s[buf][s_ai][ks][x == 0 ? 0 : 1];  // clamped edge sample
     };
 #pragma unroll 2
     for (int t = 0; t < kJPT; ++t) {
       const int j = s_jl + kTPA * t;
-      const int d = lo + j;
       const float jc = (float)(j - kHalf);
       float av[S], dv[S];
 #pragma unroll
       for (int ks = 0; ks < S; ++ks) {
+        // detector bin of window index j for slice ks (shifted in a group)
+        const int d = lo + j + ks * gsp;
         float v = 0.f, w = 0.f;
         if (ks < nsl) {
           if (interior) {
-            v = atb::to_float(rb[ks * kRaw + d - base]);
-            w = atb::to_float(rb[ks * kRaw + d + 1 - base]) - v;
+            const T *rk = rb + (kGroup ? 0 : ks * kRaw);
+            v = atb::to_float(rk[d - base]);
+            w = atb::to_float(rk[d + 1 - base]) - v;
           } else if (slope) {
             // derivative in p of the back-projected interpolant with its two
             // edge steps (+s[0] at p = 0, -s[ncol-1] at p = ncol-1) smoothed
@@ -633,6 +662,36 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
             int j = __float_as_int(tq) - kMagicBits;
             bool inr = true;
             bool moved = false;
+            if constexpr (kChecked && kGroup && S > 1 && !K::kHalfPairs) {
+              // centre group near a detector edge: each slice has its own
+              // range [0, ncol - 1] in window coordinates, shifted by its
+              // spacing, decided as for a single centre
+              const double xc = (double)(x0 + tx + 8 * c) - ic;
+              const double yc = (double)(y0 + ty + 4 * b) - ic;
+              float vv[S];
+#pragma unroll
+              for (int ks = 0; ks < S; ++ks) {
+                const int sh = ks * gsp;
+                const float dl = q - (p.qlo - (float)sh), dr = q - (p.qmax - (float)sh);
+                bool in = (dl >= 0.f) && (dr <= 0.f);
+                int jk = j;
+                if (fabsf(dl) < kEdgeTol || fabsf(dr) < kEdgeTol) {
+                  const double pe = __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)),
+                                              ctr + (double)sh);
+                  in = (pe >= 0.0) && (pe <= (double)(ncol - 1));
+                  jk = max(j, p.j0 - sh - kHalf);
+                }
+                const float4 pr = reinterpret_cast<const float4 *>(w)[(ks >> 1) * kWin + jk];
+                vv[ks] = in ? fmaf((ks & 1) ? pr.w : pr.z, q, (ks & 1) ? pr.y : pr.x) : 0.f;
+              }
+#pragma unroll
+              for (int g = 0; g < S / 2; ++g) {
+                unsigned long long acc = acc2[b][c][g];
+                asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc) : "l"(pack2(vv[2 * g], vv[2 * g + 1])));
+                acc2[b][c][g] = acc;
+              }
+              continue;
+            }
             if constexpr (kChecked) {
               const float dl = q - p.qlo, dr = q - p.qmax;
               inr = (dl >= 0.f) && (dr <= 0.f);
@@ -642,7 +701,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
                 const double xc = (double)(x0 + tx + 8 * c) - ic;
                 const double yc = (double)(y0 + ty + 4 * b) - ic;
                 const double pe =
-                    __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)), a.center);
+                    __dadd_rn(__dadd_rn(__dmul_rn(xc, p.c64), __dmul_rn(yc, p.s64)), ctr);
                 inr = (pe >= 0.0) && (pe <= (double)(ncol - 1));
                 moved = j < p.j0 - kHalf;
                 j = max(j, p.j0 - kHalf);
@@ -751,17 +810,17 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   }
 }
 
-template <typename T, int S, bool kPerAngleKahan, int V>
+template <typename T, int S, bool kPerAngleKahan, int V, bool kGroup = false>
 __global__ void __launch_bounds__(BPCfg<T, S, V>::kThreads, BPCfg<T, S, V>::kMinBlocks)
     bp_kernel(BPArgs a, const __grid_constant__ CUtensorMap tmap) {
   using K = BPCfg<T, S, V>;
   extern __shared__ __align__(16) unsigned char smem[];
   if constexpr (kPerAngleKahan) {
-    bp_tile<T, S, true, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0u, &tmap);
+    bp_tile<T, S, true, V, kGroup>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0u, &tmap);
   } else {
     __shared__ uint32_t tmem_slot;
     const uint32_t tmem = tmem_alloc_cta<K::kTmemCols>(&tmem_slot);
-    bp_tile<T, S, false, V>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, tmem, &tmap);
+    bp_tile<T, S, false, V, kGroup>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, tmem, &tmap);
     tmem_free_cta<K::kTmemCols>(tmem);
   }
 }
@@ -797,6 +856,7 @@ __global__ void __launch_bounds__(BPCfg<T, 1, V>::kThreads, BPCfg<T, 1, V>::kMin
     a.vec16 = sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(it.sino) % 16) == 0 &&
               it.sino_row_stride % 4 == 0 && it.ncol % 4 == 0;
     a.tma = 0;
+    a.spacing = 0;
     const int tiles_x = (it.ncol + K::TX - 1) / K::TX;
     bp_tile<T, 1, false, V>(a, tile % tiles_x, tile / tiles_x, 0, smem, tmem, nullptr);
   }
@@ -835,18 +895,23 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // The [nrow][nslice][ncol] sinogram array as a TMA tensor (bins, slices,
 // angles) whose box is one angle's windows of S slices; false when the
 // layout does not allow it (the kernel then stages with cp.async).
-template <typename T, int S, int V>
+template <typename T, int S, int V, bool kGroup>
 bool make_window_map(const BPArgs &a, CUtensorMap *map) {
   using K = BPCfg<T, S, V>;
   auto encode = tensor_map_encoder();
   if (!encode || !a.vec16) return false;
   const cuuint64_t es = sizeof(T);
-  // vec16: 16-byte aligned base and strides; a single slice takes the row
-  // length as its (unused) slice stride
-  const cuuint64_t dims[3] = {(cuuint64_t)a.ncol, (cuuint64_t)a.nslice, (cuuint64_t)a.nrow};
-  const cuuint64_t strides[2] = {a.nslice == 1 ? (cuuint64_t)a.ncol * es : (cuuint64_t)a.sss * es,
+  // vec16: 16-byte aligned base and strides; a single row per angle (one
+  // slice, or a centre group's one sinogram) takes the row length as its
+  // (unused) slice stride
+  const bool one_row = kGroup || a.nslice == 1;
+  const cuuint64_t dims[3] = {(cuuint64_t)a.ncol, one_row ? 1u : (cuuint64_t)a.nslice, (cuuint64_t)a.nrow};
+  const cuuint64_t strides[2] = {one_row ? (cuuint64_t)a.ncol * es : (cuuint64_t)a.sss * es,
                                  (cuuint64_t)a.srs * es};
-  const cuuint32_t box[3] = {(cuuint32_t)K::kRaw, (cuuint32_t)S, 1u};
+  // a centre group stages one row segment per angle
+  const cuuint32_t box[3] = {
+      (cuuint32_t)(kGroup ? group_segment(K::kWin, S, a.spacing, K::kVecElems) : K::kRaw),
+      kGroup ? 1u : (cuuint32_t)S, 1u};
   const cuuint32_t estr[3] = {1u, 1u, 1u};
   if (strides[0] % 16 || strides[1] % 16 || strides[0] == 0 || strides[1] == 0) return false;
   return encode(map, tma_type<T>(), 3, const_cast<void *>(a.sino), dims, strides, box, estr,
@@ -854,10 +919,10 @@ bool make_window_map(const BPArgs &a, CUtensorMap *map) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <typename T, int S, bool kPerAngleKahan, int V = 0>
+template <typename T, int S, bool kPerAngleKahan, int V = 0, bool kGroup = false>
 int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
   using K = BPCfg<T, S, V>;
-  auto fn = bp_kernel<T, S, kPerAngleKahan, V>;
+  auto fn = bp_kernel<T, S, kPerAngleKahan, V, kGroup>;
   const int rc = atb::ensure_smem(fn, K::kSmem, "atb_backproject", K::kThreads, kPerAngleKahan ? 0 : K::kTmemCols);
   if (rc != ATB_OK) return rc;
   CUtensorMap map;
@@ -865,7 +930,7 @@ int launch_bp(BPArgs a, int nslices, cudaStream_t st) {
   // TMA staging for 2- and 4-slice CTAs (a 4-slice stack of 2560 x 1801
   // measured 4 % faster); single-slice windows are small copies that TMA
   // does not speed up, so they keep cp.async
-  a.tma = a.tma && S >= 2 && make_window_map<T, S, V>(a, &map);
+  a.tma = a.tma && S >= 2 && make_window_map<T, S, V, kGroup>(a, &map);
   dim3 grid((a.ncol + K::TX - 1) / K::TX, (a.ncol + K::TY - 1) / K::TY, (nslices + S - 1) / S);
   fn<<<grid, K::kThreads, K::kSmem, st>>>(a, map);
   return atb::check_launch("atb_backproject");
@@ -913,6 +978,7 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride;
   a.slope = (flags >> 1) & 1;
   a.tma = !((flags >> 4) & 1);
+  a.spacing = 0;
   {
     const int ve = sino_dtype == ATB_F32 ? 4 : 8;  // elements per 16-byte vector
     a.vec16 = (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % ve == 0 &&
@@ -940,6 +1006,54 @@ extern "C" int atb_backproject_status(int reset) {
       return atb::fail(ATB_ECUDA, "atb_backproject_status: %s", cudaGetErrorString(cudaGetLastError()));
   }
   return v;
+}
+
+extern "C" int atb_backproject_centers(const float *sino, int64_t sino_row_stride, int nrow, int ncol,
+                                       const double *trig, double center, int spacing, int ncenter, int edge_pad,
+                                       double mask_r2, float scale, float *out, int64_t out_row_stride,
+                                       int64_t out_center_stride, int flags, void *stream) {
+  if (!sino || !trig || !out) return atb::fail(ATB_EINVAL, "atb_backproject_centers: null pointer");
+  if (nrow < 1 || ncol < 1 || ncenter < 1)
+    return atb::fail(ATB_EINVAL, "atb_backproject_centers: bad shape nrow=%d ncol=%d ncenter=%d", nrow, ncol,
+                     ncenter);
+  if (ncenter > 4 * 65535) return atb::fail(ATB_ERANGE, "atb_backproject_centers: ncenter=%d too large", ncenter);
+  if (ncol > (1 << 20)) return atb::fail(ATB_ERANGE, "atb_backproject_centers: ncol=%d too large", ncol);
+  // the staged row segment of a 4-centre CTA must fit its slot and a TMA box
+  using K4 = BPCfg<float, 4, 0>;
+  using K1 = BPCfg<float, 1, 0>;
+  if (spacing < 1 || group_segment(K4::kWin, 4, spacing, 4) > 256 ||
+      group_segment(K4::kWin, 4, spacing, 4) > K4::kRawSlot ||
+      group_segment(BPCfg<float, 2, 0>::kWin, 2, spacing, 4) > BPCfg<float, 2, 0>::kRawSlot ||
+      group_segment(K1::kWin, 1, spacing, 4) > K1::kRawSlot)
+    return atb::fail(ATB_ERANGE, "atb_backproject_centers: spacing=%d outside [1, 56]", spacing);
+  const double last = center + (double)(ncenter - 1) * (double)spacing;
+  if (!(center >= 0.0) || last >= (double)ncol)
+    return atb::fail(ATB_EINVAL, "atb_backproject_centers: centres %g..%g outside [0, %d)", center, last, ncol);
+  BPArgs a;
+  a.sino = sino; a.srs = sino_row_stride; a.sss = 0;
+  a.nrow = nrow; a.nslice = ncenter; a.ncol = ncol; a.slice_base = 0;
+  a.trig = reinterpret_cast<const double2 *>(trig);
+  a.center = center; a.edge_pad = edge_pad ? 1 : 0; a.mask_r2 = mask_r2; a.scale = scale;
+  a.out = out; a.ors = out_row_stride; a.oss = out_center_stride;
+  a.slope = 0;
+  a.tma = !((flags >> 4) & 1);
+  a.spacing = spacing;
+  a.vec16 = (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % 4 == 0 && ncol % 4 == 0;
+  cudaStream_t st = atb::as_stream(stream);
+  // four centres per CTA, then the remainder
+  const int n4 = (ncenter / 4) * 4;
+  int rc = ATB_OK;
+  if (n4 > 0) rc = launch_bp<float, 4, false, 0, true>(a, n4, st);
+  if (rc != ATB_OK) return rc;
+  const int rem = ncenter - n4;
+  if (rem == 0) return ATB_OK;
+  a.slice_base = n4;
+  if (rem >= 2) {
+    rc = launch_bp<float, 2, false, 0, true>(a, 2, st);
+    if (rc != ATB_OK || rem == 2) return rc;
+    a.slice_base = n4 + 2;
+  }
+  return launch_bp<float, 1, false, 0, true>(a, 1, st);
 }
 
 namespace {

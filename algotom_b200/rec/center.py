@@ -134,6 +134,36 @@ def _backproject_items(items, device, variant):
     return items_dev, units_dev, counter
 
 
+def _centre_groups(centers, max_classes=16, max_spacing=56):
+    """Split candidate centres into progressions whose float32 values differ
+    by whole pixels: ``[(r, R, c0, spacing, count)]`` where candidates
+    ``r, r + R, r + 2R, ...`` sit at exactly ``c0 + m * spacing``.  None
+    when no ``R <= max_classes`` splits them so (e.g. irregular centres).
+    Such candidates share one back-projection (``atb_backproject_centers``):
+    a centre one pixel further reads the same positions one detector bin
+    further."""
+    c = np.float32(np.asarray(centers, dtype=np.float64)).astype(np.float64)
+    n = len(c)
+    if n < 2:
+        return None
+    for nclass in range(1, min(max_classes, n) + 1):
+        groups = []
+        for r in range(nclass):
+            cls = c[r::nclass]
+            d = np.diff(cls)
+            if len(d) == 0:
+                groups.append((r, nclass, float(cls[0]), 1, 1))
+                continue
+            g = d[0]
+            if not (g == np.round(g) and 1 <= g <= max_spacing and
+                    np.all(d == g)):
+                break
+            groups.append((r, nclass, float(cls[0]), int(g), len(cls)))
+        else:
+            return groups
+    return None
+
+
 class _Source:
     """The sinogram of one search, prepared once for every candidate: the
     ramp-filtered rows for FBP, the -log rows for BPF."""
@@ -175,8 +205,22 @@ class _Source:
                           device=dev)
         scale = R._scale(nrow)
         fbp = self.method == "fbp"
+        keep = None
+        masks = {R._mask_r2(ratio, float(c), ncol) if fbp else -1.0
+                 for c in centers}
+        groups = _centre_groups(centers) if len(masks) == 1 else None
+        if groups is not None:
+            # candidates a whole number of pixels apart: 4 per CTA
+            mask_r2 = masks.pop()
+            st = R._stream_ptr(dev)
+            for r, ncls, c0, g, cnt in groups:
+                nat.call("atb_backproject_centers", self.src.data_ptr(),
+                         self.src_rs, nrow, ncol, self.trig.data_ptr(), c0,
+                         g, cnt, 0 if fbp else 1, mask_r2,
+                         scale if fbp else 1.0, out[r].data_ptr(),
+                         out.stride(1), ncls * out.stride(0), 0, st)
         items = []
-        for k, c in enumerate(centers):
+        for k, c in enumerate([] if groups is not None else centers):
             it = nat.BpItem()
             it.sino, it.sino_row_stride = self.src.data_ptr(), self.src_rs
             it.trig = self.trig.data_ptr()
@@ -189,7 +233,8 @@ class _Source:
             else:
                 it.mask_r2, it.scale, it.edge_pad = -1.0, 1.0, 1
             items.append(it)
-        keep = _backproject_items(items, dev, 1 if ncol <= 512 else 0)
+        if items:
+            keep = _backproject_items(items, dev, 1 if ncol <= 512 else 0)
         if not fbp:
             out = R._circular_filter(out, None, self.filter_name, self.pad,
                                      "edge")

@@ -156,6 +156,35 @@ int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int flags, void *stream);
 
 /*
+ * Back-projection of ONE sinogram at ncenter rotation centres
+ * center + m * spacing (m = 0 .. ncenter-1, spacing a whole number of
+ * pixels); replaces the per-candidate reconstructions of a centre search
+ * (_find_center_based_slice_metric, reconstruction.py:1254-1346, through
+ * _reconstruct_slice, :1177-1208) for candidates whose float32 centres
+ * differ by whole pixels.  Image m equals atb_backproject of the sinogram
+ * at centre center + m * spacing (same positions, pairs and edge decisions;
+ * only the grouping of the FP32 partial sums differs).  Centres at a
+ * non-integer step, e.g. 0.25, form one such progression per residue:
+ * call once per residue with out offset by the residue's image.
+ *
+ *   sino      float32 [nrow][ncol] at sino_row_stride
+ *   trig, edge_pad, scale, flags (bit 4)   as atb_backproject
+ *   center    the float32-rounded first centre, as a double; every centre
+ *             center + m * spacing must lie in [0, ncol)
+ *   spacing   1 .. 56
+ *   mask_r2   as atb_backproject, the same for every centre
+ *   out       float32 image m at out + m * out_center_stride, rows
+ *             out_row_stride apart
+ */
+int atb_backproject_centers(const float *sino, int64_t sino_row_stride,
+                            int nrow, int ncol, const double *trig,
+                            double center, int spacing, int ncenter,
+                            int edge_pad, double mask_r2, float scale,
+                            float *out, int64_t out_row_stride,
+                            int64_t out_center_stride, int flags,
+                            void *stream);
+
+/*
  * Status word of the back-projection kernels: bit 0 is set when a CTA gave
  * up waiting (after about 70 ms) for a TMA window load and left its tile
  * unwritten.  Returns the word (0 = no such event since the last reset) and

@@ -213,6 +213,73 @@ def test_integer_sinogram_search_matches_reference(cuda, golden):
     assert np.array_equal(counts, g["counts"])
 
 
+def test_centre_groups():
+    from algotom_b200.rec.center import _centre_groups
+    g = _centre_groups(np.arange(1270.3, 1278.3, 0.25))
+    assert len(g) == 4 and all(x[3] == 1 and x[4] == 8 for x in g)
+    assert [x[0] for x in g] == [0, 1, 2, 3]
+    assert _centre_groups(np.arange(40.0, 50.0, 1.0)) == [(0, 1, 40.0, 1, 10)]
+    g = _centre_groups(np.arange(40.0, 50.0, 0.3))  # 10 classes, 3 px apart
+    assert len(g) == 10 and all(x[3] == 3 for x in g)
+    for r, ncls, c0, sp, cnt in g:
+        c = np.float32(np.arange(40.0, 50.0, 0.3)[r::ncls])
+        assert np.array_equal(c.astype(np.float64), c0 + sp * np.arange(cnt))
+    assert _centre_groups([5.0]) is None
+    assert _centre_groups(np.linspace(10.0, 11.0, 40) ** 1.5) is None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ncol,nrow,c0,spacing,count,edge_pad,r2", [
+    (256, 181, 127.3, 1, 11, 0, 128.0 ** 2),   # 4 + 4 + 2 + 1 centres
+    (200, 91, 3.25, 2, 9, 0, -1.0),            # near the first edge, no mask
+    (200, 91, 160.5, 3, 13, 0, -1.0),          # last centres near ncol - 1
+    (256, 120, 100.75, 1, 8, 1, -1.0),         # BPF: edge padding
+    (96, 60, 10.0, 7, 12, 0, 48.0 ** 2)])
+def test_centre_group_equals_single_centres(cuda, ncol, nrow, c0, spacing,
+                                            count, edge_pad, r2):
+    """atb_backproject_centers image m equals the single-centre
+    back-projection at c0 + m * spacing (only the FP32 partial sums are
+    grouped differently), with TMA and cp.async staging identical."""
+    import torch
+    from algotom_b200 import _native as nat
+    from algotom_b200.rec import reconstruction as R
+    rng = np.random.default_rng(ncol + count)
+    s = rng.standard_normal((nrow, ncol)).astype(np.float32)
+    ang = np.concatenate([[0.0, np.pi / 2, np.pi / 4], rng.uniform(0, np.pi,
+                                                                   nrow)])
+    ang = ang[:nrow]
+    t = torch.from_numpy(s).to(cuda)
+    trig = R._trig(ang, t.device)
+    outs = []
+    for flags in (0, 16):
+        out = torch.full((count, ncol, ncol), np.nan, device=cuda)
+        nat.call("atb_backproject_centers", t.data_ptr(), t.stride(0), nrow,
+                 ncol, trig.data_ptr(), float(np.float32(c0)), spacing,
+                 count, edge_pad, r2, 0.5, out.data_ptr(), out.stride(1),
+                 out.stride(0), flags, R._stream_ptr(t.device))
+        outs.append(out)
+    assert torch.equal(outs[0], outs[1])
+    assert nat.call("atb_backproject_status", 0) == 0
+    for m in range(count):
+        c = float(np.float32(c0)) + m * spacing
+        one = R.backproject(t[:, None], ang, c, edge_pad=bool(edge_pad),
+                            mask_r2=r2, scale=0.5, trig=trig)[:, 0]
+        got = outs[0][m]
+        err = (got - one).abs().max().item()
+        assert err <= 1e-5 * one.abs().max().item(), (m, c, err)
+
+
+def test_centre_group_argument_errors():
+    """Rejected before any device work (the pointers are never read)."""
+    lib = nat.load()
+    args = (16, 64, 4, 64, 16)
+    tail = (0, -1.0, 1.0, 16, 64, 4096, 0, None)
+    assert lib.atb_backproject_centers(*args, 10.0, 57, 2, *tail) == -3
+    assert lib.atb_backproject_centers(*args, 10.0, 0, 2, *tail) == -3
+    assert lib.atb_backproject_centers(*args, 60.0, 2, 3, *tail) == -1
+    assert lib.atb_backproject_centers(*args, 10.0, 1, 0, *tail) == -1
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("z", [0.5, 0.8, 0.33])
 def test_zoom_bit_exact(cuda, golden, z):
