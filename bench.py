@@ -664,8 +664,9 @@ def run_center(args):
     """Centre search on one benchmark slice (1801 angles x 2560 det, centre
     1278.3): the entropy metric of 128 candidate centres at step 0.25
     through ``_find_center_based_slice_metric`` (Gaussian smoothing sigma 2,
-    one ramp filter, a batched back-projection of all candidates, device
-    metrics), from a device tensor (``value``) and from a host NumPy array
+    one ramp filter, the candidates back-projected four per CTA -- one
+    launch per residue class of centres 1 px apart -- device metrics),
+    from a device tensor (``value``) and from a host NumPy array
     (``e2e``); plus the two-pass ``find_center_based_slice_metric`` (coarse
     zoom 0.5, +/-16 px).  CPU baseline: the oracle port's reference-
     arithmetic FBP and the metric on 2 candidates (plus the normalisation
@@ -761,9 +762,24 @@ def run_center(args):
                         "true_center": CENTER},
         "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
         # per step: Gaussian rows, row filter, normalisation image
-        # (batched back-projection + 2 range kernels), candidates (batched
-        # back-projection, histogram, entropy)
-        "gpu_launches": 8 * args.steps}), flush=True)
+        # (batched back-projection + 2 range kernels), candidates (the
+        # centre-group back-projections, histogram, entropy)
+        "gpu_launches": (7 + _group_launches(CC, cs)) * args.steps}),
+        flush=True)
+
+
+def _group_launches(CC, centers):
+    """Back-projection launches of a centre search over ``centers``: per
+    residue class, 4-centre CTAs and then the 2- and 1-centre remainder
+    (one batched launch when the centres do not form such classes)."""
+    groups = CC._centre_groups(centers)
+    if groups is None:
+        return 1
+    n = 0
+    for _, _, _, _, cnt in groups:
+        rem = cnt % 4
+        n += int(cnt >= 4) + int(rem >= 2) + int(rem % 2)
+    return n
 
 
 def _profile_figure(prefix, key):
