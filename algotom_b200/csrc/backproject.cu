@@ -88,7 +88,7 @@ template <> struct Geo<1, 1> {
   static constexpr int PX = 2, PY = 4, WX = 2, WY = 2, kChunk = 32, kWin = 48, kThreads = 128, kMinBlocks = 4;
 };
 template <> struct Geo<2, 0> {
-  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 32, kWin = 80, kThreads = 256, kMinBlocks = 2;
+  static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 16, kWin = 80, kThreads = 256, kMinBlocks = 2;
 };
 template <> struct Geo<4, 0> {
   static constexpr int PX = 2, PY = 4, WX = 4, WY = 2, kChunk = 16, kWin = 80, kThreads = 256, kMinBlocks = 2;
@@ -303,8 +303,10 @@ struct BPCfg {
   // to a multiple of 128 bytes (TMA destinations are 128-byte aligned)
   static constexpr int kBoxBytes = S * kRaw * (int)sizeof(T);
   static constexpr int kRawSlot = ((kBoxBytes + 127) / 128) * 128 / (int)sizeof(T);
-  static constexpr size_t kRawSmem = 2 * (size_t)kChunk * kRawSlot * sizeof(T);
-  static constexpr size_t kSmem = kPairsSmem + kRawSmem + 128;  // + slack to align the raw region
+  // pairs double-buffered (one chunk accumulates while the next is built),
+  // raw windows single-buffered (consumed before the next chunk's arrive)
+  static constexpr size_t kRawSmem = (size_t)kChunk * kRawSlot * sizeof(T);
+  static constexpr size_t kSmem = 2 * kPairsSmem + kRawSmem + 128;  // + slack to align the raw region
   // compensated totals in TMEM: kAcc accumulators per thread, as (total,
   // compensation) cells in 2 kAcc columns; moved kXfer accumulators at a time
   static constexpr int kAcc = PX * G::PY * S;
@@ -336,14 +338,19 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   constexpr int kChunk = K::kChunk, kWin = K::kWin, kHalf = K::kHalf, kRaw = K::kRaw;
   constexpr int NP = (S + 1) / 2;  // packed accumulator words per pixel
 
-  unsigned char *pairs = smem;  // S == 1: [kChunk][kWin] float2; else [kChunk][S/2][kWin] float4
-  // [2][kChunk] slots of [S][kRaw], on a 128-byte boundary
-  T *raw = reinterpret_cast<T *>(smem + K::kPairsSmem + ((128u - (smem_u32(smem + K::kPairsSmem) & 127u)) & 127u));
-  __shared__ __align__(8) uint64_t raw_bar[2];  // TMA completion per raw buffer
-  __shared__ AngleParam prm[2][kChunk];
-  __shared__ int lo_s[2][kChunk];
-  __shared__ int flag_s[2][kChunk];  // bit 0: skip angle, bit 1: checked path
-  __shared__ float edge_s[2][kChunk][S][2];  // s[0], s[ncol-1] (edge padding)
+  // two buffers of pairs, S == 1: [kChunk][kWin] float2; else
+  // [kChunk][S/2][kWin] float4; chunk k uses buffer k & 1
+  unsigned char *pairs_buf = smem;
+  // [kChunk] slots of [S][kRaw] (one centre group row: [seglen]), on a
+  // 128-byte boundary
+  const unsigned raw_off = 2 * (unsigned)K::kPairsSmem;
+  T *raw = reinterpret_cast<T *>(smem + raw_off + ((128u - (smem_u32(smem + raw_off) & 127u)) & 127u));
+  __shared__ __align__(8) uint64_t raw_bar;  // TMA completion of the raw windows (phase k & 1: chunk k)
+  // per-angle parameters in three slots (chunk k: slot k % 3), so chunk
+  // k + 2's are written while chunk k accumulates and k + 1's are in use
+  __shared__ AngleParam prm[3][kChunk];
+  __shared__ int lo_s[3][kChunk];
+  __shared__ int flag_s[3][kChunk];  // bit 0: skip angle, bit 1: checked path
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -457,8 +464,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   const long long srs = a.srs, sss = a.sss;
   const bool edge_pad = a.edge_pad, slope = a.slope, vec16 = a.vec16;
   if (use_tma && tid == 0) {  // one arrival per angle of a chunk
-    mbar_init(&raw_bar[0], kChunk);
-    mbar_init(&raw_bar[1], kChunk);
+    mbar_init(&raw_bar, kChunk);
     mbar_init_fence();
   }
 
@@ -475,18 +481,17 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
         const int lo = lo_s[buf][tid];
         const int base = (lo / kV - (lo % kV < 0)) * kV;  // a 16-byte multiple, as TMA requires
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&raw_bar[buf], (unsigned)(kGroup ? seglen * (int)sizeof(T) : K::kBoxBytes));
-        tma_load_3d(raw + ((size_t)buf * kChunk + tid) * K::kRawSlot, tmap, base, kGroup ? 0 : slice0, it,
-                    &raw_bar[buf]);
+        mbar_arrive_expect_tx(&raw_bar, (unsigned)(kGroup ? seglen * (int)sizeof(T) : K::kBoxBytes));
+        tma_load_3d(raw + (size_t)tid * K::kRawSlot, tmap, base, kGroup ? 0 : slice0, it, &raw_bar);
       } else {
-        mbar_arrive(&raw_bar[buf]);
+        mbar_arrive(&raw_bar);
       }
     }
     const int i = k * kChunk + s_ai;
     if (i < a.nrow && !(flag_s[buf][s_ai] & 1)) {
       const int base = (lo_s[buf][s_ai] / kV - (lo_s[buf][s_ai] % kV < 0)) * kV;  // floor to a vector
       const T *src = sino + i * srs;
-      T *rb = raw + ((size_t)buf * kChunk + s_ai) * K::kRawSlot;
+      T *rb = raw + (size_t)s_ai * K::kRawSlot;
       if (use_tma) {
         // the window arrives by TMA
       } else if (vec16) {
@@ -513,17 +518,14 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
           if (ks < nrows && d >= 0 && d < ncol) rb[ks * kRaw + v] = src[ks * sss + d];
         }
       }
-      if ((edge_pad || slope) && s_jl < nsl) {
-        edge_s[buf][s_ai][s_jl][0] = atb::load_as_float(src + s_jl * sss);
-        edge_s[buf][s_ai][s_jl][1] = atb::load_as_float(src + s_jl * sss + ncol1);
-      }
     }
     cp_async_commit();
   };
 
   // chunk k's windows -> interpolation pairs (skipped angles are left as
   // they are: the accumulation never reads them)
-  auto make_pairs = [&](int k, int buf) {
+  auto make_pairs = [&](int k, int buf, int pb) {
+    unsigned char *pairs = pairs_buf + (size_t)pb * K::kPairsSmem;
     const int i = k * kChunk + s_ai;
     if (i >= a.nrow || (flag_s[buf][s_ai] & 1)) return;
     const int lo = lo_s[buf][s_ai];
@@ -534,12 +536,13 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     const int span = (S - 1) * gsp;  // a centre group's last slice reads span bins further
     const bool interior =
         slope ? (lo >= 1 && lo + kWin <= ncol1 - 1) : (lo >= 0 && lo + kWin + span <= ncol1);
-    const T *rb = raw + ((size_t)buf * kChunk + s_ai) * K::kRawSlot;
+    const T *rb = raw + (size_t)s_ai * K::kRawSlot;
+    const T *src = sino + i * srs;  // this angle's rows (edge samples)
     // detector sample x (0 <= x <= ncol-1) of slice ks
     auto val = [&](int ks, int x) -> float {
       const int r = x - base;
       if (r >= 0 && r < seglen) return atb::to_float(rb[(kGroup ? 0 : ks * kRaw) + r]);
-      return edge_s[buf][s_ai][ks][x == 0 ? 0 : 1];  // clamped edge sample
+      return atb::load_as_float(src + ks * sss + (x == 0 ? 0 : ncol1));  // clamped edge sample
     };
 #pragma unroll 2
     for (int t = 0; t < kJPT; ++t) {
@@ -615,30 +618,27 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     }
   };
 
+  // Prologue: chunk 0's windows and pairs, chunk 1's parameters and windows
+  // in flight.  Then per chunk k: accumulate k from pairs buffer k & 1;
+  // wait for k + 1's windows; write k + 2's parameters; build k + 1's
+  // pairs into the other buffer; one barrier; request k + 2's windows.
+  // (cp.async staging adds a barrier after its wait: other threads' copies.)
   params(0, 0);
   __syncthreads();
   issue_raw(0, 0);
+  bool late = false;
+  if (use_tma) late = !mbar_wait(&raw_bar, 0u);
+  else cp_async_wait_all();
+  __syncthreads();
+  if (nchunk > 1) params(1, 1);
+  make_pairs(0, 0, 0);
+  bool stalled = __syncthreads_or(late);  // pairs(0), params(1) visible; raw free
+  int pending = 0;                          // chunk whose windows are awaited
+  if (!stalled && nchunk > 1) issue_raw(1, 1);
 
-  bool stalled = false;
-  for (int k = 0; k < nchunk; ++k) {
-    const int buf = k & 1, nbuf = buf ^ 1;
-    bool late = false;
-    if (use_tma) late = !mbar_wait(&raw_bar[buf], (unsigned)((k >> 1) & 1));
-    else cp_async_wait_all();
-    // raw(k) landed; pairs(k-1) and params(k-1) no longer read
-    if (__syncthreads_or(late)) {
-      // a window load never completed: record it, give that copy one more
-      // bounded wait, and leave without writing this tile
-      if (tid == 0) atomicOr(&g_bp_status, 1);
-      mbar_wait(&raw_bar[buf], (unsigned)((k >> 1) & 1));
-      stalled = true;
-      break;
-    }
-    if (k + 1 < nchunk) params(k + 1, nbuf);
-    make_pairs(k, buf);
-    __syncthreads();  // pairs(k) and params(k+1) visible
-    if (k + 1 < nchunk) issue_raw(k + 1, nbuf);
-
+  for (int k = 0; k < nchunk && !stalled; ++k) {
+    const int buf = k % 3;
+    const unsigned char *pairs = pairs_buf + (size_t)(k & 1) * K::kPairsSmem;
     // accumulate chunk k
     const int nang = min(kChunk, a.nrow - k * kChunk);
     for (int ai = 0; ai < nang; ++ai) {
@@ -767,8 +767,33 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
           for (int g = 0; g < NP; ++g) acc2[b][c][g] = 0ull;
         }
     }
+
+    // chunk k + 1: its windows, k + 2's parameters, k + 1's pairs
+    if (k + 1 < nchunk) {
+      late = false;
+      if (use_tma) {
+        late = !mbar_wait(&raw_bar, (unsigned)((k + 1) & 1));
+      } else {
+        cp_async_wait_all();
+        __syncthreads();  // every thread's copies landed
+      }
+      if (k + 2 < nchunk) params(k + 2, (k + 2) % 3);
+      make_pairs(k + 1, (k + 1) % 3, (k + 1) & 1);
+      if (__syncthreads_or(late)) {  // pairs(k + 1), params(k + 2) visible; raw free
+        pending = k + 1;
+        stalled = true;
+        break;
+      }
+      if (k + 2 < nchunk) issue_raw(k + 2, (k + 2) % 3);
+    }
   }
-  if (stalled) return;  // CTA-uniform
+  if (stalled) {  // CTA-uniform; only TMA waits run out
+    // a window load never completed: record it, give that copy one more
+    // bounded wait, and leave without writing this tile
+    if (tid == 0) atomicOr(&g_bp_status, 1);
+    mbar_wait(&raw_bar, (unsigned)(pending & 1));
+    return;
+  }
   if constexpr (!kPerAngleKahan) {
     __syncwarp();
 #pragma unroll
