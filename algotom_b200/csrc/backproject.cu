@@ -23,8 +23,10 @@
 // add.rn.f32x2 update two slices, and the position, floor and address work
 // is shared by all S slices.
 //
-// Staging is double-buffered: while a chunk is being accumulated, the raw
-// detector windows of the next chunk stream into shared memory.  For CTAs
+// Staging is pipelined: while chunk k accumulates from one of two pairs
+// buffers, chunk k + 1's raw detector windows stream into shared memory;
+// then k + 1's pairs are built into the other buffer, and after one CTA
+// barrier k + 2's windows are requested into the single raw buffer.  For CTAs
 // of 2 or 4 slices whose rows are 16-byte aligned, each angle's window of
 // all S slices is one TMA box load (cp.async.bulk.tensor.3d over the
 // [angle][slice][bin] array, zero fill outside it) issued by one thread per
