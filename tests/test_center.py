@@ -213,6 +213,21 @@ def test_integer_sinogram_search_matches_reference(cuda, golden):
     assert np.array_equal(counts, g["counts"])
 
 
+def test_integer_input_detection():
+    """Which inputs scipy's filters would store as integers."""
+    import torch
+    from algotom_b200.rec.center import _integer_input
+    assert _integer_input(np.zeros(3, np.uint16))
+    assert _integer_input(np.zeros(3, np.int32))
+    assert _integer_input([1, 2, 3])
+    assert not _integer_input(np.zeros(3, np.float32))
+    assert not _integer_input([1.0, 2.0])
+    assert _integer_input(torch.zeros(3, dtype=torch.int16))
+    assert not _integer_input(torch.zeros(3))
+    assert not _integer_input(torch.zeros(3, dtype=torch.bool))
+    assert not _integer_input(torch.zeros(3, dtype=torch.complex64))
+
+
 def test_centre_groups():
     from algotom_b200.rec.center import _centre_groups
     g = _centre_groups(np.arange(1270.3, 1278.3, 0.25))
