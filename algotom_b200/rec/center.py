@@ -8,10 +8,12 @@ signatures, defaults, errors, warnings and results.
 The reference reconstructs the slice once per candidate centre, each time
 filtering the sinogram again, and evaluates the metric on the host.  Here
 the ramp filter (independent of the centre) runs once; the candidates are
-then back-projected by ONE persistent batched launch whose work items share
-the filtered sinogram and differ only in their centre
-(``atb_backproject_batch``), and the metric of every candidate image is
-computed on the device (``atb_slice_metric``).  The pre-steps -- Gaussian
+then back-projected together: candidates whose float32 centres lie a whole
+number of pixels apart share a 4-centre CTA (``atb_backproject_centers``,
+one launch per residue class of the progression), others go to ONE
+persistent batched launch whose work items share the filtered sinogram and
+differ only in their centre (``atb_backproject_batch``).  The metric of
+every candidate image is computed on the device (``atb_slice_metric``).  The pre-steps -- Gaussian
 smoothing along the detector and the linear zoom of the coarse pass -- are
 device kernels with scipy's float32 results (``atb_gaussian_rows``,
 ``atb_zoom_linear``).  Only the per-candidate metric values (8 bytes each)
