@@ -284,6 +284,44 @@ def test_centre_group_equals_single_centres(cuda, ncol, nrow, c0, spacing,
         assert err <= 1e-5 * one.abs().max().item(), (m, c, err)
 
 
+def test_centre_group_launch_plan(monkeypatch):
+    """The host's calls for a search at step 0.25: one
+    atb_backproject_centers per residue class, each writing every fourth
+    image (first image r, image stride 4 images) at float32 centres 1 px
+    apart; ratio=0.0 (a mask per centre) falls back to the batch path."""
+    import torch
+    from algotom_b200.rec import center as CC
+    from algotom_b200.rec import reconstruction as R
+    calls = []
+    monkeypatch.setattr(CC.nat, "call", lambda name, *a: calls.append(
+        (name, a)) or 1)
+    monkeypatch.setattr(R, "_stream_ptr", lambda dev=None: 0)
+    monkeypatch.setattr(CC, "_backproject_items",
+                        lambda items, dev, v: calls.append(
+                            ("batch", len(items))))
+    ncol, nrow = 64, 30
+    src = CC._Source.__new__(CC._Source)
+    src.method, src.nrow, src.ncol = "fbp", nrow, ncol
+    src.sino = torch.zeros((nrow, ncol))
+    src.angles = np.linspace(0.0, np.pi, nrow)
+    src.src, src.src_rs = torch.zeros((nrow, 1, ncol)), ncol
+    src.trig = torch.zeros((nrow, 2), dtype=torch.float64)
+    cs = np.arange(30.3, 32.3, 0.25)   # 8 candidates, 4 classes of 2
+    out = src.reconstruct(cs, 1.0)
+    assert out.shape == (8, ncol, ncol)
+    assert [c[0] for c in calls] == ["atb_backproject_centers"] * 4
+    esize = out.element_size()
+    for r, (_, a) in enumerate(calls):
+        assert a[5] == float(np.float32(cs[r]))       # first centre
+        assert a[6] == 1 and a[7] == 2                  # spacing, count
+        assert a[8] == 0 and a[10] == R._scale(nrow)    # FBP: no edge pad
+        assert (a[11] - out.data_ptr()) == r * ncol * ncol * esize
+        assert a[12] == ncol and a[13] == 4 * ncol * ncol
+    calls.clear()
+    src.reconstruct(cs, 0.0)                            # mask per centre
+    assert calls == [("batch", 8)]
+
+
 def test_centre_group_argument_errors():
     """Rejected before any device work (the pointers are never read)."""
     lib = nat.load()
