@@ -151,6 +151,26 @@ def test_abi_argument_errors():
     assert b"atb_slice_entropy64" in lib.atb_last_error()
 
 
+def test_gaussian_slab_passes_truncation_flag(monkeypatch):
+    """Both passes get to_int (the argument before the stream)."""
+    import torch
+    from algotom_b200.rec import vertrec as VR
+    calls = []
+    monkeypatch.setattr(VR.nat, "call", lambda name, *a: calls.append(
+        (name, a)))
+    monkeypatch.setattr(VR.R, "_stream_ptr", lambda dev=None: 0)
+    x = torch.zeros((2, 5, 7))
+    w = torch.zeros(4, dtype=torch.float64)
+    for flag in (False, True):
+        calls.clear()
+        VR._gaussian_slab(x, w, torch.empty_like(x), torch.empty_like(x),
+                          to_int=flag)
+        assert [c[0] for c in calls] == ["atb_gaussian_cols",
+                                         "atb_gaussian_rows"]
+        assert all(c[1][-2] == int(flag) for c in calls)
+        assert calls[0][1][3:6] == (2, 5, 7) and calls[0][1][7] == 3
+
+
 def test_metric_argument_error():
     from algotom_b200.rec import vertrec as VR
     with pytest.raises(ValueError, match="Please select one of three"):
