@@ -799,8 +799,12 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
     at every centre of ``np.arange(start, stop + step, step)``;
     ``vertrec.py:1264-1383``.
 
-    The projections are smoothed (``sigma``) and ``-log``-ed on the device
-    chunk by chunk, and every candidate centre -- plus the mean centre that
+    The projections are smoothed (``sigma``; integer projections such as
+    uint16 counts truncated toward zero after each pass, as scipy stores
+    them) and ``-log``-ed on the device chunk by chunk.  Integer counts with
+    ``apply_log=False`` and the "after" filter are back-projected as float32;
+    the reference's CPU back-projector would interpolate them in the integer
+    type and wrap around.  Every candidate centre -- plus the mean centre that
     sets the entropy's normalisation -- is a line of the same vertical
     back-projection launch, so the data are read once for all of them
     (in passes of about 4 GB of FP64 slices when there are many).  Metrics:
