@@ -1317,6 +1317,19 @@ def run_dfi(args):
         "gpu_launches": 4 * args.steps}), flush=True)
 
 
+def _spawn_ranks(n):
+    """Re-run this command as n ranks (one process per GPU) under
+    torch.distributed.run on this node; returns its exit code."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(n), "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = _args()
     if args.workload == "dfi":
@@ -1349,9 +1362,14 @@ def main():
     if args.workload == "single":
         run_single(args)
         return
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(_spawn_ranks(args.gpus))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit("bench.py: --gpus %d but WORLD_SIZE=%d"
+                         % (args.gpus, world))
     if args.impl == "reference":
         run_reference(args, rank)
         return
