@@ -1174,6 +1174,14 @@ extern "C" int atb_backproject_batch(const atb_bp_item *items, int nitems, const
 // caller (item table, work list, counter).  The entry point below keeps them
 // instead in one file-scope __device__ array of fixed size, which every GPU
 // that loads this library holds until the process exits.
+//
+// Nothing of the call stays in host memory: the item table travels to the
+// device inside the parameters of small upload launches (each launch's
+// parameters are copied when it is enqueued), and the work list is built on
+// the device from that table, in the same longest-processing-time order as
+// atb_bp_batch_plan.  So the caller may reuse or free its host table as soon
+// as the call returns, and the call never waits for earlier work on the
+// stream (no copy from pageable host memory).
 namespace {
 
 constexpr int kNoAllocMaxItems = 4096;
@@ -1185,12 +1193,96 @@ constexpr size_t kNoAllocBytes = kNoAllocUnitsOffset + sizeof(int) * (size_t)kNo
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// host-side staging of the item table and work list (static: no heap use);
-// guarded by g_noalloc_mu together with the per-device scratch addresses
-atb_bp_item g_noalloc_items[kNoAllocMaxItems];
-int g_noalloc_order[kNoAllocMaxItems];
-int g_noalloc_units[kNoAllocMaxUnits];
+// items per upload launch: the chunk stays inside the 32764-byte kernel
+// parameter limit of sm_70 and later devices (CUDA 12.1 and later)
+constexpr int kNoAllocChunk = 440;
+struct NoAllocChunk {
+  int first, count;
+  atb_bp_item items[kNoAllocChunk];
+};
+static_assert(sizeof(NoAllocChunk) + sizeof(void *) <= 32764, "upload chunk exceeds the kernel parameter limit");
+
+__global__ void __launch_bounds__(256) noalloc_upload_kernel(const __grid_constant__ NoAllocChunk c,
+                                                             atb_bp_item *dst) {
+  for (int k = threadIdx.x; k < c.count; k += blockDim.x) dst[c.first + k] = c.items[k];
+}
+
+// Work list of the uploaded table: units[o_r + t] = item << 16 | t for the
+// item of rank r in (angle count descending, index ascending) order, o_r the
+// sum of the tile counts of the ranks before r; also zeroes the counter pair
+// (the array keeps the previous call's contents).  One CTA.
+__global__ void __launch_bounds__(1024) noalloc_plan_kernel(const atb_bp_item *items, int nitems, int *units,
+                                                            int *counter) {
+  __shared__ int key[kNoAllocMaxItems];   // angle counts, then tile counts by rank, then offsets
+  __shared__ int item_at[kNoAllocMaxItems];
+  __shared__ int warp_sum[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) {
+    counter[0] = 0;
+    counter[1] = 0;
+  }
+  for (int b = tid; b < nitems; b += nt) key[b] = items[b].nrow;
+  __syncthreads();
+  for (int b = tid; b < nitems; b += nt) {  // stable rank, largest angle count first
+    const int kb = key[b];
+    int r = 0;
+    for (int j = 0; j < nitems; ++j) {
+      const int kj = key[j];
+      r += (kj > kb) || (kj == kb && j < b);
+    }
+    item_at[r] = b;
+  }
+  __syncthreads();
+  int tiles[4];
+  int local = 0;
+  for (int q = 0; q < 4; ++q) {  // each thread owns ranks 4 tid .. 4 tid + 3
+    const int r = 4 * tid + q;
+    int t = 0;
+    if (r < nitems) {
+      const int tx = (items[item_at[r]].ncol + kBatchTile - 1) / kBatchTile;
+      t = tx * tx;
+    }
+    tiles[q] = t;
+    local += t;
+  }
+  // exclusive scan of the per-thread sums over the CTA
+  const int lane = tid & 31, warp = tid >> 5;
+  int incl = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < (nt >> 5) ? warp_sum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    warp_sum[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  int off = incl - local + (warp > 0 ? warp_sum[warp - 1] : 0);
+  for (int q = 0; q < 4; ++q) {
+    const int r = 4 * tid + q;
+    if (r < nitems) key[r] = off;
+    off += tiles[q];
+  }
+  __syncthreads();
+  for (int r = 0; r < nitems; ++r) {
+    const int b = item_at[r];
+    const int tx = (items[b].ncol + kBatchTile - 1) / kBatchTile;
+    const int o = key[r];
+    for (int t = tid; t < tx * tx; t += nt) units[o + t] = (int)(((unsigned)b << 16) | (unsigned)t);
+  }
+}
+
+// per-device address of g_noalloc_scratch, looked up once per device, and
+// the host-side upload chunk (static rather than on the caller's stack);
+// both guarded by g_noalloc_mu
 unsigned char *g_noalloc_dev[64] = {nullptr};
+NoAllocChunk g_noalloc_chunk;
 std::mutex g_noalloc_mu;
 
 }  // namespace
@@ -1208,8 +1300,6 @@ extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitem
       return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: item %d is incomplete", b);
     if (it.ncol > 16384)
       return atb::fail(ATB_ERANGE, "atb_backproject_batch_noalloc: item %d has ncol=%d > 16384", b, it.ncol);
-    if (!(it.center >= 0.0) || it.center >= (double)it.ncol)
-      return atb::fail(ATB_EINVAL, "atb_backproject_batch_noalloc: item %d centre outside [0, ncol)", b);
     const long long t = (it.ncol + kBatchTile - 1) / kBatchTile;
     nunits += t * t;
   }
@@ -1218,12 +1308,12 @@ extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitem
                      "atb_backproject_batch_noalloc: %lld tiles of 64 x 64 exceed the fixed limit of %d",
                      nunits, kNoAllocMaxUnits);
 
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= 64)
     return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: no usable current device");
-  if (!g_noalloc_dev[dev]) {  // first call on this device: host address of the scratch array
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_dev[dev]) {  // first call on this device: device address of the scratch array
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
@@ -1235,43 +1325,27 @@ extern "C" int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitem
   int *counter = reinterpret_cast<int *>(base);
   atb_bp_item *items_dev = reinterpret_cast<atb_bp_item *>(base + kNoAllocItemsOffset);
   int *units_dev = reinterpret_cast<int *>(base + kNoAllocUnitsOffset);
-
-  // work list in longest-processing-time order, as atb_bp_batch_plan
-  for (int b = 0; b < nitems; ++b) {
-    g_noalloc_items[b] = items[b];
-    g_noalloc_order[b] = b;
-  }
-  for (int x = 1; x < nitems; ++x) {
-    const int v = g_noalloc_order[x];
-    int y = x - 1;
-    while (y >= 0 && items[g_noalloc_order[y]].nrow < items[v].nrow) {
-      g_noalloc_order[y + 1] = g_noalloc_order[y];
-      --y;
-    }
-    g_noalloc_order[y + 1] = v;
-  }
-  int n = 0;
-  for (int q = 0; q < nitems; ++q) {
-    const int b = g_noalloc_order[q];
-    const int tx = (items[b].ncol + kBatchTile - 1) / kBatchTile;
-    for (int t = 0; t < tx * tx; ++t) g_noalloc_units[n++] = (int)(((unsigned)b << 16) | (unsigned)t);
-  }
-
   cudaStream_t st = atb::as_stream(stream);
-  // the array keeps the previous call's contents: the counter must start at 0
-  if ((e = cudaMemsetAsync(counter, 0, 2 * sizeof(int), st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(items_dev, g_noalloc_items, sizeof(atb_bp_item) * (size_t)nitems,
-                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(units_dev, g_noalloc_units, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, st)) !=
-          cudaSuccess)
-    return atb::fail(ATB_ECUDA, "atb_backproject_batch_noalloc: %s", cudaGetErrorString(e));
+
   using K = BPCfg<float, 1, 0>;
   const int rc =
       atb::ensure_smem(bp_batch_kernel<float, 0>, K::kSmem, "atb_backproject_batch_noalloc", K::kThreads, K::kTmemCols);
   if (rc != ATB_OK) return rc;
+  NoAllocChunk &chunk = g_noalloc_chunk;
+  for (int first = 0; first < nitems; first += kNoAllocChunk) {
+    chunk.first = first;
+    chunk.count = nitems - first < kNoAllocChunk ? nitems - first : kNoAllocChunk;
+    std::memcpy(chunk.items, items + first, sizeof(atb_bp_item) * (size_t)chunk.count);
+    noalloc_upload_kernel<<<1, 256, 0, st>>>(chunk, items_dev);
+    const int r = atb::check_launch("atb_backproject_batch_noalloc (item upload)");
+    if (r != ATB_OK) return r;
+  }
+  noalloc_plan_kernel<<<1, 1024, 0, st>>>(items_dev, nitems, units_dev, counter);
+  const int r = atb::check_launch("atb_backproject_batch_noalloc (work list)");
+  if (r != ATB_OK) return r;
   int grid = 2 * sm_count();
   if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
-  if (grid > n) grid = n;
-  bp_batch_kernel<float, 0><<<grid, K::kThreads, K::kSmem, st>>>(items_dev, units_dev, n, counter);
+  if (grid > nunits) grid = (int)nunits;
+  bp_batch_kernel<float, 0><<<grid, K::kThreads, K::kSmem, st>>>(items_dev, units_dev, (int)nunits, counter);
   return atb::check_launch("atb_backproject_batch_noalloc");
 }

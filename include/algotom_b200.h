@@ -276,7 +276,13 @@ int atb_backproject_batch(const atb_bp_item *items, int nitems,
  * of its own.  Takes the item table in HOST memory (device pointers inside)
  * and keeps the work list, item table and counter in a fixed __device__
  * array of this library (about 4.4 MB, held by every GPU that loads the
- * library until the process exits).  It allocates nothing.
+ * library until the process exits).  It allocates nothing.  The table is
+ * read during the call only: its entries travel to the device inside the
+ * parameters of the launches the call enqueues, and the work list is built
+ * on the device, so the caller may reuse or free the host table as soon as
+ * the call returns, and the call does not wait for earlier work on the
+ * stream.  Items are accepted as atb_backproject_batch accepts them (any
+ * centre).
  *
  *   items     host array [nitems], nitems <= 4096; ncol <= 16384 per item
  *   max_ctas  as atb_backproject_batch

@@ -4,8 +4,9 @@ atb_backproject_batch_noalloc serves callers that hold device buffers for
 their data but may not call cudaMalloc (e.g. a plugin whose host application
 owns the device memory budget).  It keeps its scratch in a fixed device
 array of the library.  This test drives it through the C ABI, twice in a
-row (the second call must not see the first call's leftovers), and compares
-its output with atb_backproject_batch, which takes caller-allocated scratch.
+row (the second call, with a smaller table, must not run the first call's
+leftover entries), and compares its output with atb_backproject_batch, which
+takes caller-allocated scratch.
 The file name keeps it last in collection order.
 """
 import ctypes
@@ -47,25 +48,52 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda):
     bf.launch()  # filter + atb_backproject_batch (caller-provided scratch)
     torch.cuda.synchronize()
     reference = [o.clone() for o in bf.outputs]
-
     stream = R._stream_ptr(cuda)
-    for call in range(2):
-        for o in bf.outputs:
-            o.fill_(float("nan"))
-        rc = nat.load().atb_backproject_batch_noalloc(
-            ctypes.addressof(bf.items_host), bf.n, 0, stream)
-        assert rc == 0, nat.last_error()
-        torch.cuda.synchronize()
-        for ref, got, s, a, c in zip(reference, bf.outputs, sinos, angs,
-                                     cens):
-            assert torch.isfinite(got).all()
-            err = O.rel_l2(got.cpu().numpy(), ref.cpu().numpy())
-            assert err < TOL, (call, err)
-        # and against the FP64 oracle, for one item per call
-        k = call
-        oracle = O.fbp_reconstruction(sinos[k], cens[k], angles=angs[k],
-                                      apply_log=False)
-        assert O.rel_l2(bf.outputs[k].cpu().numpy(), oracle) < TOL
+    lib = nat.load()
+
+    # first call: the whole 6-item table
+    for o in bf.outputs:
+        o.fill_(float("nan"))
+    table = (nat.BpItem * bf.n)()
+    ctypes.memmove(table, bf.items_host, ctypes.sizeof(table))
+    rc = lib.atb_backproject_batch_noalloc(ctypes.addressof(table), bf.n, 0,
+                                           stream)
+    assert rc == 0, nat.last_error()
+    # the host table is the caller's again once the call has returned
+    ctypes.memset(table, 0, ctypes.sizeof(table))
+    torch.cuda.synchronize()
+    for ref, got in zip(reference, bf.outputs):
+        assert torch.isfinite(got).all()
+        assert O.rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < TOL
+    oracle = O.fbp_reconstruction(sinos[0], cens[0], angles=angs[0],
+                                  apply_log=False)
+    assert O.rel_l2(bf.outputs[0].cpu().numpy(), oracle) < TOL
+
+    # second call: a smaller, different table (items 4 and 1, in that
+    # order); the first call's six entries are still in the shared array,
+    # and none of them may be run again
+    for o in bf.outputs:
+        o.fill_(float("nan"))
+    pick = [4, 1]
+    small = (nat.BpItem * len(pick))()
+    for k, b in enumerate(pick):
+        ctypes.memmove(ctypes.addressof(small) + k * ctypes.sizeof(nat.BpItem),
+                       ctypes.addressof(bf.items_host)
+                       + b * ctypes.sizeof(nat.BpItem),
+                       ctypes.sizeof(nat.BpItem))
+    rc = lib.atb_backproject_batch_noalloc(ctypes.addressof(small), len(pick),
+                                           0, stream)
+    assert rc == 0, nat.last_error()
+    torch.cuda.synchronize()
+    for b, (ref, got) in enumerate(zip(reference, bf.outputs)):
+        if b in pick:
+            assert torch.isfinite(got).all(), b
+            assert O.rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < TOL, b
+        else:
+            assert torch.isnan(got).all(), b
+    oracle = O.fbp_reconstruction(sinos[1], cens[1], angles=angs[1],
+                                  apply_log=False)
+    assert O.rel_l2(bf.outputs[1].cpu().numpy(), oracle) < TOL
 
 
 def test_noalloc_rejects_oversized_batches(cuda):
