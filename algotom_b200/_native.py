@@ -15,8 +15,9 @@ LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
            "atb_backproject_status", "atb_backproject_centers",
-           "atb_radon_adjoint", "atb_bp_batch_plan", "atb_backproject_batch",
-           "atb_backproject_batch_noalloc", "atb_gaussian_rows",
+           "atb_radon_workspace", "atb_radon_adjoint", "atb_bp_batch_plan",
+           "atb_backproject_batch", "atb_backproject_batch_noalloc",
+           "atb_gaussian_rows",
            "atb_gaussian_cols", "atb_zoom_linear", "atb_image_range",
            "atb_slice_metric_workspace", "atb_slice_metric",
            "atb_slice_entropy64", "atb_vertical_backproject",
@@ -68,9 +69,10 @@ _SIGS = {
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_double,
         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
         ctypes.c_float, _vp, _c_i64, _c_i64, ctypes.c_int, _vp]),
+    "atb_radon_workspace": (_c_i64, [ctypes.c_int, ctypes.c_int]),
     "atb_radon_adjoint": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
-        ctypes.c_double, _vp, _c_i64, _c_i64, _vp]),
+        ctypes.c_double, _vp, _c_i64, _c_i64, _vp, _c_i64, _vp]),
     "atb_bp_batch_plan": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int,
                                          ctypes.c_int]),
     "atb_backproject_batch": (ctypes.c_int, [

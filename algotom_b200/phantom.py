@@ -149,3 +149,32 @@ def ellipse_sinogram(seed, nrow, ncol, center, photons=1e4, angles=None,
     sino = clean.astype(np.float32) if photons is None else \
         poisson_log(clean, photons, seed)
     return sino, np.asarray(angles), params
+
+
+def gaussian_noise_sinogram(seed, nrow, ncol, center, noise=0.01,
+                            device=None):
+    """Sinogram of a seeded 12-ellipse phantom with additive Gaussian noise.
+
+    The sparse-view model-based reconstruction workload: exact line
+    integrals at ``nrow`` angles uniform over [0, pi) (endpoint excluded)
+    plus zero-mean Gaussian noise of standard deviation ``noise`` times the
+    largest clean value.  With ``device`` set the data is made with torch on
+    that device.  Returns (sinogram float32, angles float64, params).
+    """
+    params = ellipse_params(seed, ncol)
+    angles = np.linspace(0.0, math.pi, nrow, endpoint=False)
+    if device is not None:
+        import torch
+        ang_t = torch.as_tensor(angles, dtype=torch.float64, device=device)
+        clean = analytic_sinogram(params, ang_t, ncol, center)
+        g = torch.Generator(device=clean.device)
+        g.manual_seed(int(seed))
+        sd = noise * float(clean.max())
+        sino = clean + sd * torch.randn(clean.shape, generator=g,
+                                        dtype=torch.float64,
+                                        device=clean.device)
+        return sino.to(torch.float32), angles, params
+    clean = analytic_sinogram(params, angles, ncol, center)
+    rng = np.random.default_rng(seed)
+    sino = clean + noise * clean.max() * rng.standard_normal(clean.shape)
+    return sino.astype(np.float32), angles, params

@@ -205,12 +205,18 @@ int atb_backproject_status(int reset);
  *   img   float32 [ncol][nslice][ncol] at img_row_stride / img_slice_stride
  *   trig, center as for atb_backproject
  *   out   float32 [nrow][nslice][ncol] at out_row_stride / out_slice_stride
+ *   workspace  device scratch of at least atb_radon_workspace(nslice, ncol)
+ *         bytes (a transposed copy of the image, read for angles whose rays
+ *         cross the image columns more steeply than its rows)
+ *
+ * Deterministic: the same inputs give the same bits.
  */
+int64_t atb_radon_workspace(int nslice, int ncol);
 int atb_radon_adjoint(const float *img, int64_t img_row_stride,
                       int64_t img_slice_stride, int nrow, int nslice,
                       int ncol, const double *trig, double center, float *out,
                       int64_t out_row_stride, int64_t out_slice_stride,
-                      void *stream);
+                      void *workspace, int64_t workspace_bytes, void *stream);
 
 /*
  * One single-slice back-projection of a batch (device pointers inside).
