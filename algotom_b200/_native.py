@@ -22,7 +22,9 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_slice_metric_workspace", "atb_slice_metric",
            "atb_slice_entropy64", "atb_vertical_backproject",
            "atb_vertical_workspace", "atb_flat_log", "atb_shift_rows",
-           "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid")
+           "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid",
+           "atb_bpf_filter2d_length", "atb_bpf_filter2d_workspace",
+           "atb_bpf_filter2d")
 
 F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
@@ -117,6 +119,13 @@ _SIGS = {
         ctypes.c_int, ctypes.c_int, _vp]),
     "atb_dfi_regrid": (ctypes.c_int, [
         _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "atb_bpf_filter2d_length": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "atb_bpf_filter2d_workspace": (_c_i64, [ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int]),
+    "atb_bpf_filter2d": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_double,
+        ctypes.c_float, _vp, _c_i64, _c_i64, _vp, _c_i64, _vp]),
     "atb_flat_log": (ctypes.c_int, [
         _vp, ctypes.c_int, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, _vp, _vp, _c_i64, ctypes.c_int, _vp, _c_i64, _c_i64,

@@ -1,0 +1,184 @@
+// Mixed-radix complex FFT in shared memory, FP64, for the 2-D filters.
+//
+// Stockham auto-sort: a transform of length n = p_0 p_1 ... p_{s-1} runs s
+// stages; the stage of radix p with L = p_0 ... p_{k-1} takes the p inputs
+// of butterfly j (j in [0, n/p)) at j + r n/p, multiplies input r by
+// w_n^(r (j mod L) n/(L p)), transforms them with a p-point DFT and writes
+// output q to (j / L) L p + (j mod L) + q L.  Each stage reads one buffer
+// and writes the other, so the result ends in natural order with one CTA
+// barrier per stage.  Radices 2, 4 and 8 use the usual butterflies; the odd
+// radices 3, 5, 7, 11 and 13 use the symmetric form of the DFT (sums and
+// differences of inputs r and p - r against cos and sin of 2 pi t / p).
+// Forward: w = exp(-2 pi i / n); inverse: its conjugate, unnormalised.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace atb {
+namespace fft {
+
+constexpr int kMaxStages = 24;
+constexpr int kOddRadices = 5;  // 3, 5, 7, 11, 13
+
+struct Plan {
+  int n;                 // transform length
+  int nstages;
+  int radix[kMaxStages];
+  const double2 *tw;     // exp(-2 pi i m / n), m in [0, n)
+  // cos / sin (2 pi t / p), t = 1 .. (p-1)/2, for p = 3, 5, 7, 11, 13
+  double2 rc[kOddRadices][6];
+};
+
+__host__ __device__ constexpr int odd_slot(int p) {
+  return p == 3 ? 0 : p == 5 ? 1 : p == 7 ? 2 : p == 11 ? 3 : 4;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+  return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// -i z (forward quarter turn) and +i z
+__device__ __forceinline__ double2 mul_mi(double2 z) { return make_double2(z.y, -z.x); }
+__device__ __forceinline__ double2 mul_pi(double2 z) { return make_double2(-z.y, z.x); }
+
+template <bool INV>
+__device__ __forceinline__ double2 quarter(double2 z) {  // w_4 z
+  return INV ? mul_pi(z) : mul_mi(z);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(double2 &v0, double2 &v1, double2 &v2, double2 &v3) {
+  const double2 a = cadd(v0, v2), b = csub(v0, v2);
+  const double2 c = cadd(v1, v3), d = quarter<INV>(csub(v1, v3));
+  v0 = cadd(a, c);
+  v2 = csub(a, c);
+  v1 = cadd(b, d);
+  v3 = csub(b, d);
+}
+
+template <int P, bool INV>
+__device__ __forceinline__ void dft(double2 (&v)[P], const double2 *rc) {
+  if constexpr (P == 2) {
+    const double2 a = v[0];
+    v[0] = cadd(a, v[1]);
+    v[1] = csub(a, v[1]);
+  } else if constexpr (P == 4) {
+    dft4<INV>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (P == 8) {
+    // two 4-point DFTs of the even and odd inputs, then w_8^q combinations
+    double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    constexpr double h = 0.70710678118654752440;  // sqrt(1/2)
+    // w_8 = (h, -h) forward, (h, h) inverse; w_8^2 = -+i; w_8^3 = (-h, -+h)
+    const double2 t1 = INV ? make_double2(h * (o1.x - o1.y), h * (o1.x + o1.y))
+                           : make_double2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    const double2 t2 = quarter<INV>(o2);
+    const double2 t3 = INV ? make_double2(-h * (o3.x + o3.y), h * (o3.x - o3.y))
+                           : make_double2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, t1);
+    v[5] = csub(e1, t1);
+    v[2] = cadd(e2, t2);
+    v[6] = csub(e2, t2);
+    v[3] = cadd(e3, t3);
+    v[7] = csub(e3, t3);
+  } else {
+    // odd P: y_q = A_q -+ i B_q, y_{P-q} = A_q +- i B_q with
+    // A_q = v_0 + sum_r (v_r + v_{P-r}) cos(2 pi q r / P),
+    // B_q = sum_r (v_r - v_{P-r}) sin(2 pi q r / P)
+    constexpr int H = (P - 1) / 2;
+    double2 s[H], d[H];
+    const double2 v0 = v[0];
+    double2 y0 = v0;
+#pragma unroll
+    for (int r = 1; r <= H; ++r) {
+      s[r - 1] = cadd(v[r], v[P - r]);
+      d[r - 1] = csub(v[r], v[P - r]);
+      y0 = cadd(y0, s[r - 1]);
+    }
+    v[0] = y0;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      double2 A = v0, B = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        int t = (q * r) % P;
+        double sg = 1.0;
+        if (t > H) {  // sin(2 pi t / P) = -sin(2 pi (P - t) / P)
+          t = P - t;
+          sg = -1.0;
+        }
+        const double c = rc[t - 1].x, sn = sg * rc[t - 1].y;
+        A.x = fma(s[r - 1].x, c, A.x);
+        A.y = fma(s[r - 1].y, c, A.y);
+        B.x = fma(d[r - 1].x, sn, B.x);
+        B.y = fma(d[r - 1].y, sn, B.y);
+      }
+      // forward: A - i B and A + i B; inverse: the other way round
+      const double2 mB = mul_mi(B), pB = mul_pi(B);
+      v[q] = INV ? cadd(A, pB) : cadd(A, mB);
+      v[P - q] = INV ? cadd(A, mB) : cadd(A, pB);
+    }
+  }
+}
+
+template <int P, bool INV>
+__device__ __forceinline__ void stage(const double2 *__restrict__ in, double2 *__restrict__ out, const Plan &pl,
+                                      int L) {
+  const int n = pl.n, m = n / P;
+  const int tstep = n / (L * P);  // twiddle index step per unit of r * k
+  const double2 *rc = pl.rc[odd_slot(P)];
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const int i = j / L, k = j - i * L;
+    double2 v[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = in[j + r * m];
+    if (k > 0) {
+#pragma unroll
+      for (int r = 1; r < P; ++r) {
+        const double2 w = __ldg(pl.tw + r * k * tstep);
+        v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+      }
+    }
+    dft<P, INV>(v, rc);
+    double2 *o = out + i * L * P + k;
+#pragma unroll
+    for (int q = 0; q < P; ++q) o[q * L] = v[q];
+  }
+}
+
+// Transform of the n values in a[] (b[] is scratch of the same size);
+// returns the buffer holding the result.  Every thread of the CTA calls it.
+template <bool INV>
+__device__ double2 *run(double2 *a, double2 *b, const Plan &pl) {
+  int L = 1;
+  for (int s = 0; s < pl.nstages; ++s) {
+    const int p = pl.radix[s];
+    switch (p) {
+      case 2: stage<2, INV>(a, b, pl, L); break;
+      case 3: stage<3, INV>(a, b, pl, L); break;
+      case 4: stage<4, INV>(a, b, pl, L); break;
+      case 5: stage<5, INV>(a, b, pl, L); break;
+      case 7: stage<7, INV>(a, b, pl, L); break;
+      case 8: stage<8, INV>(a, b, pl, L); break;
+      case 11: stage<11, INV>(a, b, pl, L); break;
+      default: stage<13, INV>(a, b, pl, L); break;
+    }
+    __syncthreads();
+    double2 *t = a;
+    a = b;
+    b = t;
+    L *= p;
+  }
+  return a;
+}
+
+}  // namespace fft
+}  // namespace atb

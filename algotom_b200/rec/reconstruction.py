@@ -23,7 +23,6 @@ import torch
 
 from .. import _native as nat
 from . import windows as win
-from .padding import pad_rows
 from .windows import (make_smoothing_window, make_2d_ramp_window,  # noqa: F401
                       make_circular_ramp_window)
 
@@ -469,77 +468,97 @@ def apply_circular_ramp_filter(rec_img, ramp_win=None, filter_name=None,
     ncol = t.shape[0]
     if pad is None:
         pad = min(int(0.15 * ncol), 150)
-    r = _circular_filter(t.unsqueeze(0), ramp_win, filter_name, pad,
-                         pad_mode)[0]
+    r = _circular_filter(t.to(torch.float32)[:, None, :], ramp_win,
+                         filter_name, pad, pad_mode)[:, 0, :]
     return r.cpu().numpy().astype(np.float64) if is_np else r
 
 
 _circ_cache = {}
 
 
-def _circular_spectrum(ramp_win, filter_name, n, device):
-    """Half spectrum [n, n//2+1] for irfft2 of the 2-D circular window.
+def _circular_spectrum(ramp_win, filter_name, ncol, pad, device):
+    """Spectrum, its kind and the twiddles of ``atb_bpf_filter2d`` for the
+    2-D circular ramp filter of ``reconstruction.py:527-560``.
 
-    The reference keeps ``real(ifft2(fft2(x) * ifftshift(W2)))``; for a real
-    image only the Hermitian part ``(H[k] + conj(H[-k])) / 2`` of
-    ``H = ifftshift(W2)`` reaches the real part, so the product can be taken
-    on the real-to-complex half spectrum.
+    The reference keeps ``real(ifft2(fft2(x) * H))`` with
+    ``H = ifftshift(W2)``; for a real image only the Hermitian part
+    ``Hh = (H[k] + conj(H[-k])) / 2`` reaches the real part.  For the
+    library's transform length T = N = ncol + 2 pad the spectrum is Hh
+    itself (real when W2 is); for a longer T (N with a prime factor above
+    13) it is the transform of the N-periodic kernel ``ifft2(Hh)`` laid on
+    the T-torus at the lags ``[pad - N + 1, pad + ncol - 1]`` that the crop
+    uses.  Either way scaled by 1 / T^2 and stored transposed ([kx][ky]).
+    Returns (spectrum, is_complex, twiddle, T), cached per (filter, ncol,
+    pad, device) for the built-in windows.
     """
+    n = ncol + 2 * pad
     key = None
     if ramp_win is None or np.shape(ramp_win) != (n, n):
-        key = (filter_name, n, device)
+        key = (filter_name, ncol, pad, str(device))
         hit = _circ_cache.get(key)
         if hit is not None:
             return hit
         ramp_win = make_circular_ramp_window(n, filter_name)
-    h = np.fft.ifftshift(np.asarray(ramp_win.cpu() if isinstance(
-        ramp_win, torch.Tensor) else ramp_win, dtype=np.complex128))
+    t = nat.call("atb_bpf_filter2d_length", ncol, pad)
+    w2 = ramp_win.cpu().numpy() if isinstance(ramp_win, torch.Tensor) \
+        else np.asarray(ramp_win)
+    h = np.fft.ifftshift(np.asarray(w2, dtype=np.complex128))
     hm = np.roll(np.flip(h, axis=(0, 1)), 1, axis=(0, 1))  # H[-k1, -k2]
     hh = 0.5 * (h + np.conj(hm))
-    t = torch.from_numpy(np.ascontiguousarray(hh[:, :n // 2 + 1])).to(
+    if t == n:
+        spec = hh / float(n) ** 2
+        if not np.any(spec.imag):
+            spec = spec.real
+    else:
+        k = np.fft.ifft2(hh).real  # real: hh is Hermitian
+        lag = np.arange(pad - n + 1, pad + ncol)
+        km = np.zeros((t, t))
+        km[np.ix_(lag % t, lag % t)] = k[np.ix_(lag % n, lag % n)]
+        spec = np.fft.fft2(km) / float(t) ** 2
+    is_complex = np.iscomplexobj(spec)
+    sp = torch.from_numpy(np.ascontiguousarray(spec.T)).to(
+        device, torch.complex128 if is_complex else torch.float64)
+    tw = torch.from_numpy(np.exp(-2j * np.pi * np.arange(t) / t)).to(
         device, torch.complex128)
+    res = (sp, is_complex, tw, t)
     if key is not None:
         if len(_circ_cache) > 8:
             _circ_cache.clear()
-        _circ_cache[key] = t
-    return t
+        _circ_cache[key] = res
+    return res
 
 
-def _pad_2d(x, pad, mode):
-    """``np.pad(img, pad, mode)`` of every image of a [k, n, n] tensor on
-    its device, for numpy's ten modes: the rows axis first over the original
-    columns, then the columns axis over all rows (numpy's order, which fixes
-    the corners of the statistic modes)."""
-    k, n, _ = x.shape
-    if pad == 0:
-        return x
-    t = pad_rows(x.transpose(1, 2).reshape(k * n, n), pad, mode)
-    t = t.reshape(k, n, n + 2 * pad).transpose(1, 2)
-    m = n + 2 * pad
-    return pad_rows(t.reshape(k * m, n), pad, mode).reshape(k, m, m)
+# device bytes of 2-D transform workspace per call of the BPF filter
+_BPF_WORKSPACE = 2 << 30
 
 
-def _circular_filter(stack, ramp_win, filter_name, pad, pad_mode, slab=16):
-    """[nslice, ncol, ncol] float32 -> filtered, same shape.
-
-    2-D circular ramp filter of ``reconstruction.py:527-560`` on the device,
-    a slab of slices at a time: pad (numpy's modes, device index maps and
-    statistics), then the library real-to-complex transform in FP64 (cuFFT
-    through torch), the product with the Hermitian half window, the inverse
-    transform, crop.  The ramp lifts the high frequencies, so float32
-    transforms would cost ~2e-5 relative; in FP64 the result keeps the
-    back-projection's ~1e-6.
-    """
-    nslice, ncol, _ = stack.shape
-    n = ncol + 2 * pad
+def _circular_filter(stack, ramp_win, filter_name, pad, pad_mode, out=None,
+                     mask_r2=-1.0, scale=1.0):
+    """2-D circular ramp filter of ``reconstruction.py:527-560`` on every
+    slice of a back-projection stack ``[ncol (y), nslice, ncol (x)]``
+    (any strides, x contiguous), with the circle mask and scale of
+    ``reconstruction.py:679-684`` fused: ``atb_bpf_filter2d`` (numpy's ten
+    pad modes, FP64 transforms of this library).  ``out`` may be ``stack``
+    itself."""
+    ncol, nslice, _ = stack.shape
     if pad_mode not in nat.PAD_MODES:
         raise ValueError("pad_mode %r is not supported" % (pad_mode,))
-    hh = _circular_spectrum(ramp_win, filter_name, n, stack.device)
-    out = torch.empty_like(stack)
-    for k0 in range(0, nslice, slab):
-        xp = _pad_2d(stack[k0:k0 + slab].to(torch.float64), pad, pad_mode)
-        y = torch.fft.irfft2(torch.fft.rfft2(xp) * hh, s=(n, n))
-        out[k0:k0 + slab] = y[:, pad:pad + ncol, pad:pad + ncol]
+    if stack.stride(-1) != 1:
+        stack = stack.contiguous()
+    spec, is_complex, tw, t = _circular_spectrum(ramp_win, filter_name, ncol,
+                                                 pad, stack.device)
+    if out is None:
+        out = torch.empty_like(stack)
+    one = nat.call("atb_bpf_filter2d_workspace", ncol, pad, 1)
+    npairs = (nslice + 1) // 2
+    pairs = max(1, min(npairs, _BPF_WORKSPACE // one))
+    nbytes = nat.call("atb_bpf_filter2d_workspace", ncol, pad, pairs)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=stack.device)
+    nat.call("atb_bpf_filter2d", stack.data_ptr(), stack.stride(0),
+             stack.stride(1), nslice, ncol, pad, nat.PAD_MODES[pad_mode],
+             spec.data_ptr(), int(is_complex), tw.data_ptr(), float(mask_r2),
+             float(scale), out.data_ptr(), out.stride(0), out.stride(1),
+             ws.data_ptr(), nbytes, _stream_ptr(stack.device))
     return out
 
 
@@ -564,16 +583,10 @@ def bpf_reconstruction(sinogram, center, angles=None, ratio=1.0,
     s3 = _neg_log(_as3(t)) if apply_log else _as3(t)
     bp = backproject(s3, angles, center, edge_pad=True, kahan=kahan)
     del s3, t
-    stack = bp.permute(1, 0, 2).contiguous()  # [nslice, ncol, ncol]
-    filt = _circular_filter(stack, ramp_win, filter_name, pad, pad_mode)
-    r2 = _mask_r2(ratio, center, ncol)
-    if r2 >= 0:
-        c = ncol // 2
-        idx = torch.arange(ncol, device=filt.device) - c
-        m = ((idx[None, :] ** 2 + idx[:, None] ** 2).to(torch.float64) <= r2)
-        filt = filt * m.to(filt.dtype)
-    filt = filt * _scale(nrow)
-    rec = filt.permute(1, 0, 2)
+    # filter, mask and scale in place, in the [ncol][nslice][ncol] layout
+    rec = _circular_filter(bp, ramp_win, filter_name, pad, pad_mode, out=bp,
+                           mask_r2=_mask_r2(ratio, center, ncol),
+                           scale=_scale(nrow))
     return _finish(rec, two_d, is_np, out,
                    np.float64 if two_d else np.float32)
 

@@ -304,6 +304,56 @@ int atb_backproject_batch(const atb_bp_item *items, int nitems,
 int atb_backproject_batch_noalloc(const atb_bp_item *items, int nitems,
                                   int max_ctas, void *stream);
 
+/*
+ * Transform length T the 2-D BPF filter uses for a slice of ncol x ncol
+ * padded by pad on every side: N = ncol + 2 pad when all prime factors of
+ * N are at most 13, else the smallest M >= N + ncol - 1 whose prime
+ * factors are at most 7 (a circular convolution of that length reproduces
+ * the N-periodic one exactly on the cropped slice).  ATB_ERANGE above 7168.
+ */
+int atb_bpf_filter2d_length(int ncol, int pad);
+
+/* Device workspace bytes of atb_bpf_filter2d processing `pairs` slice
+ * pairs at once (it processes the stack in groups of as many pairs as the
+ * workspace it is given holds; one pair is the minimum). */
+int64_t atb_bpf_filter2d_workspace(int ncol, int pad, int pairs);
+
+/*
+ * 2-D circular ramp filter of every slice of a back-projection stack, with
+ * the circle mask and scale of BPF fused; replaces
+ * apply_circular_ramp_filter (algotom/rec/reconstruction.py:527-560) as
+ * bpf_reconstruction applies it per slice, then its mask and
+ * pi/(nrow-1) scale (reconstruction.py:675-684).  Each slice is padded to
+ * N x N with numpy's mode (both axes, axis 0 first as numpy does), filtered
+ * with the spectrum, cropped; FP64 transforms of this library, two slices
+ * per complex transform.
+ *
+ *   src       float32 [ncol (y)][nslice][ncol (x)] at the given strides
+ *             (the layout atb_backproject writes)
+ *   pad, pad_mode  as apply_circular_ramp_filter (ATB_PAD_*)
+ *   spectrum  device [T][T] with T = atb_bpf_filter2d_length(ncol, pad),
+ *             stored transposed ([kx][ky]) and scaled by 1 / T^2: for
+ *             T = N the Hermitian part (H(k) + conj(H(-k))) / 2 of
+ *             H = ifftshift(W2); for T > N the 2-D transform of the
+ *             N-periodic kernel ifft2 of that part, placed on the T x T
+ *             torus at the lags [pad - N + 1, pad + ncol - 1] of each axis.
+ *             float64 when spectrum_complex == 0, else complex128
+ *   twiddle   complex128 [T]: exp(-2 pi i m / T)
+ *   mask_r2   < 0: no mask; else pixels with (x-c)^2 + (y-c)^2 > mask_r2,
+ *             c = ncol/2, are written as 0
+ *   scale     multiplies every written pixel
+ *   dst       float32 [ncol][nslice][ncol] at the given strides; may be src
+ *   workspace device scratch of at least
+ *             atb_bpf_filter2d_workspace(ncol, pad, 1) bytes
+ */
+int atb_bpf_filter2d(const float *src, int64_t src_row_stride,
+                     int64_t src_slice_stride, int nslice, int ncol, int pad,
+                     int pad_mode, const void *spectrum, int spectrum_complex,
+                     const void *twiddle, double mask_r2, float scale,
+                     float *dst, int64_t dst_row_stride,
+                     int64_t dst_slice_stride, void *workspace,
+                     int64_t workspace_bytes, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Centre search by slice metrics (find_center_based_slice_metric,        */
 /* algotom/rec/reconstruction.py:1212-1458).  The candidate centres are   */

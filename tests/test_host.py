@@ -157,25 +157,6 @@ def test_autotuner_survives_corrupt_cache(tmp_path):
     assert json.loads(path.read_text())["k"]["choice"] == 1
 
 
-@pytest.mark.parametrize("mode", ["edge", "constant", "reflect", "symmetric",
-                                  "wrap", "linear_ramp", "mean", "maximum",
-                                  "minimum", "median"])
-def test_bpf_image_padding_matches_numpy(mode):
-    """The 2-D padding before the BPF filter (``np.pad(rec_img, pad,
-    pad_mode)``, reconstruction.py:549) for numpy's ten modes, including
-    pads wider than the image and the corners of the statistic modes."""
-    import torch
-    from algotom_b200.rec import reconstruction as R
-    rng = np.random.default_rng(2)
-    for n in (1, 2, 5, 8):
-        x = rng.standard_normal((2, n, n))
-        for pad in (0, 1, 3, 11):
-            got = R._pad_2d(torch.from_numpy(x), pad, mode).numpy()
-            ref = np.stack([np.pad(a, pad, mode=mode) for a in x])
-            assert got.shape == ref.shape
-            assert np.allclose(got, ref, rtol=1e-14, atol=1e-14), (n, pad)
-
-
 def test_stream_slab_spans_cover_the_stack():
     """Slabs of a host stack streamed through the device: contiguous, cover
     every slice once, at most ``slab`` slices, ramped at both ends of long
