@@ -45,7 +45,7 @@ namespace {
 using atb::fft::Plan;
 
 constexpr int kThreads = 256;
-constexpr int kMaxLen = 7168;        // two buffers of T complex doubles fit 227 KB
+constexpr int kMaxLen = 7168;        // two buffers of T complex doubles + twiddles fit 227 KB
 constexpr int kStatThreads = 1024;
 constexpr int kMaxStatLen = 8192;    // lines sorted in shared memory (median)
 
@@ -123,9 +123,15 @@ __device__ double pad_value(const BpfArgs &a, const float *X, int ks, int ry, in
   }
 }
 
+// Grids put the slice pair on x, so that the CTAs of one row / column of
+// every pair run together (the columns kernel then reads each spectrum
+// column once from DRAM).  Shared memory: two buffers of T values, then
+// the twiddle table.
 __global__ void __launch_bounds__(kThreads) bpf_rows_kernel(BpfArgs a, const __grid_constant__ Plan pl) {
   extern __shared__ double2 sm[];
-  const int ry = blockIdx.x, g = blockIdx.y, T = pl.n;
+  const int ry = blockIdx.y, g = blockIdx.x, T = pl.n;
+  double2 *tws = sm + 2 * T;
+  atb::fft::load_twiddles(pl, tws);
   const int sa = a.slice0 + 2 * g, sb = sa + 1;
   const bool hb = sb < a.nslice;
   const float *Xa = a.src + (long long)sa * a.sss;
@@ -139,19 +145,21 @@ __global__ void __launch_bounds__(kThreads) bpf_rows_kernel(BpfArgs a, const __g
     sm[rx] = z;
   }
   __syncthreads();
-  const double2 *res = atb::fft::run<false>(sm, sm + T, pl);
+  const double2 *res = atb::fft::run<false>(sm, sm + T, pl, tws);
   double2 *w = a.work + ((long long)g * a.n + ry) * T;
   for (int kx = threadIdx.x; kx < T; kx += blockDim.x) w[kx] = res[kx];
 }
 
 __global__ void __launch_bounds__(kThreads) bpf_cols_kernel(BpfArgs a, const __grid_constant__ Plan pl) {
   extern __shared__ double2 sm[];
-  const int kx = blockIdx.x, g = blockIdx.y, T = pl.n, n = a.n;
+  const int kx = blockIdx.y, g = blockIdx.x, T = pl.n, n = a.n;
+  double2 *tws = sm + 2 * T;
+  atb::fft::load_twiddles(pl, tws);
   double2 *w = a.work + (long long)g * n * T + kx;
   for (int ry = threadIdx.x; ry < T; ry += blockDim.x)
     sm[ry] = ry < n ? w[(long long)ry * T] : make_double2(0.0, 0.0);
   __syncthreads();
-  double2 *res = atb::fft::run<false>(sm, sm + T, pl);
+  double2 *res = atb::fft::run<false>(sm, sm + T, pl, tws);
   double2 *other = res == sm ? sm + T : sm;
   if (a.spec_complex) {
     const double2 *S = static_cast<const double2 *>(a.spec) + (long long)kx * T;
@@ -165,17 +173,19 @@ __global__ void __launch_bounds__(kThreads) bpf_cols_kernel(BpfArgs a, const __g
     }
   }
   __syncthreads();
-  const double2 *out = atb::fft::run<true>(res, other, pl);
+  const double2 *out = atb::fft::run<true>(res, other, pl, tws);
   for (int u = a.pad + threadIdx.x; u < a.pad + a.ncol; u += blockDim.x) w[(long long)u * T] = out[u];
 }
 
 __global__ void __launch_bounds__(kThreads) bpf_out_kernel(BpfArgs a, const __grid_constant__ Plan pl) {
   extern __shared__ double2 sm[];
-  const int y = blockIdx.x, g = blockIdx.y, T = pl.n;
+  const int y = blockIdx.y, g = blockIdx.x, T = pl.n;
+  double2 *tws = sm + 2 * T;
+  atb::fft::load_twiddles(pl, tws);
   const double2 *w = a.work + ((long long)g * a.n + y + a.pad) * T;
   for (int kx = threadIdx.x; kx < T; kx += blockDim.x) sm[kx] = w[kx];
   __syncthreads();
-  const double2 *res = atb::fft::run<true>(sm, sm + T, pl);
+  const double2 *res = atb::fft::run<true>(sm, sm + T, pl, tws);
   const int sa = a.slice0 + 2 * g, sb = sa + 1;
   const bool hb = sb < a.nslice;
   const int c = a.ncol / 2;
@@ -381,14 +391,14 @@ extern "C" int atb_bpf_filter2d(const float *src, int64_t src_row_stride, int64_
   if (workspace_bytes < per_pair)
     return atb::fail(ATB_EINVAL, "atb_bpf_filter2d: workspace of %lld bytes needed for one slice pair",
                      (long long)per_pair);
-  // as many slice pairs per group as the workspace holds (grid y <= 65535)
+  // as many slice pairs per group as the workspace holds
   const int npairs = (nslice + 1) / 2;
   int pairs = npairs < 32768 ? npairs : 32768;
   while (pairs > 1 && atb_bpf_filter2d_workspace(ncol, pad, pairs) > workspace_bytes) pairs = (pairs + 1) / 2;
   while (pairs < npairs && pairs < 32768 && atb_bpf_filter2d_workspace(ncol, pad, pairs + 1) <= workspace_bytes)
     ++pairs;
 
-  const size_t smem = 2 * (size_t)t * sizeof(double2);
+  const size_t smem = (2 * (size_t)t + atb::fft::twiddle_entries(t)) * sizeof(double2);
   int rc = atb::ensure_smem(bpf_rows_kernel, smem, "atb_bpf_filter2d");
   if (rc == ATB_OK) rc = atb::ensure_smem(bpf_cols_kernel, smem, "atb_bpf_filter2d");
   if (rc == ATB_OK) rc = atb::ensure_smem(bpf_out_kernel, smem, "atb_bpf_filter2d");
@@ -431,9 +441,9 @@ extern "C" int atb_bpf_filter2d(const float *src, int64_t src_row_stride, int64_
       bpf_stats_kernel<<<dim3(2 * ncol, gs), kStatThreads, 0, st>>>(a, colstat, rowstat);
       bpf_padstat_kernel<<<gs, kStatThreads, stat_smem, st>>>(a, colstat, padstat);
     }
-    bpf_rows_kernel<<<dim3(n, gp), kThreads, smem, st>>>(a, pl);
-    bpf_cols_kernel<<<dim3(t, gp), kThreads, smem, st>>>(a, pl);
-    bpf_out_kernel<<<dim3(ncol, gp), kThreads, smem, st>>>(a, pl);
+    bpf_rows_kernel<<<dim3(gp, n), kThreads, smem, st>>>(a, pl);
+    bpf_cols_kernel<<<dim3(gp, t), kThreads, smem, st>>>(a, pl);
+    bpf_out_kernel<<<dim3(gp, ncol), kThreads, smem, st>>>(a, pl);
     rc = atb::check_launch("atb_bpf_filter2d");
     if (rc != ATB_OK) return rc;
   }

@@ -61,7 +61,7 @@ __device__ __forceinline__ void dft4(double2 &v0, double2 &v1, double2 &v2, doub
 }
 
 template <int P, bool INV>
-__device__ __forceinline__ void dft(double2 (&v)[P], const double2 *rc) {
+__device__ __forceinline__ void dft(double2 (&v)[P], const double2 (&rc)[6]) {
   if constexpr (P == 2) {
     const double2 a = v[0];
     v[0] = cadd(a, v[1]);
@@ -129,12 +129,36 @@ __device__ __forceinline__ void dft(double2 (&v)[P], const double2 *rc) {
   }
 }
 
+// Twiddles w_n^e in shared memory as a two-level table: e = 64 h + l,
+// w^e = hi[h] lo[l] (one complex product, within two roundings of the
+// correctly rounded value); 64 + ceil(n / 64) entries instead of n.
+constexpr int kTwLo = 64;
+__host__ __device__ constexpr int twiddle_entries(int n) { return kTwLo + (n + kTwLo - 1) / kTwLo; }
+
+// Fills the table from the plan's full table; call before the first run
+// (a CTA barrier separates them).
+__device__ __forceinline__ void load_twiddles(const Plan &pl, double2 *tws) {
+  const int nhi = (pl.n + kTwLo - 1) / kTwLo;
+  for (int i = threadIdx.x; i < kTwLo + nhi; i += blockDim.x)
+    tws[i] = i < kTwLo ? (i < pl.n ? __ldg(pl.tw + i) : make_double2(1.0, 0.0)) : __ldg(pl.tw + (i - kTwLo) * kTwLo);
+}
+
+__device__ __forceinline__ double2 twiddle(const double2 *tws, int e) {
+  return cmul(tws[kTwLo + (e >> 6)], tws[e & (kTwLo - 1)]);
+}
+
 template <int P, bool INV>
 __device__ __forceinline__ void stage(const double2 *__restrict__ in, double2 *__restrict__ out, const Plan &pl,
-                                      int L) {
+                                      const double2 *tws, int L) {
   const int n = pl.n, m = n / P;
   const int tstep = n / (L * P);  // twiddle index step per unit of r * k
-  const double2 *rc = pl.rc[odd_slot(P)];
+  // the odd radix's cos / sin in registers for the whole stage (read
+  // through a pointer the compiler would reload them for every butterfly)
+  double2 rc[6];
+  if constexpr (P % 2 == 1) {
+#pragma unroll
+    for (int t = 0; t < (P - 1) / 2; ++t) rc[t] = pl.rc[odd_slot(P)][t];
+  }
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     const int i = j / L, k = j - i * L;
     double2 v[P];
@@ -143,7 +167,7 @@ __device__ __forceinline__ void stage(const double2 *__restrict__ in, double2 *_
     if (k > 0) {
 #pragma unroll
       for (int r = 1; r < P; ++r) {
-        const double2 w = __ldg(pl.tw + r * k * tstep);
+        const double2 w = twiddle(tws, r * k * tstep);
         v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
       }
     }
@@ -154,22 +178,23 @@ __device__ __forceinline__ void stage(const double2 *__restrict__ in, double2 *_
   }
 }
 
-// Transform of the n values in a[] (b[] is scratch of the same size);
-// returns the buffer holding the result.  Every thread of the CTA calls it.
+// Transform of the n values in a[] (b[] is scratch of the same size; tws
+// the table of load_twiddles); returns the buffer holding the result.
+// Every thread of the CTA calls it.
 template <bool INV>
-__device__ double2 *run(double2 *a, double2 *b, const Plan &pl) {
+__device__ double2 *run(double2 *a, double2 *b, const Plan &pl, const double2 *tws) {
   int L = 1;
   for (int s = 0; s < pl.nstages; ++s) {
     const int p = pl.radix[s];
     switch (p) {
-      case 2: stage<2, INV>(a, b, pl, L); break;
-      case 3: stage<3, INV>(a, b, pl, L); break;
-      case 4: stage<4, INV>(a, b, pl, L); break;
-      case 5: stage<5, INV>(a, b, pl, L); break;
-      case 7: stage<7, INV>(a, b, pl, L); break;
-      case 8: stage<8, INV>(a, b, pl, L); break;
-      case 11: stage<11, INV>(a, b, pl, L); break;
-      default: stage<13, INV>(a, b, pl, L); break;
+      case 2: stage<2, INV>(a, b, pl, tws, L); break;
+      case 3: stage<3, INV>(a, b, pl, tws, L); break;
+      case 4: stage<4, INV>(a, b, pl, tws, L); break;
+      case 5: stage<5, INV>(a, b, pl, tws, L); break;
+      case 7: stage<7, INV>(a, b, pl, tws, L); break;
+      case 8: stage<8, INV>(a, b, pl, tws, L); break;
+      case 11: stage<11, INV>(a, b, pl, tws, L); break;
+      default: stage<13, INV>(a, b, pl, tws, L); break;
     }
     __syncthreads();
     double2 *t = a;
