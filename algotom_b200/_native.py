@@ -24,7 +24,7 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_vertical_workspace", "atb_flat_log", "atb_shift_rows",
            "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid",
            "atb_bpf_filter2d_length", "atb_bpf_filter2d_workspace",
-           "atb_bpf_filter2d")
+           "atb_bpf_filter2d", "atb_filter_rows_batch")
 
 F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
@@ -35,6 +35,15 @@ PAD_MODES = {"edge": 0, "constant": 1, "reflect": 2, "symmetric": 3,
 
 class NativeLibraryError(RuntimeError):
     """The CUDA library is missing, failed to load, or a call failed."""
+
+
+class FilterItem(ctypes.Structure):
+    """``atb_filter_item`` of include/algotom_b200.h."""
+    _fields_ = [("src", ctypes.c_void_p), ("src_row_stride", ctypes.c_int64),
+                ("dst", ctypes.c_void_p), ("dst_row_stride", ctypes.c_int64),
+                ("spec", ctypes.c_void_p), ("nrow", ctypes.c_int),
+                ("ncol", ctypes.c_int), ("pad", ctypes.c_int),
+                ("pair_offset", ctypes.c_int)]
 
 
 class BpItem(ctypes.Structure):
@@ -59,6 +68,9 @@ _SIGS = {
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
         ctypes.c_int, _vp, ctypes.c_int, _c_i64, _c_i64, _vp]),
+    "atb_filter_rows_batch": (ctypes.c_int, [
+        _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+        ctypes.c_int, ctypes.c_int, _vp]),
     "atb_neg_log": (ctypes.c_int, [
         _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
         _c_i64, _c_i64, _vp]),

@@ -247,8 +247,9 @@ __device__ float2 block_select2(const float2 *x, int pad, int ncol, int rank, fl
   return make_float2(fkey_inv(lo1), fkey_inv(lo2));
 }
 
+// Filters row pair `pair` of a (CTA-uniform).
 template <typename OutT, int T>
-__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) filter_rows_kernel(FilterArgs a) {
+__device__ __forceinline__ void filter_rows_body(const FilterArgs &a, long long pair) {
   extern __shared__ float2 sm[];  // M complex, padded by pidx
   __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
   __shared__ float2 ta[128], tb[128];
@@ -265,13 +266,13 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) filter_rows_kernel(Filter
   int i1, k1, i2, k2;
   bool ok2;
   if (a.pair_within_angle) {
-    i1 = blockIdx.x / a.pairs_per_angle;
-    k1 = 2 * (blockIdx.x % a.pairs_per_angle);
+    i1 = (int)(pair / a.pairs_per_angle);
+    k1 = (int)(2 * (pair % a.pairs_per_angle));
     i2 = i1;
     k2 = k1 + 1;
     ok2 = k2 < a.nslice;
   } else {
-    const long long r1 = 2LL * blockIdx.x, r2 = r1 + 1;
+    const long long r1 = 2LL * pair, r2 = r1 + 1;
     i1 = (int)(r1 / a.nslice);
     k1 = (int)(r1 % a.nslice);
     i2 = (int)(r2 / a.nslice);
@@ -376,6 +377,36 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) filter_rows_kernel(Filter
   }
 }
 
+template <typename OutT, int T>
+__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) filter_rows_kernel(FilterArgs a) {
+  filter_rows_body<OutT, T>(a, blockIdx.x);
+}
+
+// One launch over the row pairs of several single-slice sinograms that
+// share the FFT length: CTA p finds the item whose pair range holds p
+// (binary search on pair_offset) and filters that pair.
+template <typename OutT, int T>
+__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
+    filter_batch_kernel(FilterArgs a, const atb_filter_item *items, int nitems) {
+  const int p = blockIdx.x;
+  int lo = 0, hi = nitems - 1;
+  while (lo < hi) {  // last item with pair_offset <= p
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].pair_offset <= p) lo = mid; else hi = mid - 1;
+  }
+  const atb_filter_item it = items[lo];
+  const int pair = p - it.pair_offset;
+  if (pair < 0 || pair >= (it.nrow + 1) / 2) return;  // CTA-uniform
+  FilterArgs b = a;
+  b.src = it.src; b.srs = it.src_row_stride; b.sss = 0;
+  b.nrow = it.nrow; b.nslice = 1; b.ncol = it.ncol; b.pad = it.pad;
+  b.spec = reinterpret_cast<const float2 *>(it.spec); b.spec_rows = 1;
+  b.dst = it.dst; b.drs = it.dst_row_stride; b.dss = 0;
+  b.pair_within_angle = 0;
+  b.pairs_per_angle = 0;
+  filter_rows_body<OutT, T>(b, pair);
+}
+
 __global__ void neg_log_kernel(const float *__restrict__ src, long long srs, long long sss, int nrow,
                                int nslice, int ncol, float *dst, long long drs, long long dss) {
   const long long total = (long long)nrow * nslice * ncol;
@@ -395,6 +426,26 @@ int launch_filter_t(const FilterArgs &a, long long npairs, cudaStream_t st) {
   if (rc != ATB_OK) return rc;
   filter_rows_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(a);
   return atb::check_launch("atb_filter_rows");
+}
+
+template <typename OutT, int T>
+int launch_batch_t(const FilterArgs &a, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * (size_t)((1 << a.log2m) + ((1 << a.log2m) >> 4));
+  const int rc = atb::ensure_smem(filter_batch_kernel<OutT, T>, smem, "atb_filter_rows_batch");
+  if (rc != ATB_OK) return rc;
+  filter_batch_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(a, items, nitems);
+  return atb::check_launch("atb_filter_rows_batch");
+}
+
+template <typename OutT>
+int launch_batch(const FilterArgs &a, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
+  switch (a.log2m) {
+    case 14: return launch_batch_t<OutT, 512>(a, items, nitems, npairs, st);
+    case 13: return launch_batch_t<OutT, 256>(a, items, nitems, npairs, st);
+    case 12: return launch_batch_t<OutT, 128>(a, items, nitems, npairs, st);
+    case 11: return launch_batch_t<OutT, 64>(a, items, nitems, npairs, st);
+    default: return launch_batch_t<OutT, 32>(a, items, nitems, npairs, st);
+  }
 }
 
 // T = max(32, M / 32): every thread holds 32 complex values per stage
@@ -463,6 +514,31 @@ int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_
     case ATB_F16: return launch_filter<__half>(a, npairs, st);
     case ATB_BF16: return launch_filter<__nv_bfloat16>(a, npairs, st);
     default: return atb::fail(ATB_EINVAL, "atb_filter_rows: unknown dst_dtype %d", dst_dtype);
+  }
+}
+
+int atb_filter_rows_batch(const atb_filter_item *items, int nitems, int npairs, int pad_mode, int apply_log,
+                          const void *twiddle, int log2m, int dst_dtype, void *stream) {
+  if (!items || !twiddle) return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: null pointer");
+  if (nitems < 1 || npairs < 1) return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: empty batch");
+  if (pad_mode < ATB_PAD_EDGE || pad_mode > ATB_PAD_MEDIAN)
+    return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown pad_mode %d", pad_mode);
+  if (log2m < kMinLog2M || log2m > kMaxLog2M)
+    return atb::fail(ATB_ERANGE, "atb_filter_rows_batch: log2m=%d outside [%d, %d]", log2m, kMinLog2M, kMaxLog2M);
+  FilterArgs a;
+  a.src = nullptr; a.srs = 0; a.sss = 0;
+  a.nrow = 0; a.nslice = 1; a.ncol = 0; a.pad = 0; a.mode = pad_mode; a.apply_log = apply_log;
+  a.spec = nullptr; a.spec_rows = 1;
+  a.tw = reinterpret_cast<const float2 *>(twiddle); a.log2m = log2m;
+  a.dst = nullptr; a.drs = 0; a.dss = 0;
+  a.pair_within_angle = 0;
+  a.pairs_per_angle = 0;
+  cudaStream_t st = atb::as_stream(stream);
+  switch (dst_dtype) {
+    case ATB_F32: return launch_batch<float>(a, items, nitems, npairs, st);
+    case ATB_F16: return launch_batch<__half>(a, items, nitems, npairs, st);
+    case ATB_BF16: return launch_batch<__nv_bfloat16>(a, items, nitems, npairs, st);
+    default: return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown dst_dtype %d", dst_dtype);
   }
 }
 

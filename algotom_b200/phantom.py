@@ -178,3 +178,29 @@ def gaussian_noise_sinogram(seed, nrow, ncol, center, noise=0.01,
     rng = np.random.default_rng(seed)
     sino = clean + noise * clean.max() * rng.standard_normal(clean.shape)
     return sino.astype(np.float32), angles, params
+
+
+def half_acquisition_sinogram(seed, nrow, ncol, cor, photons=1e4,
+                              device=None):
+    """A 360-degree half-acquisition scan: ``nrow`` angles uniform over
+    [0, 2 pi) (endpoint excluded) on a detector of ``ncol`` pixels whose
+    rotation axis sits at column ``cor`` near one edge, so that each view
+    covers one side of the object and the opposite view the other.  The
+    seeded 12-ellipse object is drawn for the field the views cover
+    together (width ``2 max(cor, ncol - 1 - cor) + 1``, the width
+    ``extend_sinogram`` restores).  Returns (-log sinogram float32, angles
+    float64, params, field width)."""
+    field = int(2 * max(cor, ncol - 1 - cor) + 1)
+    params = ellipse_params(seed, field)
+    angles = np.linspace(0.0, 2.0 * math.pi, nrow, endpoint=False)
+    if device is not None:
+        import torch
+        ang_t = torch.as_tensor(angles, dtype=torch.float64, device=device)
+        clean = analytic_sinogram(params, ang_t, ncol, cor, size=field)
+        sino = clean if photons is None else poisson_log(clean, photons,
+                                                         seed)
+        return sino.to(torch.float32), angles, params, field
+    clean = analytic_sinogram(params, angles, ncol, cor, size=field)
+    sino = clean.astype(np.float32) if photons is None else \
+        poisson_log(clean, photons, seed)
+    return sino, angles, params, field

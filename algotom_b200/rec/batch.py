@@ -3,8 +3,9 @@
 The reference reconstructs one slice (or one chunk of slices sharing a
 geometry) per call (``algotom/rec/reconstruction.py:362-493``).  Here a whole
 list of single-slice problems -- each with its own width, angles and centre --
-is filtered (one ``atb_filter_rows`` launch per item) and back-projected in
-ONE persistent launch (``atb_backproject_batch``): a device counter hands out
+is filtered (one ``atb_filter_rows_batch`` launch per FFT length among the
+items: at most four for widths 512-6600) and back-projected in ONE
+persistent launch (``atb_backproject_batch``): a device counter hands out
 (item, 64 x 64 tile) work units, largest angle counts first.  The whole
 sequence can be captured once into a CUDA graph and replayed; the persistent
 kernel returns its counter to zero, so replays need no reset.
@@ -84,6 +85,27 @@ class BatchedFBP:
         raw = bytes(items)
         self.items_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8
                                           ).to(self.dev)
+        # one filter launch per FFT length: a device table of the items
+        # that share it, each with the index of its first row pair
+        self._filter_groups = []
+        for log2m in sorted(set(self._log2m)):
+            members = [b for b in range(self.n) if self._log2m[b] == log2m]
+            tab = (nat.FilterItem * len(members))()
+            off = 0
+            for e, b in enumerate(members):
+                x, f = self.inputs[b], self.filtered[b]
+                it = tab[e]
+                it.src, it.src_row_stride = x.data_ptr(), x.stride(0)
+                it.dst, it.dst_row_stride = f.data_ptr(), f.stride(0)
+                it.spec = self._spec[b].data_ptr()
+                it.nrow, it.ncol, it.pad = x.shape[0], x.shape[1], \
+                    self._pad[b]
+                it.pair_offset = off
+                off += (x.shape[0] + 1) // 2
+            dev_tab = torch.frombuffer(bytearray(bytes(tab)),
+                                       dtype=torch.uint8).to(self.dev)
+            self._filter_groups.append((log2m, len(members), off, dev_tab,
+                                        self._tw[members[0]]))
         self.counter = torch.zeros(2, dtype=torch.int32, device=self.dev)
         self.graph = None
         self.updates = int(sum(r * c * c for r, c in shapes))
@@ -111,17 +133,21 @@ class BatchedFBP:
         self.nunits, self.units_dev = self._units[variant]
         self.graph = None
 
+    def launch_plan(self):
+        """The launches of one :meth:`launch`: one filter launch per FFT
+        length among the items, then the persistent back-projection."""
+        return [("atb_filter_rows_batch", log2m, n, pairs)
+                for log2m, n, pairs, _, _ in self._filter_groups] + \
+            [("atb_backproject_batch", self.n, self.nunits)]
+
     def launch(self, max_ctas=0):
-        """Filter every item, then one persistent back-projection launch."""
+        """Filter every item (one launch per FFT length), then one
+        persistent back-projection launch."""
         st = R._stream_ptr(self.dev)
-        for b in range(self.n):
-            x, f = self.inputs[b], self.filtered[b]
-            nrow, ncol = x.shape
-            nat.call("atb_filter_rows", x.data_ptr(), x.stride(0), 0, nrow, 1,
-                     ncol, self._pad[b], nat.PAD_MODES[self.pad_mode], 0,
-                     self._spec[b].data_ptr(), 1, self._tw[b].data_ptr(),
-                     self._log2m[b], f.data_ptr(), nat.F32, f.stride(0), 0,
-                     st)
+        for log2m, n, pairs, tab, tw in self._filter_groups:
+            nat.call("atb_filter_rows_batch", tab.data_ptr(), n, pairs,
+                     nat.PAD_MODES[self.pad_mode], 0, tw.data_ptr(), log2m,
+                     nat.F32, st)
         nat.call("atb_backproject_batch", self.items_dev.data_ptr(), self.n,
                  self.units_dev.data_ptr(), self.nunits,
                  self.counter.data_ptr(), int(max_ctas), self.variant, st)
@@ -153,17 +179,22 @@ class BatchedFBP:
 
 
 def uneven_batch_geometry(seed=3000, n_items=64, wmin=512, wmax=4096,
-                          amin=361, amax=3601, half_acq_every=8):
+                          amin=361, amax=3601, half_acq_every=8,
+                          axis_offset=0.3):
     """Seeded geometry of the uneven batch workload.
 
-    Widths log-uniform in [wmin, wmax], angle counts uniform in
+    Detector widths log-uniform in [wmin, wmax], angle counts uniform in
     [amin, amax] over [0, pi), centres jittered +/-3 px around the middle.
-    Every ``half_acq_every``-th item stands for a 360-degree half-acquisition
-    scan after its conversion to 180 degrees: the stitched sinogram is
-    1.6 x the width (rotation axis 0.3 of the width off the detector
-    centre, i.e. at 0.8 of the width from the left edge, mirrored), with
-    the angle count of the 180-degree half.  Returns a list of dicts with
-    nrow, ncol, center, angles, half_acquisition.
+    Every ``half_acq_every``-th item is a 360-degree half-acquisition scan
+    instead: 2 x the angle count over [0, 2 pi) on a detector of the drawn
+    width whose rotation axis sits ``axis_offset`` of the width right of
+    the detector centre (jittered +/-3 px), to be widened by
+    ``extend_sinogram`` (algotom/prep/conversion.py:395-454) before it is
+    batched.  An offset of 0.3 of the width gives an overlap of 0.4 of the
+    width and an extended width of 1.6 of it (2 ncol - overlap).  Returns a
+    list of dicts with nrow, ncol, center, angles, half_acquisition; for
+    the half-acquisition items also raw_ncol and raw_center (the detector
+    as scanned), and ncol / center are those of the extended sinogram.
     """
     rng = np.random.default_rng(seed)
     out = []
@@ -171,10 +202,48 @@ def uneven_batch_geometry(seed=3000, n_items=64, wmin=512, wmax=4096,
         w = int(round(np.exp(rng.uniform(np.log(wmin), np.log(wmax)))))
         nrow = int(rng.integers(amin, amax + 1))
         half = half_acq_every and (b % half_acq_every == half_acq_every - 1)
-        if half:
-            w = int(round(1.6 * w))
-        cen = (w - 1) / 2.0 + rng.uniform(-3.0, 3.0)
-        ang = np.linspace(0.0, np.pi, nrow, endpoint=False)
-        out.append(dict(nrow=nrow, ncol=w, center=cen, angles=ang,
-                        half_acquisition=bool(half)))
+        jitter = rng.uniform(-3.0, 3.0)
+        if not half:
+            out.append(dict(nrow=nrow, ncol=w, center=(w - 1) / 2.0 + jitter,
+                            angles=np.linspace(0.0, np.pi, nrow,
+                                               endpoint=False),
+                            half_acquisition=False))
+            continue
+        cor = (w - 1) / 2.0 + axis_offset * w + jitter
+        # extend_sinogram's geometry (conversion.py:425-454)
+        overlap = 2.0 * (w - cor) - 1.0
+        overlap_int = int(np.round(overlap + 1.0e-3))
+        nrow360 = 2 * nrow
+        out.append(dict(nrow=nrow360, ncol=2 * w - overlap_int,
+                        center=w - overlap_int / 2.0 - 0.5,
+                        angles=np.linspace(0.0, 2.0 * np.pi, nrow360,
+                                           endpoint=False),
+                        half_acquisition=True, raw_ncol=w, raw_center=cor))
     return out
+
+
+def batch_sinograms(geo, seed0=3000, device=None, photons=1e4):
+    """Seeded -log sinograms of :func:`uneven_batch_geometry` items on the
+    device, ready to batch: ellipse phantoms; half-acquisition items are
+    scanned over 360 degrees with the offset axis and widened with the
+    device ``extend_sinogram``.  Returns a list of float32 [nrow, ncol]
+    tensors."""
+    from .. import phantom
+    from ..prep.conversion import extend_sinogram
+    sinos = []
+    for k, g in enumerate(geo):
+        if g["half_acquisition"]:
+            raw, _, _, _ = phantom.half_acquisition_sinogram(
+                seed0 + k, g["nrow"], g["raw_ncol"], g["raw_center"],
+                photons=photons, device=device)
+            s, cor = extend_sinogram(raw, g["raw_center"], apply_log=False)
+            if abs(cor - g["center"]) > 1e-9 or s.shape[1] != g["ncol"]:
+                raise RuntimeError("extended geometry differs from the plan")
+        else:
+            s, _, _ = phantom.ellipse_sinogram(seed0 + k, g["nrow"],
+                                               g["ncol"], g["center"],
+                                               photons=photons,
+                                               angles=g["angles"],
+                                               device=device)
+        sinos.append(s)
+    return sinos

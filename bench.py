@@ -54,6 +54,9 @@ def _args():
     ap.add_argument("--slices", type=int, default=NSLICE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="leave the uneven-batch figure out of the default "
+                         "line (profiling runs)")
     ap.add_argument("--storage", default="float32",
                     choices=["float32", "float16", "bfloat16"],
                     help="element type of the filtered sinogram (stack)")
@@ -152,22 +155,24 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+TRAFFIC_PROFILE = "profiles/backproject_c2_16slices.md"
+
+
 def _traffic_per_update():
-    """DRAM bytes per update of the back-projection kernel, from the
-    committed ncu summary of the back-projector under profiles/ (its
-    `dram_bytes_per_update:` line), if present."""
-    d = os.path.join(ROOT, "profiles")
+    """DRAM bytes per update of the back-projection kernel as an ncu capture
+    measured them: the `dram_bytes_per_update:` line of the committed
+    summary TRAFFIC_PROFILE (dram__bytes_read.sum + dram__bytes_write.sum of
+    one launch on 16 slices, divided by its updates; the bench cannot read
+    DRAM counters itself).  Returns (bytes per update, the summary's
+    `build:` line) or (None, None)."""
     try:
-        names = sorted(os.listdir(d))
+        text = open(os.path.join(ROOT, TRAFFIC_PROFILE)).read()
     except OSError:
-        return None
-    for n in names:
-        if n.startswith("backproject") and n.endswith(".md"):
-            m = re.search(r"dram_bytes_per_update:\s*([0-9.eE+-]+)",
-                          open(os.path.join(d, n)).read())
-            if m:
-                return float(m.group(1))
-    return None
+        return None, None
+    m = re.search(r"dram_bytes_per_update:\s*([0-9.eE+-]+)", text)
+    b = re.search(r"build:\s*(.+)", text)
+    return (float(m.group(1)) if m else None,
+            b.group(1).strip() if b else None)
 
 
 def make_sinograms(nslice, device, seed0=2000):
@@ -184,33 +189,113 @@ def make_sinograms(nslice, device, seed0=2000):
     return out, ang
 
 
-def cpu_fbp_sample(nslice_max, budget_s, nthreads=None):
-    """Reference-arithmetic CPU FBP (oracle port) on a bounded slice sample."""
-    from algotom_b200 import phantom
+def _algotom():
+    """The unmodified reference (algotom) from its pip install under
+    baseline/_ref, or None.  Its pywt / h5py imports are unused on the FBP
+    path and are stubbed; Numba caches its kernels under the system temp
+    folder."""
+    import tempfile
+    import types
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "algotom")):
+        return None
+    try:
+        for m in ("pywt", "h5py"):
+            sys.modules.setdefault(m, types.ModuleType(m))
+        os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(
+            tempfile.gettempdir(), "algotom_numba_cache"))
+        sys.path.insert(0, ref)
+        import algotom.rec.reconstruction as rec
+        if not os.path.abspath(rec.__file__).startswith(ref):
+            return None
+        return rec
+    except Exception:  # noqa: BLE001
+        return None
+    finally:
+        if sys.path and sys.path[0] == ref:
+            sys.path.pop(0)
+
+
+def _fp64_fbp(sino, ang):
+    """FP64 FBP of one benchmark slice (the checker): the oracle's filter
+    and its C FP64 back-projector, circle mask, pi/(nrow-1)."""
     from oracle import cpu_port
+    from oracle import fbp_oracle as O
+    f = O.apply_ramp_filter(sino, None, "hann", 150, "edge")
+    ref = cpu_port.back_projection(f.astype(np.float32), ang, CENTER,
+                                   ref_arith=False)
+    return ref * O.make_circle_mask(NCOL, 1.0) * (np.pi / (NROW - 1))
+
+
+def cpu_fbp_sample(nslice_max, budget_s, nthreads=None, check=False):
+    """CPU FBP of up to ``nslice_max`` benchmark slices (at least one, more
+    while the time stays under ``budget_s``) on all host cores.
+
+    The reference itself when its install is present (``kind``
+    "reference": ``fbp_reconstruction(gpu=False)``, its Numba back-projector
+    parallel over angles, which races on the shared image, and its joblib
+    filter); otherwise the oracle's port of its arithmetic (``kind``
+    "port": numpy filter + the C back-projector, race-free).  Returns
+    (updates/s, slices, seconds, threads, kind, rel L2 of the first slice
+    against FP64 or None)."""
+    from algotom_b200 import phantom
     ang = np.linspace(0.0, np.pi, NROW, endpoint=False)
-    done, t_total = 0, 0.0
-    nt = nthreads or cpu_port.max_threads()
-    # warm the thread pool / FFT plans on a small case
-    cpu_port.fbp_reconstruction(np.ones((16, 1, 64), np.float32), 31.5,
-                                np.linspace(0, np.pi, 16), nthreads=nt)
+    rec = _algotom()
+    if rec is not None:
+        import numba
+        nt = numba.get_num_threads()
+        kind = "reference"
+
+        def fbp(s):
+            return rec.fbp_reconstruction(s, CENTER, angles=ang, ratio=1.0,
+                                          filter_name="hann",
+                                          apply_log=False, gpu=False)
+        warm = np.ones((16, 64), np.float32)  # compile Numba's kernels
+        rec.fbp_reconstruction(warm, 31.5, angles=np.linspace(0, np.pi, 16),
+                               apply_log=False, gpu=False)
+    else:
+        from oracle import cpu_port
+        nt = nthreads or cpu_port.max_threads()
+        kind = "port"
+
+        def fbp(s):
+            return cpu_port.fbp_reconstruction(s[:, None, :], CENTER, ang,
+                                               nthreads=nt)[:, 0, :]
+        cpu_port.fbp_reconstruction(np.ones((16, 1, 64), np.float32), 31.5,
+                                    np.linspace(0, np.pi, 16), nthreads=nt)
+    done, t_total, err = 0, 0.0, None
     while done < 1 or (done < nslice_max and t_total < budget_s):
         s, _, _ = phantom.ellipse_sinogram(2000 + done, NROW, NCOL, CENTER,
                                            photons=PHOTONS, angles=ang)
         t0 = time.perf_counter()
-        cpu_port.fbp_reconstruction(s[:, None, :], CENTER, ang, nthreads=nt)
+        r = fbp(s)
         t_total += time.perf_counter() - t0
+        if check and done == 0:
+            from oracle import fbp_oracle as O
+            err = O.rel_l2(np.asarray(r, np.float64), _fp64_fbp(s, ang))
         done += 1
     ups = done * NCOL * NCOL * NROW / t_total
-    return ups, done, t_total, nt
+    return ups, done, t_total, nt, kind, err
+
+
+def _cpu_sample_text(kind, done, t=None):
+    what = ("algotom's own fbp_reconstruction(gpu=False) from baseline/_ref "
+            "(Numba back-projector parallel over angles, joblib filter)"
+            if kind == "reference" else
+            "numpy filter + C back-projection with the reference's "
+            "arithmetic (port; the reference install is absent)")
+    return "%d of 256 slices (1801 x 2560)%s: %s" % (
+        done, "" if t is None else ", %.1f s" % t, what)
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
-    steps = []
+    steps, err, kind, nt = [], None, None, 0
     for i in range(args.warmup + args.steps):
-        ups, done, t, nt = cpu_fbp_sample(1, 0.0)
+        ups, done, t, nt, kind, e = cpu_fbp_sample(1, 0.0, check=(i == 0))
+        if e is not None:
+            err = e
         if i >= args.warmup:
             steps.append(t)
     t_step = statistics.mean(steps)
@@ -224,11 +309,14 @@ def run_reference(args, rank):
         "config": {"workload": WORKLOAD, "slices": NSLICE, "nrow": NROW,
                    "ncol": NCOL, "sample": "1 slice per step"},
         "slices_per_s": 1.0 / t_step,
+        "accuracy": {"rel_l2_vs_fp64": err, "slices_checked": 1,
+                     "note": "all-core run: the reference's back-projector "
+                             "races on its shared image"
+                             if kind == "reference" else "port, race-free"},
         "cpu_baseline": {"value": ups, "unit": "updates/s", "cores": nt,
-                         "kind": "port",
-                         "sample": "1 of 256 slices per step (1801 x 2560): "
-                                   "numpy filter + C back-projection with "
-                                   "the reference's arithmetic"},
+                         "kind": kind,
+                         "sample": "1 slice per step; " + _cpu_sample_text(
+                             kind, 1)},
         "e2e": {"value": ups, "unit": "updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -358,12 +446,15 @@ def run_ours(args, rank, world, local_rank):
                                         / np.abs(ref).max()),
                "slices_checked": 1}
         if world == 1:
-            ups, done, t, nt = cpu_fbp_sample(8, 15.0)
+            ups, done, t, nt, kind, e = cpu_fbp_sample(8, 15.0, check=True)
             cpu = {"value": ups, "unit": "updates/s", "cores": nt,
-                   "kind": "port",
-                   "sample": "%d of 256 slices (1801 x 2560), %.1f s: numpy "
-                             "filter + C back-projection with the "
-                             "reference's arithmetic" % (done, t)}
+                   "kind": kind, "rel_l2_vs_fp64": e,
+                   "sample": _cpu_sample_text(kind, done, t)}
+
+    # the uneven batch workload (one persistent launch under a CUDA graph):
+    # the batched back-projector's own roofline in the same line
+    batch = None if args.no_batch else batch_measure(
+        64, steps=3, warmup=3, check=not args.no_oracle)
 
     peaks, src = _peaks()
     f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
@@ -372,7 +463,7 @@ def run_ours(args, rank, world, local_rank):
     bp_upd = nslice * NCOL * NCOL * NROW
     achieved = FLOP_PER_UPDATE * bp_upd / t_bp / 1e12
     smem_achieved = SMEM_BYTES_PER_UPDATE * bp_upd / t_bp / 1e9
-    tpu = _traffic_per_update()
+    tpu, tbuild = _traffic_per_update()
     filt_bytes = NROW * nslice * NCOL * 8.0
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s",
@@ -394,8 +485,12 @@ def run_ours(args, rank, world, local_rank):
                      "updates_per_s": bp_upd / t_bp,
                      "ms_per_launch": t_bp * 1e3,
                      "peak_source": "shared-memory delivery, 128 B/clk x 148 "
-                                    "SM x sm_max_mhz (%s); traffic = DRAM "
-                                    "bytes per launch" % src},
+                                    "SM x sm_max_mhz (%s)" % src,
+                     "traffic_source": ("ncu dram__bytes_read.sum + "
+                                        "dram__bytes_write.sum per update "
+                                        "from %s (%s), times this launch's "
+                                        "updates" % (TRAFFIC_PROFILE, tbuild)
+                                        if tpu else None)},
         "fp32_roofline": {"bound": "fp32", "achieved": achieved,
                           "peak": fp32_peak, "unit": "TFLOP/s",
                           "frac": achieved / fp32_peak,
@@ -411,86 +506,82 @@ def run_ours(args, rank, world, local_rank):
                             "ms_per_launch": t_filt * 1e3},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "batch": batch,
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args):
-    """64 uneven sinograms (widths 512-4096 log-uniform, 361-3601 angles,
-    every 8th a stitched half-acquisition), filter + persistent
-    back-projection replayed from a captured CUDA graph."""
+def batch_measure(n_items=64, steps=3, warmup=3, check=True):
+    """The uneven batch workload: 64 sinograms (widths 512-4096
+    log-uniform, 361-3601 angles over [0, pi); every 8th a 360-degree
+    half-acquisition scan, axis 0.3 of the width off centre, widened by the
+    device extend_sinogram to ~1.6x with twice the angles), filter +
+    persistent back-projection replayed from a captured CUDA graph.
+    Returns a dict: replay time, the persistent back-projection alone
+    (CUDA events on its stream) and its shared-memory roofline, and the
+    FP64-oracle error of the narrowest item."""
     import torch
-    from algotom_b200 import phantom
+    from algotom_b200 import _native as nat
     from algotom_b200.rec import batch as B
+    from algotom_b200.rec import reconstruction as R
     dev = torch.device("cuda", 0)
-    geo = B.uneven_batch_geometry(n_items=args.items)
-    sinos = []
-    for k, g in enumerate(geo):
-        s, _, _ = phantom.ellipse_sinogram(3000 + k, g["nrow"], g["ncol"],
-                                           g["center"], photons=1e4,
-                                           angles=g["angles"], device=dev)
-        sinos.append(s)
+    geo = B.uneven_batch_geometry(n_items=n_items)
+    sinos = B.batch_sinograms(geo, device=dev)
     bf = B.BatchedFBP([(g["nrow"], g["ncol"]) for g in geo],
                       [g["center"] for g in geo], [g["angles"] for g in geo])
     for x, s in zip(bf.inputs, sinos):
         x.copy_(s)
     bf.capture()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bf.replay()
+    st = torch.cuda.current_stream(dev)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), \
         torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
+    e0.record(st)
+    for _ in range(steps):
         bf.replay()
-    e1.record()
+    e1.record(st)
     torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / 1e3 / args.steps
-    # the persistent back-projection alone, on the stream it launches on
-    from algotom_b200 import _native as nat
-    from algotom_b200.rec import reconstruction as R
-    st = torch.cuda.current_stream(dev)
+    t = e0.elapsed_time(e1) / 1e3 / steps
     b0, b1 = torch.cuda.Event(enable_timing=True), \
         torch.cuda.Event(enable_timing=True)
     b0.record(st)
-    for _ in range(args.steps):
+    for _ in range(steps):
         nat.call("atb_backproject_batch", bf.items_dev.data_ptr(), bf.n,
                  bf.units_dev.data_ptr(), bf.nunits, bf.counter.data_ptr(), 0,
                  bf.variant, R._stream_ptr(dev))
     b1.record(st)
     torch.cuda.synchronize()
-    t_bp = b0.elapsed_time(b1) / 1e3 / args.steps
+    t_bp = b0.elapsed_time(b1) / 1e3 / steps
     peaks, src = _peaks()
     f_clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
     smem_peak = SMEM_BYTES_PER_CLK_PER_SM * N_SM * f_clk / 1e9
     smem_achieved = SMEM_BYTES_PER_UPDATE * bf.updates / t_bp / 1e9
     err = None
-    if not args.no_oracle:
+    if check:
         from oracle import fbp_oracle as O
         k = min(range(len(geo)), key=lambda i: geo[i]["ncol"])
         ref = O.fbp_reconstruction(sinos[k].cpu().numpy(), geo[k]["center"],
                                    angles=geo[k]["angles"], apply_log=False)
-        from algotom_b200.rec import reconstruction as RR
-        single = RR.fbp_reconstruction(sinos[k], geo[k]["center"],
-                                       angles=geo[k]["angles"],
-                                       apply_log=False)
+        single = R.fbp_reconstruction(sinos[k], geo[k]["center"],
+                                      angles=geo[k]["angles"],
+                                      apply_log=False)
         got = bf.outputs[k].cpu().numpy()
         err = {"rel_l2": O.rel_l2(got, ref),
                "rel_l2_vs_single_slice_path": O.rel_l2(got,
                                                        single.cpu().numpy()),
                "item": k, "ncol": geo[k]["ncol"]}
-    print(json.dumps({
-        "metric": "batched uneven FBP pixel-angle updates/s",
-        "value": bf.updates / t, "unit": "updates/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
-        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "%d uneven sinograms, one persistent launch "
-                               "under a CUDA graph" % len(geo),
-                   "items": len(geo),
-                   "tile_variant": bf.variant, "units": bf.nunits,
-                   "updates": bf.updates},
+    half = [g for g in geo if g["half_acquisition"]]
+    out = {
+        "updates_per_s": bf.updates / t, "ms_per_replay": t * 1e3,
+        "items": len(geo), "updates": bf.updates, "tile_variant": bf.variant,
+        "units": bf.nunits,
+        "widths": [min(g["ncol"] for g in geo), max(g["ncol"] for g in geo)],
+        "angles": [min(g["nrow"] for g in geo), max(g["nrow"] for g in geo)],
+        "half_acquisition_items": len(half),
         "roofline": {"bound": "smem", "kernel": "bp_batch_kernel",
                      "achieved": smem_achieved, "peak": smem_peak,
                      "unit": "GB/s", "frac": smem_achieved / smem_peak,
@@ -499,8 +590,32 @@ def run_batch(args):
                      "ms_per_launch": t_bp * 1e3,
                      "peak_source": "shared-memory delivery, 128 B/clk x 148 "
                                     "SM x sm_max_mhz (%s)" % src},
-        "gpu_launches": (bf.n + 1) * args.steps + args.steps,
-        "accuracy": err}), flush=True)
+        "gpu_launches_per_replay": len(bf.launch_plan()),
+        "accuracy": err}
+    del bf, sinos
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_batch(args):
+    """The uneven batch workload alone (see batch_measure)."""
+    r = batch_measure(args.items, args.steps, args.warmup,
+                      check=not args.no_oracle)
+    print(json.dumps({
+        "metric": "batched uneven FBP pixel-angle updates/s",
+        "value": r["updates_per_s"], "unit": "updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms_per_replay"], "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "%d uneven sinograms, one persistent launch "
+                               "under a CUDA graph" % r["items"],
+                   "items": r["items"], "tile_variant": r["tile_variant"],
+                   "units": r["units"], "updates": r["updates"],
+                   "widths": r["widths"], "angles": r["angles"],
+                   "half_acquisition_items": r["half_acquisition_items"]},
+        "roofline": r["roofline"],
+        "gpu_launches": (r["gpu_launches_per_replay"] + 1) * args.steps,
+        "accuracy": r["accuracy"]}), flush=True)
 
 
 def run_autograd(args):

@@ -104,6 +104,40 @@ int atb_filter_rows(const float *src, int64_t src_row_stride,
                     int64_t dst_slice_stride, void *stream);
 
 /*
+ * One single-slice sinogram of a batched filter launch (device pointers
+ * inside).  pair_offset: index of its first row pair in the launch (the
+ * running sum of (nrow + 1) / 2 over the items before it).
+ */
+typedef struct {
+  const float *src;         /* [nrow][ncol] */
+  int64_t src_row_stride;
+  void *dst;                /* [nrow][ncol] of the launch's dst_dtype */
+  int64_t dst_row_stride;
+  const void *spec;         /* as atb_filter_rows, spec_rows = 1 */
+  int nrow;
+  int ncol;
+  int pad;
+  int pair_offset;
+} atb_filter_item;
+
+/*
+ * atb_filter_rows over a batch of single-slice sinograms of uneven width
+ * and angle count that share the FFT length 2^log2m, in ONE launch: CTA p
+ * filters row pair p - pair_offset of the item whose pair range holds p.
+ * The uneven-batch counterpart of the reference's per-slice filtering
+ * (reconstruction.py:460-475); no counterpart of the batching itself.
+ *
+ *   items     DEVICE array [nitems], ordered by pair_offset (0 first)
+ *   npairs    total row pairs (sum of (nrow + 1) / 2)
+ *   pad_mode, apply_log, twiddle, log2m, dst_dtype as atb_filter_rows;
+ *             every item needs 2^log2m >= ncol + 2 pad + ncol - 1
+ */
+int atb_filter_rows_batch(const atb_filter_item *items, int nitems,
+                          int npairs, int pad_mode, int apply_log,
+                          const void *twiddle, int log2m, int dst_dtype,
+                          void *stream);
+
+/*
  * Elementwise -log of a float32 sinogram stack, values <= 0 read as 1;
  * the BPF pre-step (reconstruction.py:632-637).  dst may equal src.
  */

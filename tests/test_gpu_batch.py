@@ -78,8 +78,76 @@ def test_uneven_geometry_is_seeded():
     assert [(d["nrow"], d["ncol"]) for d in g1] == \
         [(d["nrow"], d["ncol"]) for d in g2]
     assert len(g1) == 64
-    assert all(361 <= d["nrow"] <= 3601 for d in g1)
     assert sum(d["half_acquisition"] for d in g1) == 8
+    for k, d in enumerate(g1):
+        half = k % 8 == 7
+        assert d["half_acquisition"] == half
+        if not half:
+            assert 361 <= d["nrow"] <= 3601 and 512 <= d["ncol"] <= 4096
+            assert abs(d["center"] - (d["ncol"] - 1) / 2) <= 3.0
+            continue
+        # 360 degrees at twice the angle count, axis 0.3 of the width
+        # right of the detector centre, widened by extend_sinogram
+        w, cor = d["raw_ncol"], d["raw_center"]
+        assert 722 <= d["nrow"] <= 7202 and d["nrow"] % 2 == 0
+        assert abs(d["angles"][1] - d["angles"][0] - 2 * np.pi / d["nrow"]) \
+            < 1e-12
+        assert abs(cor - ((w - 1) / 2 + 0.3 * w)) <= 3.0
+        ov = int(np.round(2 * (w - cor) - 1 + 1e-3))
+        assert d["ncol"] == 2 * w - ov and 1.55 * w < d["ncol"] < 1.65 * w
+        assert d["center"] == w - ov / 2.0 - 0.5
+
+
+def test_half_acquisition_item_reconstructs_the_object(cuda):
+    """A generated 360-degree offset-axis scan, widened on the device by
+    extend_sinogram and reconstructed over 360 degrees, shows the phantom
+    (the generator, the extension and the batch geometry agree)."""
+    w, cor, nrow = 300, 299 / 2 + 0.3 * 300, 720
+    raw, ang, params, field = phantom.half_acquisition_sinogram(
+        7, nrow, w, cor, photons=None)
+    from algotom_b200.prep.conversion import extend_sinogram
+    ext, c2 = extend_sinogram(raw, cor, apply_log=False)
+    assert ext.shape[1] == field or abs(ext.shape[1] - field) <= 1
+    rec = R.fbp_reconstruction(ext, c2, angles=ang, apply_log=False)
+    n = ext.shape[1]
+    truth = phantom.phantom_image(params, n)
+    mask = O.make_circle_mask(n, 0.9)
+    assert O.rel_l2(rec * mask, truth * mask) < 0.35
+
+
+def test_full_uneven_batch_against_oracle(cuda):
+    """The 64-item workload (widths 512-4096 and half-acquisition items
+    widened to ~1.6x, 361-7202 angles) in one persistent launch: the
+    narrowest and the widest item against the FP64 oracle, every item
+    against the single-slice path."""
+    geo = B.uneven_batch_geometry()
+    sinos = B.batch_sinograms(geo, device=cuda)
+    bf = B.BatchedFBP([(g["nrow"], g["ncol"]) for g in geo],
+                      [g["center"] for g in geo], [g["angles"] for g in geo])
+    for x, s in zip(bf.inputs, sinos):
+        x.copy_(s)
+    bf.capture()
+    bf.replay()
+    torch.cuda.synchronize()
+    widths = [g["ncol"] for g in geo]
+    for k in (int(np.argmin(widths)), int(np.argmax(widths))):
+        g = geo[k]
+        sn = sinos[k].cpu().numpy()
+        f = O.apply_ramp_filter(sn, None, "hann", min(int(0.15 * g["ncol"]),
+                                                      150), "edge")
+        from oracle import cpu_port
+        ref = cpu_port.back_projection(f.astype(np.float32), g["angles"],
+                                       g["center"], ref_arith=False)
+        ref = ref * O.make_circle_mask(g["ncol"], 1.0) * \
+            (np.pi / (g["nrow"] - 1))
+        err = O.rel_l2(bf.outputs[k].cpu().numpy(), ref)
+        assert err < 1e-5, (k, g["ncol"], g["nrow"], err)
+    for k in range(0, len(geo), 5):
+        g = geo[k]
+        single = R.fbp_reconstruction(sinos[k], g["center"],
+                                      angles=g["angles"], apply_log=False)
+        assert O.rel_l2(bf.outputs[k].cpu().numpy(),
+                        single.cpu().numpy()) < 1e-5, k
 
 
 @pytest.mark.parametrize("variant", [0, 1])
