@@ -113,6 +113,9 @@ struct BPArgs {
   int spacing;  // centre-group launches: slice m is centre center + m spacing
                 // of the one sinogram (sss = 0)
   int slope;  // back-project the interpolant's slope D_j instead of its value
+  int wait_polls;  // polls before a staging wait gives up (kWaitPolls)
+  int inject;      // test only: CTA (0, 0, 0) arms its first staging wait
+                   // for 16 bytes more than its copies deliver
 };
 
 struct __align__(16) AngleParam {
@@ -254,9 +257,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned by
 }
 // waits for the phase of the given parity to complete; false if it has not
 // after kWaitPolls polls
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int polls) {
   const uint32_t addr = smem_u32(bar);
-  for (int n = 0; n < kWaitPolls; ++n) {
+  for (int n = 0; n < polls; ++n) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -483,7 +486,9 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
         const int lo = lo_s[buf][tid];
         const int base = (lo / kV - (lo % kV < 0)) * kV;  // a 16-byte multiple, as TMA requires
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&raw_bar, (unsigned)(kGroup ? seglen * (int)sizeof(T) : K::kBoxBytes));
+        unsigned bytes = (unsigned)(kGroup ? seglen * (int)sizeof(T) : K::kBoxBytes);
+        if (a.inject && k == 0 && tid == 0 && bx == 0 && by == 0 && bz == 0) bytes += 16u;
+        mbar_arrive_expect_tx(&raw_bar, bytes);
         tma_load_3d(raw + (size_t)tid * K::kRawSlot, tmap, base, kGroup ? 0 : slice0, it, &raw_bar);
       } else {
         mbar_arrive(&raw_bar);
@@ -629,7 +634,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
   __syncthreads();
   issue_raw(0, 0);
   bool late = false;
-  if (use_tma) late = !mbar_wait(&raw_bar, 0u);
+  if (use_tma) late = !mbar_wait(&raw_bar, 0u, a.wait_polls);
   else cp_async_wait_all();
   __syncthreads();
   if (nchunk > 1) params(1, 1);
@@ -774,7 +779,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     if (k + 1 < nchunk) {
       late = false;
       if (use_tma) {
-        late = !mbar_wait(&raw_bar, (unsigned)((k + 1) & 1));
+        late = !mbar_wait(&raw_bar, (unsigned)((k + 1) & 1), a.wait_polls);
       } else {
         cp_async_wait_all();
         __syncthreads();  // every thread's copies landed
@@ -793,7 +798,7 @@ __device__ __forceinline__ void bp_tile(const BPArgs &a, int bx, int by, int bz,
     // a window load never completed: record it, give that copy one more
     // bounded wait, and leave without writing this tile
     if (tid == 0) atomicOr(&g_bp_status, 1);
-    mbar_wait(&raw_bar, (unsigned)(pending & 1));
+    mbar_wait(&raw_bar, (unsigned)(pending & 1), a.wait_polls);
     return;
   }
   if constexpr (!kPerAngleKahan) {
@@ -880,6 +885,8 @@ __global__ void __launch_bounds__(BPCfg<T, 1, V>::kThreads, BPCfg<T, 1, V>::kMin
     a.center = it.center; a.edge_pad = it.edge_pad; a.mask_r2 = it.mask_r2; a.scale = it.scale;
     a.out = it.out; a.ors = it.out_row_stride; a.oss = 0;
     a.slope = 0;
+    a.wait_polls = kWaitPolls;
+    a.inject = 0;
     a.vec16 = sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(it.sino) % 16) == 0 &&
               it.sino_row_stride % 4 == 0 && it.ncol % 4 == 0;
     a.tma = 0;
@@ -1005,6 +1012,10 @@ extern "C" int atb_backproject(const void *sino, int sino_dtype, int64_t sino_ro
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride;
   a.slope = (flags >> 1) & 1;
   a.tma = !((flags >> 4) & 1);
+  // bit 5 (tests): make the first CTA's first staging wait run out, with
+  // every copy complete, after a short limit
+  a.inject = (flags >> 5) & 1;
+  a.wait_polls = a.inject ? 4096 : kWaitPolls;
   a.spacing = 0;
   {
     const int ve = sino_dtype == ATB_F32 ? 4 : 8;  // elements per 16-byte vector
@@ -1064,6 +1075,8 @@ extern "C" int atb_backproject_centers(const float *sino, int64_t sino_row_strid
   a.out = out; a.ors = out_row_stride; a.oss = out_center_stride;
   a.slope = 0;
   a.tma = !((flags >> 4) & 1);
+  a.inject = 0;
+  a.wait_polls = kWaitPolls;
   a.spacing = spacing;
   a.vec16 = (reinterpret_cast<uintptr_t>(sino) % 16) == 0 && sino_row_stride % 4 == 0 && ncol % 4 == 0;
   cudaStream_t st = atb::as_stream(stream);

@@ -238,8 +238,9 @@ class _Source:
         if items:
             keep = _backproject_items(items, dev, 1 if ncol <= 512 else 0)
         if not fbp:
-            out = R._circular_filter(out, None, self.filter_name, self.pad,
-                                     "edge")
+            v = out.permute(1, 0, 2)  # [y, candidate, x], filtered in place
+            R._circular_filter(v, None, self.filter_name, self.pad, "edge",
+                               out=v)
             idx = torch.arange(ncol, device=dev) - ncol // 2
             d2 = (idx[None, :] ** 2 + idx[:, None] ** 2).to(torch.float64)
             for k, c in enumerate(centers):

@@ -180,7 +180,13 @@ int atb_neg_log(const float *src, int64_t src_row_stride,
  *            autotuner; stacks of 2 or more slices always use 64 x 32 tiles);
  *            bit 4: stage the detector windows with cp.async even where
  *            TMA box loads are used by default (CTAs of 2 or 4 slices with a
- *            16-byte aligned base, strides and row length); same results
+ *            16-byte aligned base, strides and row length); same results;
+ *            bit 5 (tests of the bounded waits only): the first CTA of a
+ *            TMA-staged launch arms its first window wait for 16 bytes more
+ *            than its copies deliver, and every wait gives up after 4096
+ *            polls instead of about 2^20.  That wait then runs out with every
+ *            copy complete: the CTA sets bit 0 of atb_backproject_status
+ *            and leaves its tile unwritten; the other tiles are unaffected
  */
 int atb_backproject(const void *sino, int sino_dtype, int64_t sino_row_stride,
                     int64_t sino_slice_stride, int nrow, int nslice, int ncol,
