@@ -350,17 +350,42 @@ def _slab_spans(nslice, slab):
     return spans
 
 
+def _resume_key(shape, center, angles, mask_r2, scale, ramp_win,
+                filter_name, pad, pad_mode, apply_log, storage, kahan, slab):
+    """What defines a streamed reconstruction's result, for its manifest."""
+    import hashlib
+    ang = np.ascontiguousarray(np.float32(angles)).tobytes()
+    win = None
+    if ramp_win is not None:
+        w = ramp_win.cpu().numpy() if isinstance(ramp_win, torch.Tensor) \
+            else np.asarray(ramp_win)
+        win = hashlib.sha1(np.ascontiguousarray(w).tobytes()).hexdigest()
+    return {"shape": [int(v) for v in shape],
+            "center": float(np.float32(center)),
+            "angles_sha1": hashlib.sha1(ang).hexdigest(),
+            "mask_r2": float(mask_r2), "scale": float(scale),
+            "ramp_win_sha1": win, "filter_name": filter_name,
+            "pad": int(pad), "pad_mode": pad_mode,
+            "apply_log": bool(apply_log), "storage": storage,
+            "kahan": kahan, "slab": int(slab)}
+
+
 def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
                   pad, pad_mode, apply_log, out_host, storage, kahan,
-                  slab=SLAB):
+                  slab=SLAB, manifest=None):
     """FBP of a host stack [nrow, nslice, ncol] streamed through the device
     in slabs of up to ``slab`` slices (ramped at both ends): while slab k is
     filtered and back-projected, slab k+1 is copied in and slab k-1 copied
-    out (one copy stream each way, double-buffered, ordered by events)."""
+    out (one copy stream each way, double-buffered, ordered by events).
+    With a :class:`~algotom_b200.rec.resume.SlabManifest`, slabs it lists
+    are skipped and every slab whose copy-out has completed is recorded."""
     nrow, nslice, ncol = host.shape
     dev = _device()
     k_sl = max(1, min(slab, nslice))
     spans = _slab_spans(nslice, k_sl)
+    if manifest is not None:
+        spans = [sp for sp in spans if not manifest.is_done(sp)]
+    pending = []  # (copy-out event, span) not yet recorded as finished
     cmp = torch.cuda.current_stream(dev)
     s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     in_buf = [torch.empty((nrow, k_sl, ncol), dtype=torch.float32, device=dev)
@@ -381,6 +406,10 @@ def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
     cmp.synchronize()
     for k, (k0, kk) in enumerate(spans):
         b = k % 2
+        if manifest is not None and pending:
+            fin = [sp for ev, sp in pending if ev.query()]
+            pending = [(ev, sp) for ev, sp in pending if not ev.query()]
+            manifest.mark(fin)
         if k >= 2:
             s_in.wait_event(ev_in_free[b])
         nat.call("atb_copy_2d", in_buf[b].data_ptr(), slab_b, hp + k0 * ncol * 4,
@@ -400,9 +429,15 @@ def _fbp_streamed(host, center, angles, mask_r2, scale, ramp_win, filter_name,
         nat.call("atb_copy_2d", op + k0 * ncol * 4, row_b, out_buf[b].data_ptr(),
                  slab_b, kk * ncol * 4, ncol, 1, s_out.cuda_stream)
         ev_out_free[b].record(s_out)
+        if manifest is not None:
+            done = torch.cuda.Event()
+            done.record(s_out)
+            pending.append((done, (k0, kk)))
         del f
     s_out.synchronize()
     s_in.synchronize()
+    if manifest is not None:
+        manifest.mark([sp for _, sp in pending])
     return out_host
 
 
@@ -410,7 +445,7 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
                        ramp_win=None, filter_name="hann", pad=None,
                        pad_mode="edge", apply_log=True, gpu=True,
                        block=(16, 16), ncore=None, *, out=None,
-                       storage="float32", kahan="chunk"):
+                       storage="float32", kahan="chunk", resume=None):
     """FBP of a 2-D [nrow, ncol] or 3-D [nrow, nslice, ncol] sinogram.
 
     Drop-in for ``algotom.rec.reconstruction.fbp_reconstruction``
@@ -419,6 +454,11 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
     without edge padding, circle mask (``ratio``; 0.0 picks the largest disc
     inside the centred field), scale pi/(nrow-1).  Returns float32
     [ncol, ncol] or [ncol, nslice, ncol].
+
+    ``resume`` (a file path; host stacks with a persistent ``out``, e.g. a
+    ``numpy.memmap``): record every finished slab in that JSON manifest and
+    skip the slabs it already lists, so a run cut short is completed by
+    calling again with the same arguments (``rec/resume.py``).
     """
     nrow, nslice, ncol, angles = _validate(sinogram, center, angles)
     if apply_log:
@@ -426,6 +466,10 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
     if pad is None:
         pad = min(int(0.15 * ncol), 150)
     on_host = not (isinstance(sinogram, torch.Tensor) and sinogram.is_cuda)
+    if resume is not None and not (on_host and len(sinogram.shape) == 3
+                                   and out is not None):
+        raise ValueError("resume needs a host 3-D stack and a persistent "
+                         "out array that holds the finished slices")
     if on_host and len(sinogram.shape) == 3:
         # host stack: stream slabs through the device, overlapping copies
         host = _host_tensor(sinogram)
@@ -439,9 +483,16 @@ def fbp_reconstruction(sinogram, center, angles=None, ratio=1.0,
                     res.dtype != torch.float32 or not res.is_contiguous():
                 raise ValueError("out must be a C-contiguous float32 array "
                                  "of shape %s" % ((ncol, nslice, ncol),))
+        manifest = None
+        if resume is not None:
+            from .resume import SlabManifest
+            manifest = SlabManifest.open(str(resume), _resume_key(
+                host.shape, center, angles, _mask_r2(ratio, center, ncol),
+                _scale(nrow), ramp_win, filter_name, pad, pad_mode,
+                apply_log, storage, kahan, SLAB))
         _fbp_streamed(host, center, angles, _mask_r2(ratio, center, ncol),
                       _scale(nrow), ramp_win, filter_name, pad, pad_mode,
-                      apply_log, res, storage, kahan)
+                      apply_log, res, storage, kahan, manifest=manifest)
         if out is not None:
             return out
         return res if isinstance(sinogram, torch.Tensor) else res.numpy()

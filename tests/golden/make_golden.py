@@ -1,9 +1,10 @@
 """Generate golden input/output vectors by running the reference itself.
 
-Run in a container that has the algotom 1.6.0 source tree (default
-``/root/reference``, or ``$ALGOTOM_REF``) plus numpy/scipy/numba/joblib:
+Run where the algotom 1.6.0 source tree is available, with
+``$ALGOTOM_REF`` naming its root (the directory that holds ``algotom/``),
+plus numpy/scipy/numba/joblib:
 
-    python tests/golden/make_golden.py
+    ALGOTOM_REF=/path/to/algotom python tests/golden/make_golden.py
 
 The reference imports ``pywt`` and ``h5py`` at module level
 (``algotom/util/utility.py:58``, ``algotom/io/loadersaver.py:44``); neither is
@@ -28,7 +29,11 @@ import numpy as np  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("ALGOTOM_REF", "/root/reference")
+REF = os.environ.get("ALGOTOM_REF")
+if not REF or not os.path.isdir(os.path.join(REF, "algotom")):
+    sys.exit("make_golden.py: set ALGOTOM_REF to the root of the algotom "
+             "1.6.0 source tree (the directory that holds algotom/); got %r"
+             % (REF,))
 
 for _m in ("pywt", "h5py"):
     sys.modules.setdefault(_m, types.ModuleType(_m))
