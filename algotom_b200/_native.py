@@ -24,7 +24,10 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_log2m",
            "atb_vertical_workspace", "atb_flat_log", "atb_shift_rows",
            "atb_extend_rows", "atb_spline_prefilter", "atb_dfi_regrid",
            "atb_bpf_filter2d_length", "atb_bpf_filter2d_workspace",
-           "atb_bpf_filter2d", "atb_filter_rows_batch")
+           "atb_bpf_filter2d", "atb_filter_rows_batch", "atb_shift_rows_ext",
+           "atb_dfi_angle_stack", "atb_wrap_shift_rows", "atb_dfi_fft_length",
+           "atb_dfi_fft_setup", "atb_dfi_rows", "atb_dfi_inverse_workspace",
+           "atb_dfi_inverse")
 
 F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
@@ -131,6 +134,29 @@ _SIGS = {
         ctypes.c_int, ctypes.c_int, _vp]),
     "atb_dfi_regrid": (ctypes.c_int, [
         _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "atb_shift_rows_ext": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_double, _vp, _c_i64, _vp]),
+    "atb_dfi_angle_stack": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, _vp, _c_i64, _c_i64, _vp]),
+    "atb_wrap_shift_rows": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _c_i64, _c_i64,
+        _vp]),
+    "atb_dfi_fft_length": (ctypes.c_int, [ctypes.c_int]),
+    "atb_dfi_fft_setup": (ctypes.c_int, [
+        ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "atb_dfi_rows": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp,
+        _vp, _vp, _c_i64, _c_i64, _vp]),
+    "atb_dfi_inverse_workspace": (_c_i64, [
+        ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "atb_dfi_inverse": (ctypes.c_int, [
+        _vp, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+        ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp, _vp, _vp, _vp,
+        _vp, _c_i64, _c_i64, ctypes.c_int, _vp, _c_i64, _vp]),
     "atb_bpf_filter2d_length": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "atb_bpf_filter2d_workspace": (_c_i64, [ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int]),

@@ -37,6 +37,7 @@ struct RowArgs {
   const float *src;
   long long srs;
   int nrow, ncol;
+  int ncol_src;  // source columns (<= ncol); the rest repeat the last one
   int flip, apply_log;
   double shift;  // 0: no shift
   int ov, side;  // extend: overlap columns and side; ov == 0: plain shift
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
   const float *src = a.src + row * a.srs;
   for (int k = threadIdx.x; k < big; k += kThreads) {
     const int col = min(max(k - kPad, 0), n - 1);
-    float v = src[a.flip ? n - 1 - col : col];
+    float v = src[min(a.flip ? n - 1 - col : col, a.ncol_src - 1)];
     if (a.apply_log) v = -logf(v);
     x[k] = v;
   }
@@ -137,7 +138,7 @@ extern "C" int atb_shift_rows(const float *src, int64_t src_row_stride, int nrow
   if (ncol > kMaxCols) return atb::fail(ATB_ERANGE, "atb_shift_rows: ncol=%d > %d", ncol, kMaxCols);
   if (!std::isfinite(shift)) return atb::fail(ATB_EINVAL, "atb_shift_rows: shift is not finite");
   RowArgs a;
-  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol;
+  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol; a.ncol_src = ncol;
   a.flip = flip ? 1 : 0; a.apply_log = 0; a.shift = shift; a.ov = 0; a.side = 0;
   a.dst = dst; a.drs = dst_row_stride;
   return launch_rows(a, "atb_shift_rows", stream);
@@ -153,8 +154,22 @@ extern "C" int atb_extend_rows(const float *src, int64_t src_row_stride, int nro
     return atb::fail(ATB_EINVAL, "atb_extend_rows: overlap %d / side %d invalid for %d columns", overlap, side, ncol);
   if (!std::isfinite(shift)) return atb::fail(ATB_EINVAL, "atb_extend_rows: shift is not finite");
   RowArgs a;
-  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol;
+  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol; a.ncol_src = ncol;
   a.flip = 0; a.apply_log = apply_log ? 1 : 0; a.shift = shift; a.ov = overlap; a.side = side;
   a.dst = dst; a.drs = dst_row_stride;
   return launch_rows(a, "atb_extend_rows", stream);
+}
+
+extern "C" int atb_shift_rows_ext(const float *src, int64_t src_row_stride, int nrow, int ncol_src, int ncol,
+                                  double shift, float *dst, int64_t dst_row_stride, void *stream) {
+  if (!src || !dst) return atb::fail(ATB_EINVAL, "atb_shift_rows_ext: null pointer");
+  if (nrow < 1 || ncol_src < 1 || ncol < ncol_src)
+    return atb::fail(ATB_EINVAL, "atb_shift_rows_ext: bad shape %dx%d -> %d columns", nrow, ncol_src, ncol);
+  if (ncol > kMaxCols) return atb::fail(ATB_ERANGE, "atb_shift_rows_ext: ncol=%d > %d", ncol, kMaxCols);
+  if (!std::isfinite(shift)) return atb::fail(ATB_EINVAL, "atb_shift_rows_ext: shift is not finite");
+  RowArgs a;
+  a.src = src; a.srs = src_row_stride; a.nrow = nrow; a.ncol = ncol; a.ncol_src = ncol_src;
+  a.flip = 0; a.apply_log = 0; a.shift = shift; a.ov = 0; a.side = 0;
+  a.dst = dst; a.drs = dst_row_stride;
+  return launch_rows(a, "atb_shift_rows_ext", stream);
 }

@@ -23,6 +23,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "dfi_grid.cuh"
 #include "spline_fir.cuh"
 
 namespace {
@@ -120,34 +121,6 @@ __global__ void __launch_bounds__(kFirThreads)
   }
 }
 
-// centred quintic B-spline
-__device__ __forceinline__ double bspline5(double u) {
-  const double a = fabs(u);
-  if (a < 1.0) {
-    const double a2 = a * a;
-    return 11.0 / 20.0 - a2 / 2.0 + a2 * a2 / 4.0 - a2 * a2 * a / 12.0;
-  }
-  if (a < 2.0) {
-    const double a2 = a * a;
-    return 17.0 / 40.0 + 5.0 * a / 8.0 - 7.0 * a2 / 4.0 + 5.0 * a2 * a / 4.0 - 3.0 * a2 * a2 / 8.0 +
-           a2 * a2 * a / 24.0;
-  }
-  if (a < 3.0) {
-    const double b = 3.0 - a, b2 = b * b;
-    return b2 * b2 * b / 120.0;
-  }
-  return 0.0;
-}
-
-// half-sample symmetric index
-__device__ __forceinline__ int reflect_index(int i, int n) {
-  if (i >= 0 && i < n) return i;
-  const int p = 2 * n;
-  int r = i % p;
-  if (r < 0) r += p;
-  return r >= n ? p - 1 - r : r;
-}
-
 __global__ void __launch_bounds__(kGridThreads)
     regrid_kernel(const double2 *__restrict__ coef, int nrow, int w, double2 *__restrict__ out) {
   const long long e = blockIdx.x * (long long)kGridThreads + threadIdx.x;
@@ -155,50 +128,90 @@ __global__ void __launch_bounds__(kGridThreads)
   const int i = (int)(e / w), j = (int)(e - (long long)i * w);
   // written where ifftshift puts it: (i - w // 2, j - w // 2) mod w
   const long long oi = (i + w - w / 2) % w, oj = (j + w - w / 2) % w;
-  double2 *o = out + oi * w + oj;
-  // circle mask of make_circle_mask(w, 1.0): integer grid centred at w // 2
-  const long long cm = w / 2, dx = j - cm, dy = i - cm;
-  if (dx * dx + dy * dy > cm * cm) {
-    *o = make_double2(0.0, 0.0);
-    return;
+  out[oi * w + oj] = atb::dfi::regrid_point(coef, w, nrow, w, i, j);
+}
+
+// __dfi_handle_angles (reconstruction.py:731-749), first half: the fold of
+// a 360-degree scan (n = nrow_in / 2 + 1 rows, row r = (row r + row
+// nrow_in - n + r mirrored) / 2 in float32, as NumPy's float32 arithmetic)
+// and the stack the angle shift runs on, rows 0 .. n - 2 followed by all n
+// rows mirrored left-right, widened to float64 for the spline prefilter.
+// One thread per output sample.
+struct StackArgs {
+  const float *src;
+  long long srs, sss;
+  int nrow_in, n, ncol, fold;
+  double *dst;
+  long long drs, dss;
+};
+
+__global__ void __launch_bounds__(kGridThreads) angle_stack_kernel(StackArgs a) {
+  const int j = blockIdx.x * kGridThreads + threadIdx.x;
+  if (j >= a.ncol) return;
+  const int i = blockIdx.y, k = blockIdx.z;
+  int r = i, col = j;
+  if (i >= a.n - 1) {
+    r = i - (a.n - 1);
+    col = a.ncol - 1 - j;
   }
-  // generate_mapping_coordinate (height_rec = width_rec = width_sino = w)
-  const double xc = (w - 1.0) * 0.5;
-  const double rmax = floor(xc);
-  const double x = (double)(w - 1 - j) - xc, y = (double)i - xc;
-  float r = (float)fmin(fmax(sqrt(x * x + y * y), 0.0), rmax);
-  double th = M_PI + atan2(y, x);
-  if (th > M_PI) r = -r;
-  r = (float)fmin(fmax((double)r + rmax, 0.0), (double)(w - 1));
-  if (th > M_PI) th -= M_PI;
-  const float tf = (float)(th * (nrow - 1.0) / M_PI);
-  // quintic B-spline interpolation at (row tf, column r)
-  const double rr = (double)tf, cc = (double)r;
-  const int fr = (int)floor(rr) - 2, fc = (int)floor(cc) - 2;
-  double wr[6], wc[6];
-  int ir[6], ic[6];
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    wr[m] = bspline5(rr - (fr + m));
-    wc[m] = bspline5(cc - (fc + m));
-    ir[m] = reflect_index(fr + m, nrow);
-    ic[m] = reflect_index(fc + m, w);
+  const float *s = a.src + k * a.sss;
+  float v = __ldg(s + r * a.srs + col);
+  if (a.fold) v = (v + __ldg(s + (long long)(a.nrow_in - a.n + r) * a.srs + (a.ncol - 1 - col))) * 0.5f;
+  a.dst[i * a.drs + k * a.dss + j] = (double)v;
+}
+
+// second half: scipy.ndimage.shift(stack, (shift, 0), order=3,
+// mode="wrap")[:nout] from the stack's cubic B-spline coefficients along
+// the rows (whole-sample symmetric prefilter): the sample coordinate
+// i - shift wrapped into [0, m - 1] with period m - 1, four taps with
+// mirrored indices, rounded to float32; flip reverses rows and columns
+// (the flipud(fliplr(.)) of descending angles).
+struct WrapArgs {
+  const double *coef;
+  long long crs, css;
+  int m, ncol, nout, flip;
+  double shift;
+  float *dst;
+  long long drs, dss;
+};
+
+__device__ __forceinline__ double bspline3(double u) {
+  const double a = fabs(u);
+  if (a < 1.0) return 2.0 / 3.0 - a * a + a * a * a / 2.0;
+  if (a < 2.0) {
+    const double b = 2.0 - a;
+    return b * b * b / 6.0;
   }
-  double re = 0.0, im = 0.0;
+  return 0.0;
+}
+
+__global__ void __launch_bounds__(kGridThreads) wrap_shift_kernel(WrapArgs a) {
+  const int j = blockIdx.x * kGridThreads + threadIdx.x;
+  if (j >= a.ncol) return;
+  const int i = blockIdx.y, k = blockIdx.z, m = a.m;
+  double cc = (double)i - a.shift;
+  const double sz = (double)(m - 1);
+  if (m > 1) {
+    if (cc < 0.0) cc += sz * (floor(-cc / sz) + 1.0);
+    if (cc > sz) cc -= sz * floor(cc / sz);
+  }
+  const double f = floor(cc);
+  const int fi = (int)f;
+  const double *c = a.coef + k * a.css + j;
+  double v = 0.0;
 #pragma unroll
-  for (int a = 0; a < 6; ++a) {
-    const double2 *row = coef + (long long)ir[a] * w;
-    double sr = 0.0, si = 0.0;
-#pragma unroll
-    for (int b = 0; b < 6; ++b) {
-      const double2 v = row[ic[b]];
-      sr += wc[b] * v.x;
-      si += wc[b] * v.y;
+  for (int t = -1; t <= 2; ++t) {
+    int idx = 0;
+    if (m > 1) {
+      const int p = 2 * (m - 1);
+      int r = (fi + t) % p;
+      if (r < 0) r += p;
+      idx = r >= m ? p - r : r;
     }
-    re += wr[a] * sr;
-    im += wr[a] * si;
+    v += bspline3(cc - (double)(fi + t)) * __ldg(c + idx * a.crs);
   }
-  *o = make_double2(re, im);
+  const int oi = a.flip ? a.nout - 1 - i : i, oj = a.flip ? a.ncol - 1 - j : j;
+  a.dst[oi * a.drs + k * a.dss + oj] = (float)v;
 }
 
 }  // namespace
@@ -251,4 +264,39 @@ extern "C" int atb_dfi_regrid(const double *coef, int nrow, int width, double *o
   regrid_kernel<<<(int)((total + kGridThreads - 1) / kGridThreads), kGridThreads, 0, atb::as_stream(stream)>>>(
       reinterpret_cast<const double2 *>(coef), nrow, width, reinterpret_cast<double2 *>(out));
   return atb::check_launch("atb_dfi_regrid");
+}
+
+extern "C" int atb_dfi_angle_stack(const float *src, int64_t src_row_stride, int64_t src_slice_stride, int nrow_in,
+                                   int nslice, int ncol, int fold, double *dst, int64_t dst_row_stride,
+                                   int64_t dst_slice_stride, void *stream) {
+  if (!src || !dst) return atb::fail(ATB_EINVAL, "atb_dfi_angle_stack: null pointer");
+  if (nrow_in < 1 || nslice < 1 || ncol < 1 || nslice > 65535)
+    return atb::fail(ATB_EINVAL, "atb_dfi_angle_stack: bad shape %dx%dx%d", nrow_in, nslice, ncol);
+  StackArgs a;
+  a.src = src; a.srs = src_row_stride; a.sss = src_slice_stride;
+  a.nrow_in = nrow_in; a.n = fold ? nrow_in / 2 + 1 : nrow_in; a.ncol = ncol; a.fold = fold ? 1 : 0;
+  a.dst = dst; a.drs = dst_row_stride; a.dss = dst_slice_stride;
+  const int m = 2 * a.n - 1;
+  if (m > 65535) return atb::fail(ATB_ERANGE, "atb_dfi_angle_stack: %d rows > 65535", m);
+  const dim3 grid((ncol + kGridThreads - 1) / kGridThreads, m, nslice);
+  angle_stack_kernel<<<grid, kGridThreads, 0, atb::as_stream(stream)>>>(a);
+  return atb::check_launch("atb_dfi_angle_stack");
+}
+
+extern "C" int atb_wrap_shift_rows(const double *coef, int64_t coef_row_stride, int64_t coef_slice_stride, int m,
+                                   int nslice, int ncol, double shift, int nout, int flip, float *dst,
+                                   int64_t dst_row_stride, int64_t dst_slice_stride, void *stream) {
+  if (!coef || !dst) return atb::fail(ATB_EINVAL, "atb_wrap_shift_rows: null pointer");
+  if (m < 1 || nslice < 1 || ncol < 1 || nout < 1 || nout > m || nslice > 65535)
+    return atb::fail(ATB_EINVAL, "atb_wrap_shift_rows: bad shape m=%d nslice=%d ncol=%d nout=%d", m, nslice, ncol,
+                     nout);
+  if (!std::isfinite(shift) || std::fabs(shift) > 1e9)
+    return atb::fail(ATB_EINVAL, "atb_wrap_shift_rows: shift %g out of range", shift);
+  WrapArgs a;
+  a.coef = coef; a.crs = coef_row_stride; a.css = coef_slice_stride;
+  a.m = m; a.ncol = ncol; a.nout = nout; a.flip = flip ? 1 : 0; a.shift = shift;
+  a.dst = dst; a.drs = dst_row_stride; a.dss = dst_slice_stride;
+  const dim3 grid((ncol + kGridThreads - 1) / kGridThreads, nout, nslice);
+  wrap_shift_kernel<<<grid, kGridThreads, 0, atb::as_stream(stream)>>>(a);
+  return atb::check_launch("atb_wrap_shift_rows");
 }

@@ -207,3 +207,99 @@ __device__ double2 *run(double2 *a, double2 *b, const Plan &pl, const double2 *t
 
 }  // namespace fft
 }  // namespace atb
+
+namespace atb {
+namespace fft {
+
+// ---------------------------------------------------------------------------
+// In-place transforms of n = 2^m values (m <= 13) in one shared-memory
+// buffer, for lengths whose two Stockham buffers would not fit.  Radices 8,
+// then 4, then 2 (the sequence ip_radices gives).  The forward transform
+// decimates in frequency: the stage of radix r on blocks of length L takes,
+// for each n1 < L / r, the r values at n1 + j L / r, transforms them and
+// multiplies output k by w_L^(k n1), in place; its output is in digit-
+// reversed order.  The inverse runs the same stages in reverse order, each
+// undoing its forward twin (conjugate twiddles, then the inverse r-point
+// DFT), so it takes digit-reversed input to natural order, unnormalised.
+// A product of two forward outputs is therefore a circular convolution
+// after the inverse, with no reordering pass.
+
+struct IpPlan {
+  int n, nstages;
+  int radix[16];
+};
+
+__host__ __device__ inline bool ip_radices(int n, IpPlan &p) {
+  p.n = n;
+  p.nstages = 0;
+  int r = n;
+  while (r > 1 && r % 8 == 0) { p.radix[p.nstages++] = 8; r /= 8; }
+  while (r > 1 && r % 4 == 0) { p.radix[p.nstages++] = 4; r /= 4; }
+  while (r > 1 && r % 2 == 0) { p.radix[p.nstages++] = 2; r /= 2; }
+  return r == 1 && p.nstages <= 16;
+}
+
+// the two-level twiddle table of a length-n transform from the full table
+__device__ __forceinline__ void load_twiddles_n(const double2 *tw, int n, double2 *tws) {
+  const int nhi = (n + kTwLo - 1) / kTwLo;
+  for (int i = threadIdx.x; i < kTwLo + nhi; i += blockDim.x)
+    tws[i] = i < kTwLo ? (i < n ? __ldg(tw + i) : make_double2(1.0, 0.0)) : __ldg(tw + (i - kTwLo) * kTwLo);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void ip_stage(double2 *x, int n, int L, const double2 *tws) {
+  const int s = L / R, tstep = n / L;
+  const double2 rc[6] = {};
+  for (int q = threadIdx.x; q < n / R; q += blockDim.x) {
+    const int b = q / s, n1 = q - b * s;
+    double2 *p = x + b * L + n1;
+    double2 v[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = p[j * s];
+    if constexpr (!INV) {
+      dft<R, false>(v, rc);
+      if (n1) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], twiddle(tws, k * n1 * tstep));
+      }
+    } else {
+      if (n1) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], twiddle(tws, k * n1 * tstep));
+      }
+      dft<R, true>(v, rc);
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) p[j * s] = v[j];
+  }
+}
+
+// every thread of the CTA calls these; a barrier separates the stages and
+// follows the last one
+template <bool INV>
+__device__ void ip_run(double2 *x, const IpPlan &pl, const double2 *tws) {
+  if constexpr (!INV) {
+    int L = pl.n;
+    for (int s = 0; s < pl.nstages; ++s) {
+      const int r = pl.radix[s];
+      if (r == 8) ip_stage<8, false>(x, pl.n, L, tws);
+      else if (r == 4) ip_stage<4, false>(x, pl.n, L, tws);
+      else ip_stage<2, false>(x, pl.n, L, tws);
+      __syncthreads();
+      L /= r;
+    }
+  } else {
+    int L = 1;
+    for (int s = pl.nstages - 1; s >= 0; --s) {
+      const int r = pl.radix[s];
+      L *= r;
+      if (r == 8) ip_stage<8, true>(x, pl.n, L, tws);
+      else if (r == 4) ip_stage<4, true>(x, pl.n, L, tws);
+      else ip_stage<2, true>(x, pl.n, L, tws);
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace fft
+}  // namespace atb

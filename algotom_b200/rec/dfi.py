@@ -3,25 +3,27 @@
 ``dfi_reconstruction`` and ``generate_mapping_coordinate`` of
 ``algotom/rec/reconstruction.py`` (algotom 1.6.0, ``:687-907``): same
 signatures, errors, warnings and output dtypes.  The direct Fourier
-inversion runs on the device:
+inversion runs on the device, every slice of a stack in the same launches:
 
-1. the sinogram is padded by one edge column when its width is even and
+1. every row is padded by one edge column when the width is even and
    centred with the cubic-spline sub-pixel shift of
-   ``scipy.ndimage.shift(mode="nearest")`` (``atb_shift_rows``); given
-   ``angles``, a 360-degree scan is folded to 180 degrees and the rows are
-   rotated to start at angle 0 with the same spline along the angle axis
-   (``mode="wrap"``, ``atb_spline_prefilter`` then the spline taps);
-2. the detector axis is padded (NumPy's modes, device index maps) and, with
-   ``apply_log``, values <= 0 are set to 1 (with the reference's warning)
-   before ``-log``;
-3. every row is transformed (library FFT, FP64) and windowed;
-4. the polar spectrum is turned into quintic B-spline coefficients along
-   both axes (``atb_spline_prefilter``, the prefilter's impulse response as
-   a parallel FIR) and regridded onto the Cartesian
-   frequency grid with the unit-circle mask (``atb_dfi_regrid``);
-5. an inverse 2-D transform (library FFT, FP64), crop and circle mask.
+   ``scipy.ndimage.shift(mode="nearest")`` (``atb_shift_rows_ext``);
+2. given ``angles``, a 360-degree scan is folded to 180 degrees and the
+   rows are rotated to start at angle 0 with the same spline along the
+   angle axis (``mode="wrap"``: ``atb_dfi_angle_stack``,
+   ``atb_spline_prefilter``, ``atb_wrap_shift_rows``);
+3. padding with NumPy's modes, ``-log`` (values <= 0 counted for the
+   reference's warning), the centred row transform and the window, two
+   rows per FP64 Bluestein transform (``atb_dfi_rows``);
+4. quintic B-spline coefficients of the polar spectrum along both axes
+   (``atb_spline_prefilter``);
+5. regridding onto the Cartesian frequency grid row by row, inverse 2-D
+   transform, crop, ``1 / w^2`` and circle mask (``atb_dfi_inverse``).
 
-FP64 from step 3 on; the reference runs its row transform in the input's
+The transforms are this library's own (``csrc/dfi_fft.cu``) for padded
+widths up to 4096 (2730 detector columns at the default ``pad_rate``);
+wider rows take the library FFT for steps 3 and 5 (``_dfi_wide``).  FP64
+from step 3 on; the reference runs its row transform in the input's
 float32 precision, so results agree to ~1e-7.  ``ncore`` is accepted and
 ignored.
 """
@@ -34,6 +36,10 @@ from .. import _native as nat
 from . import reconstruction as R
 from . import windows as win
 from .padding import pad_rows
+
+_SPECTRA_BYTES = 4 << 30   # polar spectra (+ their coefficients) per launch
+_TABLES = {}
+_WINDOWS = {}
 
 
 def generate_mapping_coordinate(width_sino, height_sino, width_rec,
@@ -73,86 +79,167 @@ def _prefilter(t, axis, order, boundary):
     return out
 
 
-def _bspline3(u):
-    a = u.abs()
-    return torch.where(a < 1, 2.0 / 3.0 - a * a + a * a * a / 2.0,
-                       torch.where(a < 2, (2.0 - a) ** 3 / 6.0,
-                                   torch.zeros_like(a)))
-
-
 def _shift_cols_wrap(t32, s):
-    """float32 ``scipy.ndimage.shift(t32, (s, 0), mode="wrap")``: cubic
-    spline along the rows' axis with whole-sample symmetric coefficients,
-    coordinates wrapped with period n - 1 and mirrored taps."""
-    n = t32.shape[0]
+    """float32 ``scipy.ndimage.shift(t32, (s, 0), mode="wrap")`` of a 2-D
+    CUDA tensor: cubic-spline coefficients along the rows (whole-sample
+    symmetric), then the wrapped taps of ``atb_wrap_shift_rows``."""
+    m, n = t32.shape
     c = _prefilter(t32.to(torch.float64).contiguous(), 0, 3, 1)
-    cc = torch.arange(n, dtype=torch.float64, device=t32.device) - s
-    sz = n - 1
-    if sz > 0:
-        cc = torch.where(cc < 0, cc + sz * (torch.floor(-cc / sz) + 1), cc)
-        cc = torch.where(cc > n - 1, cc - sz * torch.floor(cc / sz), cc)
-    f = torch.floor(cc).to(torch.int64)
-    out = torch.zeros(c.shape, dtype=torch.float64, device=c.device)
-    for m in range(-1, 3):
-        idx = f + m
-        if n > 1:
-            p = 2 * (n - 1)
-            r = torch.remainder(idx, p)
-            idx = torch.where(r >= n, p - r, r)
-        else:
-            idx = torch.zeros_like(idx)
-        out += _bspline3(cc - (f + m).to(torch.float64))[:, None] * c[idx]
-    return out.to(torch.float32)
+    out = torch.empty((m, n), dtype=torch.float32, device=t32.device)
+    nat.call("atb_wrap_shift_rows", c.data_ptr(), n, 0, m, 1, n, float(s),
+             m, 0, out.data_ptr(), n, 0, R._stream_ptr(t32.device))
+    return out
 
 
-def _handle_angles(t, angles):
-    """``__dfi_handle_angles`` (reconstruction.py:731-749) on the device."""
-    nrow = t.shape[0]
+def _fft_tables(w, device):
+    """(chirp, twiddle, bfwd, binv) device tables of the width-w Bluestein
+    transforms, made once per (device, w).  The chirp's phase pi m^2 / w is
+    reduced exactly (m^2 mod 2w in integers) before the trigonometry."""
+    key = (device.index, w)
+    tab = _TABLES.get(key)
+    if tab is None:
+        M = nat.call("atb_dfi_fft_length", w)
+        m = np.arange(w, dtype=np.int64)
+        chirp = np.exp(1j * (np.pi * ((m * m) % (2 * w)) / w))
+        k = np.arange(M, dtype=np.float64)
+        tw = np.exp(-2j * np.pi * k / M)
+        chirp = torch.from_numpy(chirp).to(device)
+        tw = torch.from_numpy(tw).to(device)
+        bfwd = torch.empty(M, dtype=torch.complex128, device=device)
+        binv = torch.empty(M, dtype=torch.complex128, device=device)
+        nat.call("atb_dfi_fft_setup", w, chirp.data_ptr(), tw.data_ptr(),
+                 bfwd.data_ptr(), binv.data_ptr(), R._stream_ptr(device))
+        tab = _TABLES[key] = (chirp, tw, bfwd, binv)
+    return tab
+
+
+def _window(filter_name, w, device):
+    key = (device.index, filter_name, w)
+    t = _WINDOWS.get(key)
+    if t is None:
+        t = _WINDOWS[key] = torch.from_numpy(
+            win.make_smoothing_window(filter_name, w)).to(device)
+    return t
+
+
+def _own_transform(w):
+    return 2 <= w and 2 * w - 1 <= 8192
+
+
+def _angle_rows(sh, angles):
+    """``__dfi_handle_angles`` (``reconstruction.py:731-749``) of every
+    slice of the [nrow, nslice, ncol1] float32 stack at once."""
+    nrow, nslice, ncol1 = sh.shape
     if len(angles) != nrow:
         raise ValueError("!!! Number of angles is not the same as the row "
                          "number of the sinogram !!!")
     angles = np.asarray(angles, dtype=np.float64)
     t_ang = np.sum(np.abs(np.diff(angles * 180.0 / np.pi)))
-    if abs(t_ang - 360) < 10:
-        nrow = nrow // 2 + 1
-        t = (t[:nrow] + torch.flip(t[-nrow:], dims=[1])) / 2
+    fold = abs(t_ang - 360) < 10
+    n1 = nrow // 2 + 1 if fold else nrow
     step = np.mean(np.abs(np.diff(angles)))
     b_ang = angles[0] - (angles[0] // (2 * np.pi)) * (2 * np.pi)
-    sino_360 = torch.cat([t[:nrow - 1], torch.flip(t, dims=[1])], dim=0)
-    t = _shift_cols_wrap(sino_360, b_ang / step)[:nrow]
-    if angles[-1] < angles[0]:
-        t = torch.flip(t, dims=[0, 1])
-    return t
+    m = 2 * n1 - 1
+    dev, st = sh.device, R._stream_ptr(sh.device)
+    lines = nslice * ncol1
+    stack = torch.empty((m, nslice, ncol1), dtype=torch.float64, device=dev)
+    nat.call("atb_dfi_angle_stack", sh.data_ptr(), lines, ncol1, nrow,
+             nslice, ncol1, int(fold), stack.data_ptr(), lines, ncol1, st)
+    coef = torch.empty_like(stack)
+    nat.call("atb_spline_prefilter", stack.data_ptr(), coef.data_ptr(), 1,
+             lines, lines, 1, m, 3, 1, st)
+    del stack
+    out = torch.empty((n1, nslice, ncol1), dtype=torch.float32, device=dev)
+    nat.call("atb_wrap_shift_rows", coef.data_ptr(), lines, ncol1, m,
+             nslice, ncol1, float(b_ang / step), n1,
+             int(angles[-1] < angles[0]), out.data_ptr(), lines, ncol1, st)
+    return out
 
 
-def _circle_mask(width, ratio, device):
-    c = width // 2
-    radius = ratio * c
-    ax = torch.arange(-c, width - c, device=device, dtype=torch.float64)
-    return (ax[None, :] ** 2 + ax[:, None] ** 2 <= radius * radius).to(
-        torch.float64)
+def _dfi_own(sh, out, pad, ncol, pad_mode, apply_log, window, mask_r2):
+    """Steps 3-5 on this library's transforms: the prepared float32
+    [nrow, nslice, ncol1] stack into ``out`` ([ncol, nslice, ncol] or
+    [ncol, ncol]), slices in groups whose spectra fit the budget.
+    Returns the number of padded values <= 0 (with ``apply_log``)."""
+    nrow, nslice, ncol1 = sh.shape
+    w = ncol1 + 2 * pad
+    dev, st = sh.device, R._stream_ptr(sh.device)
+    chirp, tw, bfwd, binv = _fft_tables(w, dev)
+    # (the row-wise prefilter takes up to 65535 lines per launch)
+    group = max(1, min(nslice, _SPECTRA_BYTES // (2 * 16 * nrow * w),
+                       65535 // nrow))
+    f32 = int(out.dtype == torch.float32)
+    ors = out.stride(0)
+    oss = out.stride(1) if out.dim() == 3 else 0
+    counter = torch.empty(1, dtype=torch.int32, device=dev)
+    bad = 0
+    spec = torch.empty((nrow, group, w), dtype=torch.complex128, device=dev)
+    tmp = torch.empty_like(spec)
+    wbytes = nat.call("atb_dfi_inverse_workspace", w, ncol, group)
+    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    for k0 in range(0, nslice, group):
+        g = min(group, nslice - k0)
+        src = sh[:, k0:k0 + g]
+        nat.call("atb_dfi_rows", src.data_ptr(), nslice * ncol1, ncol1,
+                 nrow, g, ncol1, pad, nat.PAD_MODES[pad_mode],
+                 int(apply_log),
+                 window.data_ptr() if window is not None else None,
+                 counter.data_ptr() if apply_log else None,
+                 chirp.data_ptr(), tw.data_ptr(), bfwd.data_ptr(),
+                 binv.data_ptr(), spec.data_ptr(), g * w, w, st)
+        if apply_log:
+            bad += int(counter.item())
+        # quintic coefficients along the angles, then along the frequencies
+        nat.call("atb_spline_prefilter", spec.data_ptr(), tmp.data_ptr(), 2,
+                 2 * g * w, g * w, 2, nrow, 5, 0, st)
+        nat.call("atb_spline_prefilter", tmp.data_ptr(), spec.data_ptr(),
+                 2 * w, 2, nrow * g, 2, w, 5, 0, st)
+        nat.call("atb_dfi_inverse", spec.data_ptr(), g * w, w, nrow, g, w,
+                 pad, ncol, float(mask_r2), chirp.data_ptr(), tw.data_ptr(),
+                 bfwd.data_ptr(), binv.data_ptr(),
+                 out.data_ptr() + k0 * oss * out.element_size(), ors, oss,
+                 f32, ws.data_ptr(), wbytes, st)
+    return bad
 
 
-def _dfi_slice(s, window, pad, ncol):
-    """Steps 3-5 for one prepared float32 [nrow, ncol2] CUDA sinogram;
-    returns the float64 [ncol, ncol] image (cropped at ``pad``).  The
-    regridding writes its grid in ifftshift order and the final fftshift
-    and crop are one index gather, so the 2-D shifts cost no extra pass."""
-    nrow, w = s.shape
-    x = s.to(torch.float64)
-    f = torch.fft.fftshift(torch.fft.fft(torch.fft.ifftshift(x, dim=1),
-                                         dim=1), dim=1)
-    if window is not None:
-        f = f * window
-    f = _prefilter(_prefilter(f.contiguous(), 0, 5, 0), 1, 5, 0)
-    reg = torch.empty((w, w), dtype=torch.complex128, device=s.device)
-    nat.call("atb_dfi_regrid", f.data_ptr(), nrow, w, reg.data_ptr(),
-             R._stream_ptr(s.device))
-    y = torch.fft.ifft2(reg).real
-    # fftshift(y)[k] = y[(k - w // 2) mod w], rows and columns pad..pad+ncol
-    idx = torch.remainder(torch.arange(pad, pad + ncol, device=s.device)
+def _dfi_wide(sh, out, pad, ncol, pad_mode, apply_log, window, mask_r2):
+    """Steps 3-5 for padded widths beyond the own transforms' 4096: padding
+    and ``-log`` as tensor operations, the row transform and the inverse 2-D
+    transform through the library FFT, the spline and regridding kernels as
+    above."""
+    nrow, nslice, ncol1 = sh.shape
+    w = ncol1 + 2 * pad
+    bad = 0
+    c = ncol // 2
+    ax = torch.arange(-c, ncol - c, device=sh.device, dtype=torch.float64)
+    mask = None if mask_r2 < 0 else \
+        (ax[None, :] ** 2 + ax[:, None] ** 2 <= mask_r2).to(torch.float64)
+    idx = torch.remainder(torch.arange(pad, pad + ncol, device=sh.device)
                           - w // 2, w)
-    return y.index_select(0, idx).index_select(1, idx)
+    for k in range(nslice):
+        s = pad_rows(sh[:, k, :], pad, pad_mode)
+        if apply_log:
+            neg = s <= 0.0
+            bad += int(neg.sum())
+            s = -torch.log(s.masked_fill(neg, 1.0))
+        x = s.to(torch.float64)
+        f = torch.fft.fftshift(torch.fft.fft(torch.fft.ifftshift(x, dim=1),
+                                             dim=1), dim=1)
+        if window is not None:
+            f = f * window
+        f = _prefilter(_prefilter(f.contiguous(), 0, 5, 0), 1, 5, 0)
+        reg = torch.empty((w, w), dtype=torch.complex128, device=sh.device)
+        nat.call("atb_dfi_regrid", f.data_ptr(), nrow, w, reg.data_ptr(),
+                 R._stream_ptr(sh.device))
+        y = torch.fft.ifft2(reg).real.index_select(0, idx).index_select(1,
+                                                                        idx)
+        if mask is not None:
+            y = y * mask
+        if out.dim() == 3:
+            out[:, k, :] = y
+        else:
+            out.copy_(y)
+    return bad
 
 
 def dfi_reconstruction(sinogram, center, angles=None, ratio=1.0,
@@ -173,47 +260,38 @@ def dfi_reconstruction(sinogram, center, angles=None, ratio=1.0,
     if pad_mode not in nat.PAD_MODES:
         raise ValueError("pad_mode %r is not supported" % (pad_mode,))
     t, is_np = R._to_device(sinogram)
-    slices = [t] if t.dim() == 2 else [t[:, k, :] for k in range(t.shape[1])]
-    prepared = []
-    pad = 0
-    for s in slices:
-        if ncol % 2 == 0:
-            s = torch.cat([s, s[:, -1:]], dim=1)
-        ncol1 = s.shape[1]
-        xshift = (ncol1 - 1) / 2.0 - center
-        pad = int(pad_rate * ncol1)
-        s = _shift_rows(s.contiguous(), xshift)
-        if angles is not None:
-            s = _handle_angles(s, angles)
-        prepared.append(pad_rows(s, pad, pad_mode))
-    stack = torch.stack(prepared)
-    if apply_log is True:
-        bad = stack <= 0.0
-        if bool(bad.any()):
-            warnings.warn("!!!Applying logarithm is enabled but "
-                          "there are values <= 0.0 in the data!!!")
-            stack = stack.masked_fill(bad, 1.0)
-        stack = -torch.log(stack)
-    nrow2, ncol2 = stack.shape[1], stack.shape[2]
-    window = None
-    if filter_name is not None:
-        window = torch.from_numpy(win.make_smoothing_window(
-            filter_name, ncol2)).to(t.device)
-    mask = None
+    if input_3d:
+        t = t.contiguous()
+    nslice = t.shape[1] if input_3d else 1
+    dev, st = t.device, R._stream_ptr(t.device)
+    ncol1 = ncol + 1 if ncol % 2 == 0 else ncol
+    xshift = (ncol1 - 1) / 2.0 - center
+    pad = int(pad_rate * ncol1)
+    # 1. edge column for an even width, centring shift: all rows of all
+    # slices in one launch
+    sh = torch.empty((nrow, nslice, ncol1), dtype=torch.float32, device=dev)
+    nat.call("atb_shift_rows_ext", t.data_ptr(), t.stride(-2),
+             nrow * nslice, ncol, ncol1, float(xshift), sh.data_ptr(),
+             ncol1, st)
+    # 2. angles
+    if angles is not None:
+        sh = _angle_rows(sh, angles)
+    w = ncol1 + 2 * pad
+    window = _window(filter_name, w, dev) if filter_name is not None \
+        else None
+    mask_r2 = -1.0
     if ratio is not None:
         if ratio == 0.0:
             ratio = min(center, ncol - center) / (0.5 * ncol)
-        mask = _circle_mask(ncol, ratio, t.device)
-    out = []
-    for s in stack:
-        r = _dfi_slice(s, window, pad, ncol)
-        out.append(r * mask if mask is not None else r)
-    rec = torch.stack(out, dim=1) if len(out) > 1 or input_3d else out[0]
+        radius = ratio * (ncol // 2)
+        mask_r2 = radius * radius
     dtype = torch.float64 if filter_name is not None else torch.float32
-    rec = rec.to(dtype)
-    return rec.cpu().numpy() if is_np else rec
-
-
-def _shift_rows(t, shift):
-    from ..prep.conversion import _shift_rows as shift_rows
-    return shift_rows(t, shift)
+    shape = (ncol, nslice, ncol) if input_3d else (ncol, ncol)
+    out = torch.empty(shape, dtype=dtype, device=dev)
+    run = _dfi_own if _own_transform(w) else _dfi_wide
+    bad = run(sh, out, pad, ncol, pad_mode, apply_log is True, window,
+              mask_r2)
+    if bad:
+        warnings.warn("!!!Applying logarithm is enabled but "
+                      "there are values <= 0.0 in the data!!!")
+    return out.cpu().numpy() if is_np else out

@@ -1531,8 +1531,9 @@ def run_dfi(args):
         "config": {"workload": "DFI of one 1801 x 2560 slice, padded to "
                                "3841, regridded to 3841^2"},
         "cpu_baseline": cpu, "accuracy": acc, "clocks": clocks,
-        # shift, pad gather, spline prefilter x 2, regrid, plus library FFTs
-        "gpu_launches": 4 * args.steps}), flush=True)
+        # centring shift, padded row transform, spline prefilter x 2,
+        # regridded inverse (rows, columns)
+        "gpu_launches": 6 * args.steps}), flush=True)
 
 
 def _spawn_ranks(n):

@@ -568,6 +568,16 @@ int atb_shift_rows(const float *src, int64_t src_row_stride, int nrow,
                    int64_t dst_row_stride, void *stream);
 
 /*
+ * The centring of __dfi_handle_sinogram (reconstruction.py:756-770): rows
+ * of ncol_src samples padded on the right with their last sample to ncol
+ * columns (np.pad(mode="edge"), one column for an even width), then
+ * shifted as atb_shift_rows does.  ncol_src <= ncol <= 16384.
+ */
+int atb_shift_rows_ext(const float *src, int64_t src_row_stride, int nrow,
+                       int ncol_src, int ncol, double shift, float *dst,
+                       int64_t dst_row_stride, void *stream);
+
+/*
  * The row work of extend_sinogram (conversion.py:425-454): optional -log,
  * the sub-pixel shift (0: none), the linear ramp over `overlap` columns on
  * `side` (1: right, 0: left), edge padding to 2 ncol - overlap columns and
@@ -619,6 +629,94 @@ int atb_spline_prefilter(const double *src, double *dst, int64_t line_stride,
  */
 int atb_dfi_regrid(const double *coef, int nrow, int width, double *out,
                    void *stream);
+
+/*
+ * __dfi_handle_angles (reconstruction.py:731-749), first half: with fold,
+ * the 360-degree fold (n = nrow_in / 2 + 1 rows, row r = (row r + row
+ * nrow_in - n + r mirrored left-right) / 2 in float32; else n = nrow_in),
+ * then the stack the angle shift runs on: rows 0 .. n - 2 followed by all
+ * n rows mirrored, 2 n - 1 rows, widened to float64.
+ *
+ *   src  float32, row r of slice k at src + k src_slice_stride
+ *        + r src_row_stride, ncol samples
+ *   dst  float64, row i of slice k at dst + k dst_slice_stride
+ *        + i dst_row_stride
+ */
+int atb_dfi_angle_stack(const float *src, int64_t src_row_stride,
+                        int64_t src_slice_stride, int nrow_in, int nslice,
+                        int ncol, int fold, double *dst,
+                        int64_t dst_row_stride, int64_t dst_slice_stride,
+                        void *stream);
+
+/*
+ * Second half: scipy.ndimage.shift(stack, (shift, 0), order=3,
+ * mode="wrap")[:nout] (reconstruction.py:746) from the stack's cubic
+ * B-spline coefficients along the rows (atb_spline_prefilter, order 3,
+ * boundary 1): coordinate i - shift wrapped into [0, m - 1] with period
+ * m - 1, mirrored tap indices, rounded to float32.  flip: reverse rows and
+ * columns (the flipud(fliplr(.)) of descending angles, :747-748).
+ */
+int atb_wrap_shift_rows(const double *coef, int64_t coef_row_stride,
+                        int64_t coef_slice_stride, int m, int nslice,
+                        int ncol, double shift, int nout, int flip,
+                        float *dst, int64_t dst_row_stride,
+                        int64_t dst_slice_stride, void *stream);
+
+/*
+ * The Fourier transforms of DFI as Bluestein transforms of the padded
+ * width w (any w >= 2 with a power-of-two M >= 2 w - 1, M <= 8192; w =
+ * 3841 at 2560 detector pixels), FP64, this library's own FFT.
+ *
+ * atb_dfi_fft_length: M for width w (ATB_ERANGE beyond 8192).
+ * atb_dfi_fft_setup: from host-made tables on the device, chirp complex128
+ *   [w] = exp(i pi (m^2 mod 2w) / w) and twiddle complex128 [M] =
+ *   exp(-2 pi i m / M), fills bfwd and binv (complex128 [M] each): the
+ *   chirp kernels' transforms that the other calls read.
+ */
+int atb_dfi_fft_length(int w);
+int atb_dfi_fft_setup(int w, const void *chirp, const void *twiddle,
+                      void *bfwd, void *binv, void *stream);
+
+/*
+ * Padding, -log and row transform of __dfi_single_slice and
+ * dfi_reconstruction (reconstruction.py:767-770, 774-776, 885-890):
+ * every row of n float32 samples padded to w = n + 2 pad columns with
+ * NumPy's pad_mode (ATB_PAD_*, end and constant values 0, statistics over
+ * the whole row), with apply_log -log'ed (values <= 0 give 0; their count
+ * over the padded rows is written to *nonpositive when it is not null),
+ * then fftshift(fft(ifftshift(row))) * window (window float64 [w] or null)
+ * as complex128.  Rows r of slice k: src + k src_slice_stride
+ * + r src_row_stride, dst + k dst_slice_stride + r dst_row_stride
+ * (strides in floats and in complex values).
+ */
+int atb_dfi_rows(const float *src, int64_t src_row_stride,
+                 int64_t src_slice_stride, int nrow, int nslice, int n,
+                 int pad, int pad_mode, int apply_log, const double *window,
+                 int *nonpositive, const void *chirp, const void *twiddle,
+                 const void *bfwd, const void *binv, void *dst,
+                 int64_t dst_row_stride, int64_t dst_slice_stride,
+                 void *stream);
+
+/*
+ * Regridding, inverse 2-D transform, crop and mask of __dfi_single_slice
+ * and dfi_reconstruction (reconstruction.py:776-787, 895-904): from the
+ * quintic B-spline coefficients of the polar spectrum (complex128 [nrow]
+ * [w] per slice, atb_spline_prefilter along both axes), the Cartesian
+ * spectrum is regridded row by row as atb_dfi_regrid does, inverted,
+ * cropped to [pad, pad + ncol) on both axes, divided by w^2 and masked by
+ * the circle of radius^2 mask_r2 about ncol / 2 (mask_r2 < 0: none);
+ * float64 out (float32 with out_f32).  Pixel (a, b) of slice k at out
+ * + k out_slice_stride + a out_row_stride + b (in elements).  workspace:
+ * atb_dfi_inverse_workspace(w, ncol, nslice) bytes.
+ */
+int64_t atb_dfi_inverse_workspace(int w, int ncol, int nslice);
+int atb_dfi_inverse(const void *coef, int64_t coef_row_stride,
+                    int64_t coef_slice_stride, int nrow, int nslice, int w,
+                    int pad, int ncol, double mask_r2, const void *chirp,
+                    const void *twiddle, const void *bfwd, const void *binv,
+                    void *out, int64_t out_row_stride,
+                    int64_t out_slice_stride, int out_f32, void *workspace,
+                    int64_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,31 @@ def test_abi_argument_errors():
     assert lib.atb_dfi_regrid(None, 8, 8, one, None) == -1
     assert lib.atb_dfi_regrid(one, 8, 50000, one, None) == -3
     assert b"too large" in lib.atb_last_error()
+    # own transforms: M = the power of two >= 2 w - 1, at most 8192
+    assert lib.atb_dfi_fft_length(3841) == 8192
+    assert lib.atb_dfi_fft_length(5) == 16
+    assert lib.atb_dfi_fft_length(4097) == -3
+    assert lib.atb_dfi_fft_length(1) == -1
+    assert lib.atb_dfi_rows(one, 8, 0, 4, 1, 8, 2, 10, 0, None, None, one,
+                            one, one, one, two, 12, 0, None) == -1
+    assert b"pad_mode" in lib.atb_last_error()
+    assert lib.atb_dfi_rows(None, 8, 0, 4, 1, 8, 2, 0, 0, None, None, one,
+                            one, one, one, two, 12, 0, None) == -1
+    assert lib.atb_dfi_inverse_workspace(15, 8, 2) == 2 * 15 * 8 * 16
+    assert lib.atb_dfi_inverse_workspace(15, 16, 1) == -1
+    assert lib.atb_dfi_inverse(one, 15, 0, 9, 1, 15, 4, 12, -1.0, one, one,
+                               one, one, two, 12, 0, 0, two, 1 << 20,
+                               None) == -1  # crop beyond the width
+    assert lib.atb_dfi_inverse(one, 15, 0, 9, 1, 15, 3, 8, -1.0, one, one,
+                               one, one, two, 8, 0, 0, two, 100,
+                               None) == -1  # workspace too small
+    assert b"workspace" in lib.atb_last_error()
+    assert lib.atb_wrap_shift_rows(one, 8, 0, 5, 1, 8, 0.5, 6, 0, two, 8, 0,
+                                   None) == -1  # nout > m
+    assert lib.atb_wrap_shift_rows(one, 8, 0, 5, 1, 8, float("nan"), 5, 0,
+                                   two, 8, 0, None) == -1
+    assert lib.atb_shift_rows_ext(one, 8, 4, 9, 8, 0.5, two, 8,
+                                  None) == -1  # fewer columns out than in
 
 
 def test_center_error():
@@ -192,3 +217,87 @@ def test_reference_centre_search_tests_with_dfi(cuda, golden):
             filter_name="hann", apply_log=False, ncore=None, sigma=1,
             metric_function=get_negative, n=2)
     assert abs(got - center) < 0.1
+
+
+@pytest.mark.gpu
+def test_dfi_row_transform_matches_numpy(cuda):
+    """atb_dfi_rows at the benchmark's width (2561 + 2 x 640 = 3841 =
+    23 x 167, M = 8192): padding, pairs of rows per transform (an odd row
+    count leaves one alone), strided slices, window; FP64 to 1e-12 (no
+    -log here: its float32 rounding would be all the test saw)."""
+    import torch
+    from algotom_b200.rec import dfi
+    from algotom_b200.rec import reconstruction as R
+    rng = np.random.default_rng(5)
+    nrow, nslice, n, pad = 5, 2, 2561, 640
+    w = n + 2 * pad
+    x = rng.random((nrow, nslice, n)).astype(np.float32) + 0.1
+    win = rng.random(w)
+    t = torch.as_tensor(x, device="cuda")
+    wt = torch.as_tensor(win, device="cuda")
+    chirp, tw, bfwd, binv = dfi._fft_tables(w, t.device)
+    out = torch.empty((nrow, nslice, w), dtype=torch.complex128,
+                      device="cuda")
+    nat.call("atb_dfi_rows", t.data_ptr(), nslice * n, n, nrow, nslice, n,
+             pad, nat.PAD_MODES["edge"], 0, wt.data_ptr(), None,
+             chirp.data_ptr(), tw.data_ptr(), bfwd.data_ptr(),
+             binv.data_ptr(), out.data_ptr(), nslice * w, w,
+             R._stream_ptr())
+    got = out.cpu().numpy()
+    for k in range(nslice):
+        s = np.pad(x[:, k, :], ((0, 0), (pad, pad)), mode="edge")
+        ref = np.fft.fftshift(np.fft.fft(np.fft.ifftshift(
+            s.astype(np.float64), axes=1)), axes=1) * win
+        err = np.abs(got[:, k, :] - ref).max() / np.abs(ref).max()
+        assert err < 1e-12, err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", sorted(nat.PAD_MODES))
+def test_dfi_pad_modes_with_log(cuda, mode):
+    """Every numpy pad mode through the fused padding of atb_dfi_rows, with
+    -log and values <= 0 (the reference's warning), against the FP64
+    oracle (np.pad itself)."""
+    from algotom_b200.rec import reconstruction as R
+    rng = np.random.default_rng(len(mode))
+    nrow, ncol = 31, 24
+    sino = np.exp(-rng.random((nrow, ncol)) * 2.0).astype(np.float32)
+    sino[3, 5] = 0.0
+    sino[7, 0] = -1.0
+    with warnings.catch_warnings(record=True) as caught:
+        warnings.simplefilter("always")
+        got = R.dfi_reconstruction(sino.copy(), 11.6, pad_mode=mode,
+                                   pad_rate=0.5)
+    assert any("logarithm" in str(w.message) for w in caught)
+    ref = D.dfi_reconstruction(sino, 11.6, pad_mode=mode, pad_rate=0.5,
+                               apply_log=True)
+    assert O.rel_l2(got, ref) < TOL
+
+
+@pytest.mark.gpu
+def test_dfi_own_transforms_match_library_fft(cuda):
+    """The benchmark slice (1801 x 2560, padded to 3841) through this
+    library's transforms and through the library-FFT path of wider rows:
+    same spline and regridding kernels, independent transforms."""
+    import torch
+    from algotom_b200 import phantom
+    from algotom_b200.rec import dfi
+    from algotom_b200.rec import reconstruction as R
+    nrow, ncol, cen = 1801, 2560, 1278.3
+    ang = np.linspace(0.0, np.pi, nrow, endpoint=False)
+    s, _, _ = phantom.ellipse_sinogram(2000, nrow, ncol, cen, angles=ang)
+    got = R.dfi_reconstruction(torch.as_tensor(s, device="cuda"), cen,
+                               apply_log=False)
+    ncol1 = ncol + 1
+    pad = int(0.25 * ncol1)
+    sh = torch.empty((nrow, 1, ncol1), dtype=torch.float32, device="cuda")
+    t = torch.as_tensor(s, device="cuda")
+    nat.call("atb_shift_rows_ext", t.data_ptr(), ncol, nrow, ncol, ncol1,
+             (ncol1 - 1) / 2.0 - cen, sh.data_ptr(), ncol1, R._stream_ptr())
+    w = ncol1 + 2 * pad
+    ref = torch.empty((ncol, ncol), dtype=torch.float64, device="cuda")
+    radius = ncol // 2
+    dfi._dfi_wide(sh, ref, pad, ncol, "edge", False,
+                  dfi._window("hann", w, t.device), float(radius * radius))
+    err = (torch.linalg.norm(got - ref) / torch.linalg.norm(ref)).item()
+    assert err < 1e-10, err
