@@ -3,43 +3,62 @@
 // Replaces apply_ramp_filter (algotom/rec/reconstruction.py:118-153), whose
 // FFT / shift / window / inverse-FFT / real / crop chain is a real circular
 // convolution of the padded row of length N = ncol + 2 pad with a periodic
-// kernel kappa, cropped to [pad, pad + ncol).  Those ncol outputs only see
-// kernel lags in [pad - N + 1, pad + ncol - 1], so the same numbers come out
-// of a circular convolution of any length M >= N + ncol - 1 whose kernel b
-// holds kappa at those lags (b[u mod M] = kappa[u mod N]) and zero elsewhere.
-// The host builds b's spectrum in FP64 for a power-of-two M; this kernel
-// then needs nothing but power-of-two FFTs: radix-16 Stockham stages (and
-// one radix-2/4/8 stage) with every thread holding 32 elements in
-// registers, twiddles from two short tables in shared memory.
+// kernel kappa, cropped to [pad, pad + ncol).  The transform length n is
+// the cheaper of two exact forms (by a flop count of the stages):
+// - n = N itself when N has no prime factor above 13 (2860 = 4 5 11 13 at
+//   2560 detector pixels and the reference's pad of 150), the reference's
+//   own transform length;
+// - otherwise the smallest 7-smooth n >= N + ncol - 1: the ncol outputs
+//   only see kernel lags in [pad - N + 1, pad + ncol - 1], so a circular
+//   convolution of that length whose kernel holds kappa at those lags
+//   (b[u mod n] = kappa[u mod N]) and zero elsewhere gives the same numbers.
+// The host builds the kernel's spectrum in FP64.  The transforms are
+// mixed-radix Stockham FFTs in FP32 (radices 16, 8, 4, 2, 13, 11, 7, 5, 3),
+// every thread holding its butterflies' inputs in registers across a
+// barrier so one shared-memory buffer suffices; twiddles come from two
+// short tables in shared memory.
 //
 // One CTA filters two rows at once: real rows x1, x2 travel as the complex
 // row x1 + i x2 through one forward FFT, a product with the (real-kernel)
-// spectrum and one inverse FFT (done as conj(FFT(conj(.))) with 1/M folded
+// spectrum and one inverse FFT (done as conj(FFT(conj(.))) with 1/n folded
 // into the spectrum); the real and imaginary parts of the result are the
 // two filtered rows.  Each row is read from HBM once (with the -log folded
 // in) and written once; padding, both transforms and the spectral product
 // stay in shared memory.
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 
 #include "common.cuh"
 
 namespace {
 
-constexpr int kMinLog2M = 4;
-constexpr int kMaxLog2M = 14;  // 16384 complex (+1/16 padding) = 136 KiB of shared memory
+constexpr int kMaxLen = 16384;  // 16384 complex (+1/16 padding) = 136 KiB of shared memory
+constexpr int kMaxStages = 14;
+constexpr int kTwLo = 64;       // two-level twiddle tables: w^t = ta[t / 64] tb[t % 64]
 
 // Shared-memory index of complex element i: one padding word per 16
 // elements keeps the strided Stockham writes free of bank conflicts.
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 
-struct FilterArgs {
+// What every CTA of a launch shares: the transform plan and the pad / log
+// settings (read from parameter space; the plan arrays are indexed at run
+// time, so kernels take it as a __grid_constant__ parameter).
+struct FilterPlan {
+  int mode, apply_log;
+  const float2 *tw;    // [n] exp(-2 pi i t / n)
+  int n, nstages;      // transform length and its radices, in stage order
+  int radix[kMaxStages];
+  float2 rc[5][6];     // (cos, sin)(2 pi q / p), q = 1 .. (p-1)/2, p = 3, 5, 7, 11, 13
+};
+
+// The rows one launch (or one batch item) filters.
+struct FilterRows {
   const float *src;
   long long srs, sss;  // src row / slice strides (elements)
-  int nrow, nslice, ncol, pad, mode, apply_log;
+  int nrow, nslice, ncol, pad;
   const float2 *spec;
   int spec_rows;
-  const float2 *tw;
-  int log2m;
   void *dst;
   long long drs, dss;
   int pair_within_angle;  // 1: a CTA takes slices 2q, 2q+1 of one angle
@@ -102,57 +121,100 @@ __device__ __forceinline__ void dft16(float2 *v) {
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = t[r];
 }
-template <int R> __device__ __forceinline__ void dft(float2 *v) {
+// odd P, forward: y_q = A_q - i B_q, y_{P-q} = A_q + i B_q with
+// A_q = v_0 + sum_r (v_r + v_{P-r}) cos(2 pi q r / P),
+// B_q = sum_r (v_r - v_{P-r}) sin(2 pi q r / P)
+template <int P>
+__device__ __forceinline__ void dft_odd(float2 *v, const float2 *rc) {
+  constexpr int H = (P - 1) / 2;
+  float2 s[H], d[H];
+  const float2 v0 = v[0];
+  float2 y0 = v0;
+#pragma unroll
+  for (int r = 1; r <= H; ++r) {
+    s[r - 1] = cadd(v[r], v[P - r]);
+    d[r - 1] = csub(v[r], v[P - r]);
+    y0 = cadd(y0, s[r - 1]);
+  }
+  v[0] = y0;
+#pragma unroll
+  for (int q = 1; q <= H; ++q) {
+    float2 A = v0, B = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int r = 1; r <= H; ++r) {
+      int t = (q * r) % P;
+      float sg = 1.f;
+      if (t > H) {  // sin(2 pi t / P) = -sin(2 pi (P - t) / P)
+        t = P - t;
+        sg = -1.f;
+      }
+      const float c = rc[t - 1].x, sn = sg * rc[t - 1].y;
+      A.x = fmaf(s[r - 1].x, c, A.x);
+      A.y = fmaf(s[r - 1].y, c, A.y);
+      B.x = fmaf(d[r - 1].x, sn, B.x);
+      B.y = fmaf(d[r - 1].y, sn, B.y);
+    }
+    v[q] = make_float2(A.x + B.y, A.y - B.x);      // A - i B
+    v[P - q] = make_float2(A.x - B.y, A.y + B.x);  // A + i B
+  }
+}
+template <int R> __device__ __forceinline__ void dft(float2 *v, const float2 *rc) {
   if constexpr (R == 2) dft2(v);
   else if constexpr (R == 4) dft4(v[0], v[1], v[2], v[3]);
   else if constexpr (R == 8) dft8(v);
-  else dft16(v);
+  else if constexpr (R == 16) dft16(v);
+  else dft_odd<R>(v, rc);
 }
 
-// Stockham stage of radix R after sub-transforms of length Ns = 2^logNs:
-// butterfly j reads x[j + r M/R], twiddles input r by w^(r k)
+__host__ __device__ constexpr int odd_slot(int p) { return p == 3 ? 0 : p == 5 ? 1 : p == 7 ? 2 : p == 11 ? 3 : 4; }
+
+// butterflies a thread holds per stage of radix R (at most ~32 values)
+__host__ __device__ constexpr int max_butterflies(int r) { return r >= 11 ? 2 : (r >= 5 ? 4 : 32 / r); }
+
+// Stockham stage of radix R after sub-transforms of length Ns: butterfly
+// j (< Q = n / R) reads x[j + r Q], twiddles input r by w^(r k)
 // (k = j mod Ns, w = exp(-2 pi i / (Ns R))), does an R-point DFT and writes
-// output r to x[(j - k) R + k + r Ns].  Every thread reads all of its inputs
-// before the barrier and writes after it, so one buffer suffices.
-// Twiddles exp(-2 pi i t / M) = ta[t >> L] * tb[t & (2^L - 1)] come from two
-// short tables in shared memory.
+// output q to x[(j - k) R + k + q Ns].  Every thread reads all of its
+// inputs before the barrier and writes after it, so one buffer suffices.
+// Twiddles exp(-2 pi i t / n) = ta[t / 64] * tb[t % 64] come from two short
+// tables in shared memory; w^r is the product of the table values of the
+// powers 1, 2, 4, 8 in r (at most three roundings, against 2 (R - 1) table
+// reads per butterfly).
 template <int R, int T>
-__device__ __forceinline__ void fft_stage(float2 *x, int log2m, int logNs, const float2 *ta, const float2 *tb,
-                                          int L) {
-  constexpr int logR = R == 2 ? 1 : (R == 4 ? 2 : (R == 8 ? 3 : 4));
-  const int M = 1 << log2m, Q = M >> logR;
-  constexpr int kMaxB = 32 / R;  // T >= M / 32 threads: at most 32 elements each
-  const int nb = (Q + T - 1) / T;
-  const int Ns = 1 << logNs;
-  const int tsh = log2m - logR - logNs;
-  const int lmask = (1 << L) - 1;
-  float2 v[kMaxB][R];
+__device__ __forceinline__ void fft_stage(float2 *x, const FilterPlan &a, int Ns, const float2 *ta,
+                                          const float2 *tb) {
+  constexpr int kB = max_butterflies(R);
+  const int n = a.n, Q = n / R, tstep = n / (Ns * R);
+  float2 rc[6];
+  if constexpr (R % 2 == 1) {
 #pragma unroll
-  for (int b = 0; b < kMaxB; ++b) {
+    for (int t = 0; t < (R - 1) / 2; ++t) rc[t] = a.rc[odd_slot(R)][t];
+  }
+  float2 v[kB][R];
+#pragma unroll
+  for (int b = 0; b < kB; ++b) {
     const int j = threadIdx.x + b * T;
-    if (b < nb && j < Q) {
+    if (j < Q) {
 #pragma unroll
       for (int r = 0; r < R; ++r) v[b][r] = x[pidx(j + r * Q)];
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int b = 0; b < kMaxB; ++b) {
+  for (int b = 0; b < kB; ++b) {
     const int j = threadIdx.x + b * T;
-    if (b < nb && j < Q) {
-      const int k = j & (Ns - 1);
+    if (j < Q) {
+      const int k = j % Ns;
       if (k) {
-        // w^(r k) for r = 1 .. R-1: the powers 1, 2, 4, 8 of w^k from the
-        // tables, each other one the product of those of its set bits (at
-        // most three roundings), against 2 (R - 1) table reads per butterfly
+        const int e = k * tstep;  // w^r = exp(-2 pi i r e / n)
         auto tw = [&](int c) {
-          const int t = (c * k) << tsh;
-          return cmul(ta[t >> L], tb[t & lmask]);
+          const int t = c * e;
+          return cmul(ta[t >> 6], tb[t & (kTwLo - 1)]);
         };
         const float2 w1 = tw(1);
-        const float2 w2 = R >= 4 ? tw(2) : w1;
-        const float2 w4 = R >= 8 ? tw(4) : w1;
-        const float2 w8 = R >= 16 ? tw(8) : w1;
+        const float2 w2 = R >= 3 ? tw(2) : w1;
+        const float2 w4 = R >= 5 ? tw(4) : w1;
+        const float2 w8 = R >= 9 ? tw(8) : w1;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           float2 w = (r & 1) ? w1 : ((r & 2) ? w2 : ((r & 4) ? w4 : w8));
@@ -162,8 +224,8 @@ __device__ __forceinline__ void fft_stage(float2 *x, int log2m, int logNs, const
           v[b][r] = cmul(v[b][r], w);
         }
       }
-      dft<R>(v[b]);
-      const int o = ((j - k) << logR) + k;
+      dft<R>(v[b], rc);
+      const int o = (j - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) x[pidx(o + r * Ns)] = v[b][r];
     }
@@ -171,20 +233,25 @@ __device__ __forceinline__ void fft_stage(float2 *x, int log2m, int logNs, const
   __syncthreads();
 }
 
-// In-place forward FFT of length M = 2^log2m: one radix-2/4/8 stage for
-// the remainder of log2m / 4, then radix-16 stages.  Force-inlined: called
-// from two kernels, the compiler otherwise emits it as a real call whose
-// ABI costs a 672-byte stack frame and a third of the filter's speed.
+// In-place forward FFT of length a.n through the plan's stages, which come
+// in a fixed order (16s, one 8 / 4 / 2, then 13s, 11s, 7s, 5s, 3s): one
+// inlined copy of each stage kind in sequence (a switch inside a loop over
+// the stages makes the compiler spill).  Force-inlined: called twice per
+// kernel, the compiler otherwise emits it as a real call whose ABI costs a
+// large stack frame and much of the speed.
 template <int T>
-__device__ __forceinline__ void fft_forward(float2 *x, int log2m, const float2 *ta, const float2 *tb, int L) {
-  int logNs = 0;
-  switch (log2m & 3) {
-    case 1: fft_stage<2, T>(x, log2m, 0, ta, tb, L); logNs = 1; break;
-    case 2: fft_stage<4, T>(x, log2m, 0, ta, tb, L); logNs = 2; break;
-    case 3: fft_stage<8, T>(x, log2m, 0, ta, tb, L); logNs = 3; break;
-    default: break;
-  }
-  for (; logNs < log2m; logNs += 4) fft_stage<16, T>(x, log2m, logNs, ta, tb, L);
+__device__ __forceinline__ void fft_forward(float2 *x, const FilterPlan &a, const float2 *ta, const float2 *tb) {
+  int s = 0, Ns = 1;
+  const int ns = a.nstages;
+  for (; s < ns && a.radix[s] == 16; ++s, Ns *= 16) fft_stage<16, T>(x, a, Ns, ta, tb);
+  if (s < ns && a.radix[s] == 8) { fft_stage<8, T>(x, a, Ns, ta, tb); ++s; Ns *= 8; }
+  if (s < ns && a.radix[s] == 4) { fft_stage<4, T>(x, a, Ns, ta, tb); ++s; Ns *= 4; }
+  if (s < ns && a.radix[s] == 2) { fft_stage<2, T>(x, a, Ns, ta, tb); ++s; Ns *= 2; }
+  for (; s < ns && a.radix[s] == 13; ++s, Ns *= 13) fft_stage<13, T>(x, a, Ns, ta, tb);
+  for (; s < ns && a.radix[s] == 11; ++s, Ns *= 11) fft_stage<11, T>(x, a, Ns, ta, tb);
+  for (; s < ns && a.radix[s] == 7; ++s, Ns *= 7) fft_stage<7, T>(x, a, Ns, ta, tb);
+  for (; s < ns && a.radix[s] == 5; ++s, Ns *= 5) fft_stage<5, T>(x, a, Ns, ta, tb);
+  for (; s < ns && a.radix[s] == 3; ++s, Ns *= 3) fft_stage<3, T>(x, a, Ns, ta, tb);
 }
 
 // Block-wide reduction over T threads (op: 0 sum, 1 max, 2 min).
@@ -249,20 +316,20 @@ __device__ float2 block_select2(const float2 *x, int pad, int ncol, int rank, fl
   return make_float2(fkey_inv(lo1), fkey_inv(lo2));
 }
 
-// Filters row pair `pair` of a (CTA-uniform).
+// Filters row pair `pair` of the rows a with the plan p (CTA-uniform).
 template <typename OutT, int T>
-__device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) {
-  extern __shared__ float2 sm[];  // M complex, padded by pidx
+__device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const FilterRows &a, int pair) {
+  extern __shared__ float2 sm[];  // n complex, padded by pidx
   __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
-  __shared__ float2 ta[128], tb[128];
-  const int log2m = a.log2m, M = 1 << log2m;
-  const int L = (log2m + 1) >> 1;
+  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
+  const int M = p.n;
   const int ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad;
   const int tid = threadIdx.x;
+  if (N > M) return;  // not a length for these rows (CTA-uniform)
 
-  // twiddle tables: ta[u] = w^(u 2^L), tb[v] = w^v, w = exp(-2 pi i / M)
-  for (int u = tid; u < (M >> L); u += T) ta[u] = __ldg(a.tw + (u << L));
-  for (int v = tid; v < (1 << L); v += T) tb[v] = __ldg(a.tw + v);
+  // twiddle tables: ta[u] = w^(64 u), tb[v] = w^v, w = exp(-2 pi i / n)
+  for (int u = tid; u < (M + kTwLo - 1) / kTwLo; u += T) ta[u] = __ldg(p.tw + u * kTwLo);
+  for (int v = tid; v < kTwLo; v += T) tb[v] = v < M ? __ldg(p.tw + v) : make_float2(1.f, 0.f);
 
   // the two rows (angle, slice) of this CTA
   int i1, k1, i2, k2;
@@ -291,7 +358,7 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
   for (int j = tid; j < ncol; j += T) {
     float v1 = __ldg(s1 + j);
     float v2 = ok2 ? __ldg(s2 + j) : 0.0f;
-    if (a.apply_log) { v1 = atb::neg_log(v1); v2 = ok2 ? atb::neg_log(v2) : 0.0f; }
+    if (p.apply_log) { v1 = atb::neg_log(v1); v2 = ok2 ? atb::neg_log(v2) : 0.0f; }
     sm[pidx(pad + j)] = make_float2(v1, v2);
   }
   for (int m = N + tid; m < M; m += T) sm[pidx(m)] = make_float2(0.f, 0.f);
@@ -300,8 +367,8 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
   // 2. padding (numpy.pad semantics along the row)
   if (pad > 0) {
     float2 stat = make_float2(0.f, 0.f);
-    if (a.mode == ATB_PAD_MEAN || a.mode == ATB_PAD_MAXIMUM || a.mode == ATB_PAD_MINIMUM) {
-      const int op = a.mode == ATB_PAD_MEAN ? 0 : (a.mode == ATB_PAD_MAXIMUM ? 1 : 2);
+    if (p.mode == ATB_PAD_MEAN || p.mode == ATB_PAD_MAXIMUM || p.mode == ATB_PAD_MINIMUM) {
+      const int op = p.mode == ATB_PAD_MEAN ? 0 : (p.mode == ATB_PAD_MAXIMUM ? 1 : 2);
       float2 acc = op == 0 ? make_float2(0.f, 0.f)
                            : (op == 1 ? make_float2(-FLT_MAX, -FLT_MAX) : make_float2(FLT_MAX, FLT_MAX));
       for (int j = tid; j < ncol; j += T) {
@@ -312,7 +379,7 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
       }
       stat = block_reduce2<T>(acc, op, scratch);
       if (op == 0) { stat.x /= (float)ncol; stat.y /= (float)ncol; }
-    } else if (a.mode == ATB_PAD_MEDIAN) {
+    } else if (p.mode == ATB_PAD_MEDIAN) {
       const float2 lo = block_select2<T>(sm, pad, ncol, (ncol - 1) / 2, scratch);
       if (ncol & 1) {
         stat = lo;
@@ -326,7 +393,7 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
       const int m = left ? t : ncol + t;   // position in the padded row
       const int q = m - pad;               // position relative to the row
       float2 v;
-      switch (a.mode) {
+      switch (p.mode) {
         case ATB_PAD_EDGE: v = sm[pidx(pad + (left ? 0 : ncol - 1))]; break;
         case ATB_PAD_CONSTANT: v = make_float2(0.f, 0.f); break;
         case ATB_PAD_WRAP: v = sm[pidx(pad + ((q % ncol) + ncol) % ncol)]; break;
@@ -363,14 +430,14 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
 
   // 3. forward transform, spectral product (conjugated), second forward
   //    transform = conjugated inverse
-  fft_forward<T>(sm, log2m, ta, tb, L);
+  fft_forward<T>(sm, p, ta, tb);
   const float2 *spec = a.spec + (a.spec_rows > 1 ? (long long)i1 * M : 0LL);
   for (int k = tid; k < M; k += T) {
     const float2 y = cmul(sm[pidx(k)], __ldg(spec + k));
     sm[pidx(k)] = make_float2(y.x, -y.y);
   }
   __syncthreads();
-  fft_forward<T>(sm, log2m, ta, tb, L);
+  fft_forward<T>(sm, p, ta, tb);
 
   // 4. crop: real part -> row 1, -imag part -> row 2
   OutT *d1 = reinterpret_cast<OutT *>(a.dst) + i1 * a.drs + k1 * a.dss;
@@ -383,33 +450,34 @@ __device__ __forceinline__ void filter_rows_body(const FilterArgs &a, int pair) 
 }
 
 template <typename OutT, int T>
-__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1) filter_rows_kernel(FilterArgs a) {
-  filter_rows_body<OutT, T>(a, (int)blockIdx.x);
+__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
+    filter_rows_kernel(const __grid_constant__ FilterPlan p, const __grid_constant__ FilterRows a) {
+  filter_rows_body<OutT, T>(p, a, (int)blockIdx.x);
 }
 
 // One launch over the row pairs of several single-slice sinograms that
-// share the FFT length: CTA p finds the item whose pair range holds p
+// share the transform length: CTA q finds the item whose pair range holds q
 // (binary search on pair_offset) and filters that pair.
 template <typename OutT, int T>
 __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
-    filter_batch_kernel(FilterArgs a, const atb_filter_item *items, int nitems) {
-  const int p = blockIdx.x;
+    filter_batch_kernel(const __grid_constant__ FilterPlan p, const atb_filter_item *items, int nitems) {
+  const int q = blockIdx.x;
   int lo = 0, hi = nitems - 1;
-  while (lo < hi) {  // last item with pair_offset <= p
+  while (lo < hi) {  // last item with pair_offset <= q
     const int mid = (lo + hi + 1) >> 1;
-    if (items[mid].pair_offset <= p) lo = mid; else hi = mid - 1;
+    if (items[mid].pair_offset <= q) lo = mid; else hi = mid - 1;
   }
   const atb_filter_item it = items[lo];
-  const int pair = p - it.pair_offset;
+  const int pair = q - it.pair_offset;
   if (pair < 0 || pair >= (it.nrow + 1) / 2) return;  // CTA-uniform
-  FilterArgs b = a;
+  FilterRows b;
   b.src = it.src; b.srs = it.src_row_stride; b.sss = 0;
   b.nrow = it.nrow; b.nslice = 1; b.ncol = it.ncol; b.pad = it.pad;
   b.spec = reinterpret_cast<const float2 *>(it.spec); b.spec_rows = 1;
   b.dst = it.dst; b.drs = it.dst_row_stride; b.dss = 0;
   b.pair_within_angle = 0;
   b.pairs_per_angle = 0;
-  filter_rows_body<OutT, T>(b, pair);
+  filter_rows_body<OutT, T>(p, b, pair);
 }
 
 __global__ void neg_log_kernel(const float *__restrict__ src, long long srs, long long sss, int nrow,
@@ -424,44 +492,160 @@ __global__ void neg_log_kernel(const float *__restrict__ src, long long srs, lon
   }
 }
 
+// ---- host side: transform length, plan, launches
+
+bool smooth(int t, const int *primes, int np) {
+  for (int k = 0; k < np; ++k)
+    while (t % primes[k] == 0) t /= primes[k];
+  return t == 1;
+}
+
+// radices of n in stage order: 16s, one 8 / 4 / 2 for the rest of the
+// power of two, then the odd ones
+bool make_radices(int n, int *radix, int &nstages) {
+  nstages = 0;
+  int r = n;
+  auto push = [&](int p) {
+    if (nstages >= kMaxStages) return false;
+    radix[nstages++] = p;
+    r /= p;
+    return true;
+  };
+  while (r % 16 == 0)
+    if (!push(16)) return false;
+  for (int p : {8, 4, 2})
+    if (r % p == 0 && !push(p)) return false;
+  static const int odd[] = {13, 11, 7, 5, 3};
+  for (int p : odd)
+    while (r % p == 0)
+      if (!push(p)) return false;
+  return r == 1;
+}
+
+// approximate flops per point of a stage of radix r (butterfly + twiddles)
+double stage_cost(int r) {
+  switch (r) {
+    case 2: return 5.0;
+    case 4: return 8.5;
+    case 8: return 13.3;
+    case 16: return 16.6;
+    case 3: return 9.3;
+    case 5: return 15.2;
+    case 7: return 19.7;
+    case 11: return 28.2;
+    default: return 32.3;  // 13
+  }
+}
+
+double transform_cost(int n) {
+  int radix[kMaxStages], ns = 0;
+  if (!make_radices(n, radix, ns)) return INFINITY;
+  double c = 0.0;
+  for (int k = 0; k < ns; ++k) c += stage_cost(radix[k]);
+  return c * n;
+}
+
+// threads per CTA: the fewest (a multiple of 32, at least 64) for which
+// every stage's butterflies fit the per-thread register budget
+int threads_for(int n, const int *radix, int ns) {
+  int need = 64;
+  for (int k = 0; k < ns; ++k) {
+    const int q = n / radix[k], b = max_butterflies(radix[k]);
+    const int t = (q + b - 1) / b;
+    if (t > need) need = t;
+  }
+  for (int t : {64, 128, 256, 512})
+    if (t >= need) return t;
+  return -1;
+}
+
+int filter_length(int ncol, int pad) {
+  static const int p13[] = {2, 3, 5, 7, 11, 13};
+  static const int p7[] = {2, 3, 5, 7};
+  const long long n = (long long)ncol + 2LL * pad;
+  int best = -1;
+  double best_cost = INFINITY;
+  if (n >= 2 && n <= kMaxLen && smooth((int)n, p13, 6)) {
+    best = (int)n;
+    best_cost = transform_cost(best);
+  }
+  // the embedding: 7-smooth lengths from N + ncol - 1 up to the next power of two
+  const long long lo = std::max(16LL, n + ncol - 1);
+  long long hi = 16;
+  while (hi < lo) hi <<= 1;
+  for (long long m = lo; m <= hi && m <= kMaxLen; ++m) {
+    if (!smooth((int)m, p7, 4)) continue;
+    const double c = transform_cost((int)m);
+    if (c < best_cost) {
+      best_cost = c;
+      best = (int)m;
+    }
+  }
+  return best;
+}
+
+// whether n is an exact transform length for rows of ncol + 2 pad samples
+bool valid_length(int n, int ncol, int pad) {
+  const long long N = (long long)ncol + 2LL * pad;
+  return n >= 2 && n <= kMaxLen && (n == N || n >= N + ncol - 1);
+}
+
+// the plan of length n (false: no radix plan or thread count for it)
+bool make_plan(int n, int mode, int apply_log, const void *twiddle, FilterPlan &p, int &threads) {
+  if (n < 2 || n > kMaxLen) return false;
+  p.mode = mode;
+  p.apply_log = apply_log ? 1 : 0;
+  p.tw = reinterpret_cast<const float2 *>(twiddle);
+  p.n = n;
+  if (!make_radices(n, p.radix, p.nstages)) return false;
+  static const int op[5] = {3, 5, 7, 11, 13};
+  for (int k = 0; k < 5; ++k)
+    for (int q = 0; q < 6; ++q) {
+      const double ang = 2.0 * M_PI * (double)(q + 1) / (double)op[k];
+      p.rc[k][q] = q < (op[k] - 1) / 2 ? make_float2((float)std::cos(ang), (float)std::sin(ang)) : make_float2(0.f, 0.f);
+    }
+  threads = threads_for(n, p.radix, p.nstages);
+  return threads > 0;
+}
+
+size_t smem_bytes(int n) { return sizeof(float2) * (size_t)(n + (n >> 4) + 1); }
+
 template <typename OutT, int T>
-int launch_filter_t(const FilterArgs &a, long long npairs, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (size_t)((1 << a.log2m) + ((1 << a.log2m) >> 4));
+int launch_filter_t(const FilterPlan &p, const FilterRows &a, long long npairs, cudaStream_t st) {
+  const size_t smem = smem_bytes(p.n);
   const int rc = atb::ensure_smem(filter_rows_kernel<OutT, T>, smem, "atb_filter_rows");
   if (rc != ATB_OK) return rc;
-  filter_rows_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(a);
+  filter_rows_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(p, a);
   return atb::check_launch("atb_filter_rows");
 }
 
+template <typename OutT>
+int launch_filter(const FilterPlan &p, const FilterRows &a, int threads, long long npairs, cudaStream_t st) {
+  switch (threads) {
+    case 512: return launch_filter_t<OutT, 512>(p, a, npairs, st);
+    case 256: return launch_filter_t<OutT, 256>(p, a, npairs, st);
+    case 128: return launch_filter_t<OutT, 128>(p, a, npairs, st);
+    default: return launch_filter_t<OutT, 64>(p, a, npairs, st);
+  }
+}
+
 template <typename OutT, int T>
-int launch_batch_t(const FilterArgs &a, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * (size_t)((1 << a.log2m) + ((1 << a.log2m) >> 4));
+int launch_batch_t(const FilterPlan &p, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
+  const size_t smem = smem_bytes(p.n);
   const int rc = atb::ensure_smem(filter_batch_kernel<OutT, T>, smem, "atb_filter_rows_batch");
   if (rc != ATB_OK) return rc;
-  filter_batch_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(a, items, nitems);
+  filter_batch_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(p, items, nitems);
   return atb::check_launch("atb_filter_rows_batch");
 }
 
 template <typename OutT>
-int launch_batch(const FilterArgs &a, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
-  switch (a.log2m) {
-    case 14: return launch_batch_t<OutT, 512>(a, items, nitems, npairs, st);
-    case 13: return launch_batch_t<OutT, 256>(a, items, nitems, npairs, st);
-    case 12: return launch_batch_t<OutT, 128>(a, items, nitems, npairs, st);
-    case 11: return launch_batch_t<OutT, 64>(a, items, nitems, npairs, st);
-    default: return launch_batch_t<OutT, 32>(a, items, nitems, npairs, st);
-  }
-}
-
-// T = max(32, M / 32): every thread holds 32 complex values per stage
-template <typename OutT>
-int launch_filter(const FilterArgs &a, long long npairs, cudaStream_t st) {
-  switch (a.log2m) {
-    case 14: return launch_filter_t<OutT, 512>(a, npairs, st);
-    case 13: return launch_filter_t<OutT, 256>(a, npairs, st);
-    case 12: return launch_filter_t<OutT, 128>(a, npairs, st);
-    case 11: return launch_filter_t<OutT, 64>(a, npairs, st);
-    default: return launch_filter_t<OutT, 32>(a, npairs, st);
+int launch_batch(const FilterPlan &p, int threads, const atb_filter_item *items, int nitems, int npairs,
+                 cudaStream_t st) {
+  switch (threads) {
+    case 512: return launch_batch_t<OutT, 512>(p, items, nitems, npairs, st);
+    case 256: return launch_batch_t<OutT, 256>(p, items, nitems, npairs, st);
+    case 128: return launch_batch_t<OutT, 128>(p, items, nitems, npairs, st);
+    default: return launch_batch_t<OutT, 64>(p, items, nitems, npairs, st);
   }
 }
 
@@ -469,20 +653,18 @@ int launch_filter(const FilterArgs &a, long long npairs, cudaStream_t st) {
 
 extern "C" {
 
-int atb_filter_log2m(int ncol, int pad) {
-  if (ncol < 1 || pad < 0) return atb::fail(ATB_EINVAL, "atb_filter_log2m: ncol=%d pad=%d", ncol, pad);
-  const long long need = (long long)ncol + 2LL * pad + ncol - 1;
-  int l = kMinLog2M;
-  while ((1LL << l) < need) ++l;
-  if (l > kMaxLog2M)
-    return atb::fail(ATB_ERANGE, "atb_filter_log2m: ncol=%d pad=%d needs FFT length 2^%d > 2^%d", ncol, pad, l,
-                     kMaxLog2M);
-  return l;
+int atb_filter_length(int ncol, int pad) {
+  if (ncol < 1 || pad < 0) return atb::fail(ATB_EINVAL, "atb_filter_length: ncol=%d pad=%d", ncol, pad);
+  const int n = filter_length(ncol, pad);
+  if (n < 0)
+    return atb::fail(ATB_ERANGE, "atb_filter_length: ncol=%d pad=%d needs a transform longer than %d", ncol, pad,
+                     kMaxLen);
+  return n;
 }
 
 int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_stride, int nrow, int nslice,
                     int ncol, int pad, int pad_mode, int apply_log, const void *spec, int spec_rows,
-                    const void *twiddle, int log2m, void *dst, int dst_dtype, int64_t dst_row_stride,
+                    const void *twiddle, int fft_len, void *dst, int dst_dtype, int64_t dst_row_stride,
                     int64_t dst_slice_stride, void *stream) {
   if (!src || !dst || !spec || !twiddle) return atb::fail(ATB_EINVAL, "atb_filter_rows: null pointer");
   if (nrow < 1 || nslice < 1 || ncol < 1 || pad < 0)
@@ -490,17 +672,17 @@ int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_
                      ncol, pad);
   if (pad_mode < ATB_PAD_EDGE || pad_mode > ATB_PAD_MEDIAN)
     return atb::fail(ATB_EINVAL, "atb_filter_rows: unknown pad_mode %d", pad_mode);
-  if (log2m < kMinLog2M || log2m > kMaxLog2M)
-    return atb::fail(ATB_ERANGE, "atb_filter_rows: log2m=%d outside [%d, %d]", log2m, kMinLog2M, kMaxLog2M);
-  if ((1LL << log2m) < (long long)ncol + 2LL * pad + ncol - 1)
-    return atb::fail(ATB_EINVAL, "atb_filter_rows: 2^%d < ncol + 2 pad + ncol - 1", log2m);
   if (spec_rows != 1 && spec_rows != nrow)
     return atb::fail(ATB_EINVAL, "atb_filter_rows: spec_rows=%d must be 1 or nrow=%d", spec_rows, nrow);
-  FilterArgs a;
+  FilterPlan p;
+  int threads = 0;
+  if (!valid_length(fft_len, ncol, pad) || !make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads))
+    return atb::fail(ATB_EINVAL, "atb_filter_rows: fft_len=%d is not a transform length for ncol=%d pad=%d "
+                     "(atb_filter_length gives one)", fft_len, ncol, pad);
+  FilterRows a;
   a.src = src; a.srs = src_row_stride; a.sss = src_slice_stride;
-  a.nrow = nrow; a.nslice = nslice; a.ncol = ncol; a.pad = pad; a.mode = pad_mode; a.apply_log = apply_log;
+  a.nrow = nrow; a.nslice = nslice; a.ncol = ncol; a.pad = pad;
   a.spec = reinterpret_cast<const float2 *>(spec); a.spec_rows = spec_rows;
-  a.tw = reinterpret_cast<const float2 *>(twiddle); a.log2m = log2m;
   a.dst = dst; a.drs = dst_row_stride; a.dss = dst_slice_stride;
   long long npairs;
   if (spec_rows > 1) {
@@ -515,34 +697,30 @@ int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_
   if (npairs > 0x7fffffffLL) return atb::fail(ATB_ERANGE, "atb_filter_rows: too many rows");
   cudaStream_t st = atb::as_stream(stream);
   switch (dst_dtype) {
-    case ATB_F32: return launch_filter<float>(a, npairs, st);
-    case ATB_F16: return launch_filter<__half>(a, npairs, st);
-    case ATB_BF16: return launch_filter<__nv_bfloat16>(a, npairs, st);
+    case ATB_F32: return launch_filter<float>(p, a, threads, npairs, st);
+    case ATB_F16: return launch_filter<__half>(p, a, threads, npairs, st);
+    case ATB_BF16: return launch_filter<__nv_bfloat16>(p, a, threads, npairs, st);
     default: return atb::fail(ATB_EINVAL, "atb_filter_rows: unknown dst_dtype %d", dst_dtype);
   }
 }
 
 int atb_filter_rows_batch(const atb_filter_item *items, int nitems, int npairs, int pad_mode, int apply_log,
-                          const void *twiddle, int log2m, int dst_dtype, void *stream) {
+                          const void *twiddle, int fft_len, int dst_dtype, void *stream) {
   if (!items || !twiddle) return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: null pointer");
   if (nitems < 1 || npairs < 1) return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: empty batch");
   if (pad_mode < ATB_PAD_EDGE || pad_mode > ATB_PAD_MEDIAN)
     return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown pad_mode %d", pad_mode);
-  if (log2m < kMinLog2M || log2m > kMaxLog2M)
-    return atb::fail(ATB_ERANGE, "atb_filter_rows_batch: log2m=%d outside [%d, %d]", log2m, kMinLog2M, kMaxLog2M);
-  FilterArgs a;
-  a.src = nullptr; a.srs = 0; a.sss = 0;
-  a.nrow = 0; a.nslice = 1; a.ncol = 0; a.pad = 0; a.mode = pad_mode; a.apply_log = apply_log;
-  a.spec = nullptr; a.spec_rows = 1;
-  a.tw = reinterpret_cast<const float2 *>(twiddle); a.log2m = log2m;
-  a.dst = nullptr; a.drs = 0; a.dss = 0;
-  a.pair_within_angle = 0;
-  a.pairs_per_angle = 0;
+  FilterPlan p;
+  int threads = 0;
+  // every item needs fft_len == its N or fft_len >= N + ncol - 1; the
+  // kernel skips items longer than fft_len
+  if (!make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads))
+    return atb::fail(ATB_ERANGE, "atb_filter_rows_batch: fft_len=%d has no plan", fft_len);
   cudaStream_t st = atb::as_stream(stream);
   switch (dst_dtype) {
-    case ATB_F32: return launch_batch<float>(a, items, nitems, npairs, st);
-    case ATB_F16: return launch_batch<__half>(a, items, nitems, npairs, st);
-    case ATB_BF16: return launch_batch<__nv_bfloat16>(a, items, nitems, npairs, st);
+    case ATB_F32: return launch_batch<float>(p, threads, items, nitems, npairs, st);
+    case ATB_F16: return launch_batch<__half>(p, threads, items, nitems, npairs, st);
+    case ATB_BF16: return launch_batch<__nv_bfloat16>(p, threads, items, nitems, npairs, st);
     default: return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown dst_dtype %d", dst_dtype);
   }
 }

@@ -23,6 +23,39 @@ from .. import _native as nat
 from . import reconstruction as R
 
 
+def _pow2_at_least(n):
+    top = 16
+    while top < n:
+        top *= 2
+    return top
+
+
+def _group_lengths(needs):
+    """Transform lengths of the items' filters in a batch, from each item's
+    exact-embedding bound N + ncol - 1: items whose bounds share a power of
+    two share one length, the smallest 7-smooth length covering all of them
+    (the per-slice filter's own choice, ``atb_filter_length``, is often N
+    itself, which differs with every width, and would cost one launch per
+    width)."""
+    groups = {}
+    for need in needs:
+        top = _pow2_at_least(need)
+        groups[top] = max(groups.get(top, 0), need)
+    length = {}
+    for top, need in groups.items():
+        m = max(16, need)
+        while True:
+            r = m
+            for q in (2, 3, 5, 7):
+                while r % q == 0:
+                    r //= q
+            if r == 1:
+                break
+            m += 1
+        length[top] = m
+    return [length[_pow2_at_least(need)] for need in needs]
+
+
 class BatchedFBP:
     """A fixed batch geometry with device buffers, runnable and capturable.
 
@@ -43,9 +76,13 @@ class BatchedFBP:
                              "per item")
         self.filter_name, self.pad_mode = filter_name, pad_mode
         self.inputs, self.filtered, self.outputs = [], [], []
-        self._trig, self._spec, self._pad, self._log2m = [], [], [], []
+        self._trig, self._spec, self._pad, self._flen = [], [], [], []
         self._tw = []
         items = (nat.BpItem * self.n)()
+        pads = [min(int(0.15 * int(c)), 150) if pad is None else int(pad)
+                for _, c in shapes]
+        flens = _group_lengths([2 * int(c) + 2 * q - 1
+                                for (_, c), q in zip(shapes, pads)])
         for b, ((nrow, ncol), cen, ang) in enumerate(zip(shapes, centers,
                                                          angles)):
             nrow, ncol = int(nrow), int(ncol)
@@ -55,9 +92,8 @@ class BatchedFBP:
             if cen < 0 or cen >= ncol:
                 raise ValueError("item %d: Center is out of the range "
                                  "[0, %d]" % (b, ncol - 1))
-            p = min(int(0.15 * ncol), 150) if pad is None else int(pad)
-            log2m = nat.call("atb_filter_log2m", ncol, p)
-            spec, _ = R._spectrum(None, filter_name, nrow, ncol, p, log2m,
+            p, flen = pads[b], flens[b]
+            spec, _ = R._spectrum(None, filter_name, nrow, ncol, p, flen,
                                   self.dev)
             x = torch.zeros((nrow, ncol), dtype=torch.float32,
                             device=self.dev)
@@ -71,8 +107,8 @@ class BatchedFBP:
             self._trig.append(trig)
             self._spec.append(spec)
             self._pad.append(p)
-            self._log2m.append(log2m)
-            self._tw.append(R._twiddle(log2m, self.dev))
+            self._flen.append(flen)
+            self._tw.append(R._twiddle(flen, self.dev))
             it = items[b]
             it.sino, it.sino_row_stride = f.data_ptr(), f.stride(0)
             it.trig = trig.data_ptr()
@@ -85,11 +121,11 @@ class BatchedFBP:
         raw = bytes(items)
         self.items_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8
                                           ).to(self.dev)
-        # one filter launch per FFT length: a device table of the items
-        # that share it, each with the index of its first row pair
+        # one filter launch per transform length: a device table of the
+        # items that share it, each with the index of its first row pair
         self._filter_groups = []
-        for log2m in sorted(set(self._log2m)):
-            members = [b for b in range(self.n) if self._log2m[b] == log2m]
+        for flen in sorted(set(self._flen)):
+            members = [b for b in range(self.n) if self._flen[b] == flen]
             tab = (nat.FilterItem * len(members))()
             off = 0
             for e, b in enumerate(members):
@@ -104,7 +140,7 @@ class BatchedFBP:
                 off += (x.shape[0] + 1) // 2
             dev_tab = torch.frombuffer(bytearray(bytes(tab)),
                                        dtype=torch.uint8).to(self.dev)
-            self._filter_groups.append((log2m, len(members), off, dev_tab,
+            self._filter_groups.append((flen, len(members), off, dev_tab,
                                         self._tw[members[0]]))
         self.counter = torch.zeros(2, dtype=torch.int32, device=self.dev)
         self.graph = None
@@ -134,19 +170,20 @@ class BatchedFBP:
         self.graph = None
 
     def launch_plan(self):
-        """The launches of one :meth:`launch`: one filter launch per FFT
-        length among the items, then the persistent back-projection."""
-        return [("atb_filter_rows_batch", log2m, n, pairs)
-                for log2m, n, pairs, _, _ in self._filter_groups] + \
+        """The launches of one :meth:`launch`: one filter launch per
+        transform length among the items, then the persistent
+        back-projection."""
+        return [("atb_filter_rows_batch", flen, n, pairs)
+                for flen, n, pairs, _, _ in self._filter_groups] + \
             [("atb_backproject_batch", self.n, self.nunits)]
 
     def launch(self, max_ctas=0):
-        """Filter every item (one launch per FFT length), then one
+        """Filter every item (one launch per transform length), then one
         persistent back-projection launch."""
         st = R._stream_ptr(self.dev)
-        for log2m, n, pairs, tab, tw in self._filter_groups:
+        for flen, n, pairs, tab, tw in self._filter_groups:
             nat.call("atb_filter_rows_batch", tab.data_ptr(), n, pairs,
-                     nat.PAD_MODES[self.pad_mode], 0, tw.data_ptr(), log2m,
+                     nat.PAD_MODES[self.pad_mode], 0, tw.data_ptr(), flen,
                      nat.F32, st)
         nat.call("atb_backproject_batch", self.items_dev.data_ptr(), self.n,
                  self.units_dev.data_ptr(), self.nunits,

@@ -89,25 +89,26 @@ def _trig(angles, device):
     return t
 
 
-def _twiddle(log2m, device):
-    key = (log2m, device)
+def _twiddle(m, device):
+    key = (m, device)
     t = _tw_cache.get(key)
     if t is None:
-        tw = win.twiddles(log2m)
+        tw = win.twiddles(m)
         t = torch.from_numpy(tw.view(np.float32).copy()).to(device)
         _tw_cache[key] = t
     return t
 
 
-def _spectrum(ramp_win, filter_name, nrow, ncol, pad, log2m, device):
-    """Device spectrum [1 or nrow, M] for the row filter."""
+def _spectrum(ramp_win, filter_name, nrow, ncol, pad, m, device):
+    """Device spectrum [1 or nrow, m] for the row filter (transform length
+    m from ``atb_filter_length``)."""
     n = ncol + 2 * pad
     if ramp_win is None or np.shape(ramp_win) != (nrow, n):
-        key = (filter_name, ncol, pad, log2m, device)
+        key = (filter_name, ncol, pad, m, device)
         t = _spec_cache.get(key)
         if t is None:
             sp = win.row_filter_spectrum(win.ramp_window_row(n, filter_name),
-                                         ncol, pad, log2m)
+                                         ncol, pad, m)
             t = torch.from_numpy(sp.view(np.float32).copy()).to(device)
             if len(_spec_cache) > 32:
                 _spec_cache.clear()
@@ -116,7 +117,7 @@ def _spectrum(ramp_win, filter_name, nrow, ncol, pad, log2m, device):
     rw = np.asarray(ramp_win.cpu() if isinstance(ramp_win, torch.Tensor)
                     else ramp_win)
     rows = rw[:1] if np.all(rw == rw[:1]) else rw
-    sp = win.row_filter_spectrum(rows, ncol, pad, log2m)
+    sp = win.row_filter_spectrum(rows, ncol, pad, m)
     return torch.from_numpy(sp.view(np.float32).copy()).to(device), len(rows)
 
 
@@ -134,16 +135,16 @@ def filter_sinograms(sino3, pad, pad_mode="edge", apply_log=False,
     nrow, nslice, ncol = sino3.shape
     if pad_mode not in nat.PAD_MODES:
         raise ValueError("pad_mode %r is not supported" % (pad_mode,))
-    log2m = nat.call("atb_filter_log2m", int(ncol), int(pad))
+    m = nat.call("atb_filter_length", int(ncol), int(pad))
     dev = sino3.device
-    spec, spec_rows = _spectrum(ramp_win, filter_name, nrow, ncol, pad, log2m,
+    spec, spec_rows = _spectrum(ramp_win, filter_name, nrow, ncol, pad, m,
                                 dev)
     tdtype, code = _STORAGE[storage]
     out = torch.empty((nrow, nslice, ncol), dtype=tdtype, device=dev)
     nat.call("atb_filter_rows", sino3.data_ptr(), sino3.stride(0),
              sino3.stride(1), nrow, nslice, ncol, int(pad),
              nat.PAD_MODES[pad_mode], int(bool(apply_log)), spec.data_ptr(),
-             spec_rows, _twiddle(log2m, dev).data_ptr(), log2m,
+             spec_rows, _twiddle(m, dev).data_ptr(), m,
              out.data_ptr(), code, out.stride(0), out.stride(1),
              _stream_ptr(dev))
     return out

@@ -164,13 +164,13 @@ def _flat_log(raw, code, dark, flat_dark, apply_log, out, nonpos):
              R._stream_ptr(raw.device))
 
 
-def _filter_rows(x3, pad, pad_mode, spec, log2m, out3):
+def _filter_rows(x3, pad, pad_mode, spec, flen, out3):
     """Row filter of a float32 [nrow, nslice, ncol] CUDA view into out3."""
     nrow, nslice, ncol = x3.shape
     dev = x3.device
     nat.call("atb_filter_rows", x3.data_ptr(), x3.stride(0), x3.stride(1),
              nrow, nslice, ncol, int(pad), nat.PAD_MODES[pad_mode], 0,
-             spec.data_ptr(), 1, R._twiddle(log2m, dev).data_ptr(), log2m,
+             spec.data_ptr(), 1, R._twiddle(flen, dev).data_ptr(), flen,
              out3.data_ptr(), nat.F32, out3.stride(0), out3.stride(1),
              R._stream_ptr(dev))
 
@@ -520,11 +520,11 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
         to_int = _integer_input(projections)
     acc = torch.zeros((nline, height, width), dtype=torch.float64,
                       device=dev)
-    log2m = nat.call("atb_filter_log2m", int(width), int(pad))
+    flen = nat.call("atb_filter_length", int(width), int(pad))
     spec_before = None
     if ramp_filter == "before":
         spec_before, _ = R._spectrum(None, filter_name, height, width, pad,
-                                     log2m, dev)
+                                     flen, dev)
     spans = [(i * chunk_size + proj_start, (i + 1) * chunk_size + proj_start)
              for i in range(num_iter)]
     if num_rest != 0:
@@ -574,7 +574,7 @@ def _reconstruct(projections, x_mat, y_mat, center, geo, flat_field,
             if filt is None:
                 filt = torch.empty_like(pre)
                 work[("filt", n)] = filt
-            _filter_rows(pre, pad, pad_mode, spec_before, log2m, filt)
+            _filter_rows(pre, pad, pad_mode, spec_before, flen, filt)
             src = filt
         _backproject(src, trig[s0 - proj_start:s1 - proj_start], pts, c,
                      edge_pad, acc)

@@ -7,8 +7,9 @@ definitions (``algotom/rec/reconstruction.py:50-115, 496-524``;
 
 :func:`row_filter_spectrum` turns a Fourier-space ramp window of width
 ``N = ncol + 2 pad`` into what ``atb_filter_rows`` needs: the spectrum of
-the periodised real kernel laid out for a power-of-two FFT length
-``M >= N + ncol - 1``.  Derivation: algotom's filter is
+the periodised real kernel at the transform length ``atb_filter_length``
+chooses, ``N`` itself or an embedding length ``M >= N + ncol - 1``.
+Derivation: algotom's filter is
 ``crop(ifftshift(real(ifft(ifftshift(fftshift(fft(x)) W)))))``; the two
 spectrum shifts cancel, so with ``H = ifftshift(W)`` the output is the real
 circular convolution of the padded row with
@@ -61,39 +62,37 @@ def make_2d_ramp_window(height, width, filter_name=None):
     return np.tile(ramp_window_row(width, filter_name), (height, 1))
 
 
-def next_log2(n):
-    n = int(n)
-    return max(4, (n - 1).bit_length())
-
-
-def row_filter_spectrum(window_rows, ncol, pad, log2m):
+def row_filter_spectrum(window_rows, ncol, pad, m):
     """FP64 spectrum of the periodised kernel for each row of a ramp window.
 
     ``window_rows``: complex [R, N] Fourier-space window rows in fftshifted
-    order (R = 1 for a tiled window).  Returns complex64 [R, M] already
-    multiplied by 1/M (the kernel's inverse transform is an unnormalised
-    forward FFT of the conjugate).
+    order (R = 1 for a tiled window).  ``m``: the transform length, N itself
+    or at least N + ncol - 1 (``atb_filter_length``).  Returns complex64
+    [R, m] already multiplied by 1/m (the kernel's inverse transform is an
+    unnormalised forward FFT of the conjugate).
     """
     w = np.atleast_2d(np.asarray(window_rows, dtype=np.complex128))
     n = ncol + 2 * pad
     if w.shape[1] != n:
         raise ValueError("window width %d != ncol + 2*pad = %d"
                          % (w.shape[1], n))
-    m = 1 << log2m
-    if m < n + ncol - 1:
-        raise ValueError("FFT length 2^%d too short" % log2m)
+    if m != n and m < n + ncol - 1:
+        raise ValueError("transform length %d is neither N = %d nor at "
+                         "least N + ncol - 1 = %d" % (m, n, n + ncol - 1))
     h = np.fft.ifftshift(w, axes=1)
     kappa = np.roll(np.real(np.fft.ifft(h, axis=1)), -(n // 2), axis=1)
-    lags = np.arange(pad - n + 1, pad + ncol)
-    b = np.zeros((w.shape[0], m))
-    b[:, lags % m] = kappa[:, lags % n]
+    if m == n:
+        b = kappa
+    else:
+        lags = np.arange(pad - n + 1, pad + ncol)
+        b = np.zeros((w.shape[0], m))
+        b[:, lags % m] = kappa[:, lags % n]
     return (np.fft.fft(b, axis=1) / m).astype(np.complex64)
 
 
 @lru_cache(maxsize=16)
-def twiddles(log2m):
-    """exp(-2 pi i t / M), t in [0, M), complex64 from FP64."""
-    m = 1 << log2m
+def twiddles(m):
+    """exp(-2 pi i t / m), t in [0, m), complex64 from FP64."""
     t = np.arange(m, dtype=np.float64)
     return np.exp(-2j * np.pi * t / m).astype(np.complex64)
 

@@ -73,12 +73,15 @@ int atb_copy_2d(void *dst, int64_t dst_pitch, const void *src,
                 void *stream);
 
 /*
- * Smallest log2 of the FFT length the row filter uses for a detector width
- * `ncol` and pad `pad`: M = 2^log2m >= (ncol + 2 pad) + ncol - 1, so that the
- * circular convolution of length ncol + 2 pad is reproduced exactly on the
- * cropped window.  Returns a negative code if the row does not fit one CTA.
+ * Transform length n the row filter uses for a detector width `ncol` and
+ * pad `pad`, the cheaper (by a flop count of its FFT stages) of
+ * N = ncol + 2 pad itself, when N has no prime factor above 13 (the
+ * reference's own transform: 2860 = 4 5 11 13 at 2560 pixels, pad 150), and
+ * the 7-smooth lengths n >= N + ncol - 1 (a circular convolution of length
+ * n then reproduces the one of length N exactly on the cropped window).
+ * At most 16384; a negative code if no length fits.
  */
-int atb_filter_log2m(int ncol, int pad);
+int atb_filter_length(int ncol, int pad);
 
 /*
  * Padded ramp-and-window filter of every row of a sinogram stack, with the
@@ -88,18 +91,21 @@ int atb_filter_log2m(int ncol, int pad);
  *
  *   src      float32 [nrow][nslice][ncol] at src_row_stride / src_slice_stride
  *   pad      detector padding on each side; pad_mode one of ATB_PAD_*
- *   spec     complex64 [spec_rows][2^log2m]: spectrum of the periodised real
- *            kernel, already scaled by 2^-log2m.  spec_rows = 1 (one kernel
- *            for every row) or nrow (one kernel per angle; then two slices of
- *            one angle share a transform)
- *   twiddle  complex64 [2^log2m]: exp(-2 pi i t / 2^log2m)
+ *   spec     complex64 [spec_rows][fft_len]: spectrum of the periodised
+ *            real kernel, already scaled by 1 / fft_len.  spec_rows = 1 (one
+ *            kernel for every row) or nrow (one kernel per angle; then two
+ *            slices of one angle share a transform)
+ *   twiddle  complex64 [fft_len]: exp(-2 pi i t / fft_len)
+ *   fft_len  a length with fft_len == ncol + 2 pad (no prime factor above
+ *            13) or fft_len >= 2 ncol + 2 pad - 1 (7-smooth), at most 16384;
+ *            atb_filter_length gives the cheapest
  *   dst      [nrow][nslice][ncol] of dst_dtype (ATB_F32/F16/BF16) at
  *            dst_row_stride / dst_slice_stride
  */
 int atb_filter_rows(const float *src, int64_t src_row_stride,
                     int64_t src_slice_stride, int nrow, int nslice, int ncol,
                     int pad, int pad_mode, int apply_log, const void *spec,
-                    int spec_rows, const void *twiddle, int log2m, void *dst,
+                    int spec_rows, const void *twiddle, int fft_len, void *dst,
                     int dst_dtype, int64_t dst_row_stride,
                     int64_t dst_slice_stride, void *stream);
 
@@ -122,19 +128,21 @@ typedef struct {
 
 /*
  * atb_filter_rows over a batch of single-slice sinograms of uneven width
- * and angle count that share the FFT length 2^log2m, in ONE launch: CTA p
+ * and angle count that share the transform length fft_len, in ONE launch: CTA p
  * filters row pair p - pair_offset of the item whose pair range holds p.
  * The uneven-batch counterpart of the reference's per-slice filtering
  * (reconstruction.py:460-475); no counterpart of the batching itself.
  *
  *   items     DEVICE array [nitems], ordered by pair_offset (0 first)
  *   npairs    total row pairs (sum of (nrow + 1) / 2)
- *   pad_mode, apply_log, twiddle, log2m, dst_dtype as atb_filter_rows;
- *             every item needs 2^log2m >= ncol + 2 pad + ncol - 1
+ *   pad_mode, apply_log, twiddle, fft_len, dst_dtype as atb_filter_rows;
+ *             every item needs fft_len == ncol + 2 pad or fft_len >=
+ *             2 ncol + 2 pad - 1, its spectrum built for fft_len (items
+ *             longer than fft_len are skipped)
  */
 int atb_filter_rows_batch(const atb_filter_item *items, int nitems,
                           int npairs, int pad_mode, int apply_log,
-                          const void *twiddle, int log2m, int dst_dtype,
+                          const void *twiddle, int fft_len, int dst_dtype,
                           void *stream);
 
 /*

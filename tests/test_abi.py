@@ -31,13 +31,22 @@ def test_version_and_no_error():
     assert isinstance(nat.last_error(), str)
 
 
-def test_filter_log2m():
-    assert nat.call("atb_filter_log2m", 1024, 150) == 12   # 2347 -> 4096
-    assert nat.call("atb_filter_log2m", 2560, 150) == 13   # 5419 -> 8192
-    assert nat.call("atb_filter_log2m", 96, 14) == 8
-    rc = nat.load().atb_filter_log2m(20000, 150)
-    assert rc == -3 and "2^" in nat.last_error()
-    assert nat.load().atb_filter_log2m(0, 1) == -1
+def test_filter_length():
+    # N itself when it is 13-smooth and cheapest: 2860 = 4 5 11 13
+    assert nat.call("atb_filter_length", 2560, 150) == 2860
+    # 1324 = 4 x 331 is not: the cheapest 7-smooth n >= N + ncol - 1 = 2347
+    n = nat.call("atb_filter_length", 1024, 150)
+    assert n >= 2347 and n <= 4096
+    r = n
+    for q in (2, 3, 5, 7):
+        while r % q == 0:
+            r //= q
+    assert r == 1
+    assert nat.call("atb_filter_length", 96, 14) in (124, 216, 224, 225,
+                                                     240, 243, 250, 252, 256)
+    rc = nat.load().atb_filter_length(20000, 150)
+    assert rc == -3 and "16384" in nat.last_error()
+    assert nat.load().atb_filter_length(0, 1) == -1
 
 
 def test_bad_arguments_are_rejected():
@@ -64,17 +73,22 @@ def test_bad_arguments_are_rejected():
     rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 42, 0, p, 1, p, 5, p, 0, 0,
                              0, None)
     assert rc == -1 and "pad_mode" in nat.last_error()
-    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 1, p, 4, p, 0, 0,
-                             0, None)
-    assert rc == -1 and "2^4" in nat.last_error()
-    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 3, p, 5, p, 0, 0,
+    # N = 12: 12 itself or a length >= 19 (4 and 13 are neither)
+    for n in (4, 13, 18):
+        rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 1, p, n, p, 0,
+                                 0, 0, None)
+        assert rc == -1 and "fft_len=%d" % n in nat.last_error()
+    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 1, p, 17, p, 0, 0,
+                             0, None)  # 17 has no radix plan
+    assert rc == -1 and "fft_len=17" in nat.last_error()
+    rc = lib.atb_filter_rows(p, 0, 0, 4, 1, 8, 2, 0, 0, p, 3, p, 12, p, 0, 0,
                              0, None)
     assert rc == -1 and "spec_rows" in nat.last_error()
 
 
 def test_call_raises_with_message():
-    with pytest.raises(nat.NativeLibraryError, match="atb_filter_log2m"):
-        nat.call("atb_filter_log2m", -5, 0)
+    with pytest.raises(nat.NativeLibraryError, match="atb_filter_length"):
+        nat.call("atb_filter_length", -5, 0)
 
 
 def test_batch_plan_orders_by_cost():

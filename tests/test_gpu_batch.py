@@ -35,7 +35,10 @@ def test_batch_matches_single_slice_and_oracle(cuda, monkeypatch):
     assert bf.counter.cpu().tolist() == [0, 0]
     for s, a, (nrow, ncol), c, o in zip(sinos, angs, shapes, cens, outs):
         single = R.fbp_reconstruction(s, c, angles=a, apply_log=False)
-        assert np.array_equal(o, single)  # same tile kernel, same order
+        # same back-projection tiles; the batch filters items of similar
+        # width at one shared transform length, the single-slice call at
+        # its own (both exact), so the two differ by float32 rounding
+        assert O.rel_l2(o, single) < 1e-6
         ref = O.fbp_reconstruction(s, c, angles=a, apply_log=False)
         assert O.rel_l2(o, ref) < 1e-5
 

@@ -91,7 +91,8 @@ def test_filter_with_log(cuda):
 
 def test_filter_limits(cuda):
     x = np.zeros((2, 9000), np.float32)
-    with pytest.raises(nat.NativeLibraryError, match="2\\^"):
+    # N = 9300 = 2^2 3 5^2 31 and N + ncol - 1 > 16384: no exact length
+    with pytest.raises(nat.NativeLibraryError, match="16384"):
         R.apply_ramp_filter(x, None, "hann", 150)
     got = R.apply_ramp_filter(np.ones((2, 8000), np.float32), None, "hann",
                               150)

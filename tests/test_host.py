@@ -8,6 +8,7 @@ packing the kernel uses), against the oracle's filter.
 import numpy as np
 import pytest
 
+from algotom_b200 import _native as nat
 from algotom_b200 import phantom
 from algotom_b200.rec import windows as W
 from oracle import fbp_oracle as O
@@ -34,12 +35,13 @@ def test_product_windows_match_reference(golden):
                                       g["mask__%d__%s" % (w, ratio)])
 
 
-def _device_filter_model(x2, pad, mode, window_row):
-    """NumPy model of atb_filter_rows for two rows."""
+def _device_filter_model(x2, pad, mode, window_row, m=None):
+    """NumPy model of atb_filter_rows for two rows (transform length m:
+    atb_filter_length's choice by default)."""
     ncol = x2.shape[1]
-    log2m = W.next_log2(2 * ncol + 2 * pad - 1)
-    m = 1 << log2m
-    spec = W.row_filter_spectrum(window_row, ncol, pad, log2m)[0]
+    if m is None:
+        m = nat.call("atb_filter_length", ncol, pad)
+    spec = W.row_filter_spectrum(window_row, ncol, pad, m)[0]
     xp = np.pad(x2, ((0, 0), (pad, pad)), mode=mode)
     z = np.zeros(m, complex)
     z[:ncol + 2 * pad] = xp[0] + 1j * xp[1]
@@ -50,23 +52,30 @@ def _device_filter_model(x2, pad, mode, window_row):
 @pytest.mark.parametrize("ncol,pad", [(96, 14), (81, 12), (50, 0), (33, 80)])
 @pytest.mark.parametrize("name", ["hann", None, "parzen"])
 def test_spectrum_embedding_reproduces_filter(ncol, pad, name):
+    """Every exact length: N itself, the smallest embedding and a longer
+    one, against the oracle's length-N filter."""
     rng = np.random.default_rng(ncol + pad)
     x = rng.standard_normal((2, ncol))
-    got = _device_filter_model(x, pad, "edge",
-                               W.ramp_window_row(ncol + 2 * pad, name))
+    n = ncol + 2 * pad
     ref = O.apply_ramp_filter(x, None, name, pad, "edge")
-    assert O.rel_l2(got, ref) < 1e-6   # complex64 spectrum
+    for m in (None, n, n + ncol - 1, 2 * (n + ncol)):
+        got = _device_filter_model(x, pad, "edge",
+                                   W.ramp_window_row(n, name), m)
+        assert O.rel_l2(got, ref) < 1e-6   # complex64 spectrum
 
 
 def test_spectrum_rejects_short_fft():
     with pytest.raises(ValueError):
-        W.row_filter_spectrum(W.ramp_window_row(100, "hann"), 80, 10, 7)
+        W.row_filter_spectrum(W.ramp_window_row(100, "hann"), 80, 10, 128)
+    with pytest.raises(ValueError):
+        W.row_filter_spectrum(W.ramp_window_row(100, "hann"), 80, 10, 101)
 
 
 def test_twiddles():
-    t = W.twiddles(6)
-    np.testing.assert_allclose(t, np.exp(-2j * np.pi * np.arange(64) / 64),
-                               atol=1e-7)
+    for m in (64, 60, 2860):
+        t = W.twiddles(m)
+        np.testing.assert_allclose(
+            t, np.exp(-2j * np.pi * np.arange(m) / m), atol=1e-7)
 
 
 def test_phantom_sinogram_is_exact_line_integral():
