@@ -21,9 +21,11 @@
 //   of the transform of a + i b), with the padding (NumPy's ten modes), the
 //   -log (values <= 0 give 0 and are counted, the reference's warning), the
 //   ifftshift, the fftshift and the window in the same pass;
-// - dfi_inv_rows_kernel: one row of the Cartesian spectrum, regridded on
-//   the fly from the B-spline coefficients of the polar spectrum
-//   (dfi_grid.cuh) in ifftshift order, inverse-transformed; only the ncol
+// - dfi_inv_rows_kernel: rows k and -k of the Cartesian spectrum,
+//   regridded on the fly from the B-spline coefficients of the polar
+//   spectrum (dfi_grid.cuh) in ifftshift order; one inverse transform of
+//   the Hermitian part's row k gives both rows' transforms (the output is
+//   the real part, which only the Hermitian part feeds); only the ncol
 //   columns the final crop keeps are stored;
 // - dfi_inv_cols_kernel: two of those columns per transform (the real
 //   parts of the inverses of z1 and z2 are the real and imaginary parts of
@@ -300,24 +302,41 @@ struct InvArgs {
   int out_f32;
 };
 
-// pass 1: row oi of the (ifftshift-ordered) Cartesian spectrum of slice
-// blockIdx.y, regridded into shared memory and inverse-transformed
+// pass 1: rows oi and w - oi (oi <= w / 2) of the (ifftshift-ordered)
+// Cartesian spectrum G of slice blockIdx.y, regridded into shared memory.
+// The output is Re(IDFT2(G)) = IDFT2(U) with U = (G + conj G(-k)) / 2, and
+// U is Hermitian, so the inverse row transform of U's row -oi is the
+// conjugate of that of its row oi: one transform per pair of rows.
 __global__ void __launch_bounds__(kThreads) dfi_inv_rows_kernel(const __grid_constant__ InvArgs a,
                                                                 const __grid_constant__ IpPlan pl, Tables t) {
   extern __shared__ double2 sm[];
   const int M = pl.n, w = a.w, oi = blockIdx.x, k = blockIdx.y;
+  const int oi2 = oi == 0 ? 0 : w - oi;
   double2 *tws = sm + M;
   atb::fft::load_twiddles_n(t.tw, M, tws);
-  const int i = oi + w / 2 >= w ? oi + w / 2 - w : oi + w / 2;  // grid row at oi
+  auto grid_row = [&](int o) { return o + w / 2 >= w ? o + w / 2 - w : o + w / 2; };
+  const int i = grid_row(oi), i2 = grid_row(oi2);
   const double2 *coef = a.coef + k * a.css;
+  // rows oi and -oi (2 w <= M: the second one in sm[w .. 2 w))
+  for (int t2 = threadIdx.x; t2 < 2 * w; t2 += blockDim.x) {
+    const int second = t2 >= w, oj = t2 - second * w;
+    sm[t2] = atb::dfi::regrid_point(coef, a.crs, a.nrow, w, second ? i2 : i, grid_row(oj));
+  }
+  __syncthreads();
+  // U[oi][oj] = (G[oi][oj] + conj G[-oi][-oj]) / 2, in place (thread per oj)
   for (int oj = threadIdx.x; oj < w; oj += blockDim.x) {
-    const int j = oj + w / 2 >= w ? oj + w / 2 - w : oj + w / 2;
-    sm[oj] = atb::dfi::regrid_point(coef, a.crs, a.nrow, w, i, j);
+    const double2 g = sm[oj], h = sm[w + (oj == 0 ? 0 : w - oj)];
+    sm[oj] = make_double2(0.5 * (g.x + h.x), 0.5 * (g.y - h.y));
   }
   __syncthreads();
   bluestein<true>(sm, w, pl, tws, t);
   double2 *out = a.z + ((long long)k * w + oi) * a.ncol;
-  for (int b = threadIdx.x; b < a.ncol; b += blockDim.x) out[b] = sm[crop_index(b, a.pad, w)];
+  double2 *out2 = a.z + ((long long)k * w + oi2) * a.ncol;
+  for (int b = threadIdx.x; b < a.ncol; b += blockDim.x) {
+    const double2 v = sm[crop_index(b, a.pad, w)];
+    out[b] = v;
+    if (oi2 != oi) out2[b] = make_double2(v.x, -v.y);
+  }
 }
 
 // pass 2: columns 2 blockIdx.x and 2 blockIdx.x + 1 of slice blockIdx.y
@@ -474,7 +493,7 @@ extern "C" int atb_dfi_inverse(const void *coef, int64_t coef_row_stride, int64_
   a.out = out; a.ors = out_row_stride; a.oss = out_slice_stride; a.out_f32 = out_f32 ? 1 : 0;
   const Tables t = tables(chirp, twiddle, bfwd, binv);
   cudaStream_t st = atb::as_stream(stream);
-  dfi_inv_rows_kernel<<<dim3(w, nslice), kThreads, smem_bytes(M), st>>>(a, pl, t);
+  dfi_inv_rows_kernel<<<dim3(w / 2 + 1, nslice), kThreads, smem_bytes(M), st>>>(a, pl, t);
   const int r = atb::check_launch("atb_dfi_inverse (rows)");
   if (r != ATB_OK) return r;
   dfi_inv_cols_kernel<<<dim3((ncol + 1) / 2, nslice), kThreads, smem_bytes(M), st>>>(a, pl, t);

@@ -18,13 +18,16 @@
 // barrier so one shared-memory buffer suffices; twiddles come from two
 // short tables in shared memory.
 //
-// One CTA filters two rows at once: real rows x1, x2 travel as the complex
+// A CTA filters two rows at once: real rows x1, x2 travel as the complex
 // row x1 + i x2 through one forward FFT, a product with the (real-kernel)
 // spectrum and one inverse FFT (done as conj(FFT(conj(.))) with 1/n folded
 // into the spectrum); the real and imaginary parts of the result are the
 // two filtered rows.  Each row is read from HBM once (with the -log folded
 // in) and written once; padding, both transforms and the spectral product
-// stay in shared memory.
+// stay in shared memory.  The kernel is persistent: each CTA loops over row
+// pairs, the next pair's rows travel into shared memory (cp.async) while
+// the current pair is transformed, and a spectrum shared by all rows is
+// read once per CTA.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -37,9 +40,11 @@ constexpr int kMaxLen = 16384;  // 16384 complex (+1/16 padding) = 136 KiB of sh
 constexpr int kMaxStages = 14;
 constexpr int kTwLo = 64;       // two-level twiddle tables: w^t = ta[t / 64] tb[t % 64]
 
-// Shared-memory index of complex element i: one padding word per 16
-// elements keeps the strided Stockham writes free of bank conflicts.
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+// Shared-memory index of complex element i.  (A padding word every 16 or
+// 32 elements trims the bank conflicts of the first stages' strided
+// writes, but its index arithmetic cost more than the conflicts: 0.84 and
+// 0.83 against 0.78 ms per 16-slice launch at 2560 pixels.)
+__device__ __forceinline__ int pidx(int i) { return i; }
 
 // What every CTA of a launch shares: the transform plan and the pad / log
 // settings (read from parameter space; the plan arrays are indexed at run
@@ -49,7 +54,18 @@ struct FilterPlan {
   const float2 *tw;    // [n] exp(-2 pi i t / n)
   int n, nstages;      // transform length and its radices, in stage order
   int radix[kMaxStages];
+  unsigned magic[kMaxStages];  // ceil(2^32 / Ns) for Ns > 1: j / Ns = umulhi(j, magic) for j, Ns < 2^14
   float2 rc[5][6];     // (cos, sin)(2 pi q / p), q = 1 .. (p-1)/2, p = 3, 5, 7, 11, 13
+};
+
+// The plan's stage data as each CTA keeps it in shared memory: the stages
+// read it there after barriers, so the compiler does not hoist it into
+// registers across the pair loop.
+struct StagePlan {
+  int n, nstages;
+  int radix[kMaxStages];
+  unsigned magic[kMaxStages];
+  float2 rc[5][6];
 };
 
 // The rows one launch (or one batch item) filters.
@@ -168,8 +184,9 @@ template <int R> __device__ __forceinline__ void dft(float2 *v, const float2 *rc
 
 __host__ __device__ constexpr int odd_slot(int p) { return p == 3 ? 0 : p == 5 ? 1 : p == 7 ? 2 : p == 11 ? 3 : 4; }
 
-// butterflies a thread holds per stage of radix R (at most ~32 values)
-__host__ __device__ constexpr int max_butterflies(int r) { return r >= 11 ? 2 : (r >= 5 ? 4 : 32 / r); }
+// butterflies a thread holds per stage of radix r, for a budget of about e
+// complex values per thread
+__host__ __device__ constexpr int butterflies(int r, int e) { return (e + r - 1) / r; }
 
 // Stockham stage of radix R after sub-transforms of length Ns: butterfly
 // j (< Q = n / R) reads x[j + r Q], twiddles input r by w^(r k)
@@ -179,12 +196,17 @@ __host__ __device__ constexpr int max_butterflies(int r) { return r >= 11 ? 2 : 
 // Twiddles exp(-2 pi i t / n) = ta[t / 64] * tb[t % 64] come from two short
 // tables in shared memory; w^r is the product of the table values of the
 // powers 1, 2, 4, 8 in r (at most three roundings, against 2 (R - 1) table
-// reads per butterfly).
-template <int R, int T>
-__device__ __forceinline__ void fft_stage(float2 *x, const FilterPlan &a, int Ns, const float2 *ta,
-                                          const float2 *tb) {
-  constexpr int kB = max_butterflies(R);
+// reads per butterfly).  The launch's thread count is a run-time value
+// (blockDim.x); a thread holds up to kB butterflies of the stage.  Values
+// of butterflies a thread skips are zeroed, not left undefined: undefined
+// values on predicated paths made the compiler keep them alive across the
+// pair loop and spill.
+template <int R, int E>
+__device__ __forceinline__ void fft_stage(float2 *x, const StagePlan &a, int Ns, unsigned magic,
+                                          const float2 *ta, const float2 *tb) {
+  constexpr int kB = butterflies(R, E);
   const int n = a.n, Q = n / R, tstep = n / (Ns * R);
+  const int nt = blockDim.x, nb = (Q + nt - 1) / nt;  // butterflies per thread (<= kB; CTA-uniform)
   float2 rc[6];
   if constexpr (R % 2 == 1) {
 #pragma unroll
@@ -193,18 +215,16 @@ __device__ __forceinline__ void fft_stage(float2 *x, const FilterPlan &a, int Ns
   float2 v[kB][R];
 #pragma unroll
   for (int b = 0; b < kB; ++b) {
-    const int j = threadIdx.x + b * T;
-    if (j < Q) {
+    const int j = threadIdx.x + b * nt;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = x[pidx(j + r * Q)];
-    }
+    for (int r = 0; r < R; ++r) v[b][r] = b < nb && j < Q ? x[pidx(j + r * Q)] : make_float2(0.f, 0.f);
   }
   __syncthreads();
 #pragma unroll
   for (int b = 0; b < kB; ++b) {
-    const int j = threadIdx.x + b * T;
-    if (j < Q) {
-      const int k = j % Ns;
+    const int j = threadIdx.x + b * nt;
+    if (b < nb && j < Q) {
+      const int k = Ns == 1 ? 0 : j - (int)__umulhi((unsigned)j, magic) * Ns;  // j mod Ns
       if (k) {
         const int e = k * tstep;  // w^r = exp(-2 pi i r e / n)
         auto tw = [&](int c) {
@@ -236,22 +256,20 @@ __device__ __forceinline__ void fft_stage(float2 *x, const FilterPlan &a, int Ns
 // In-place forward FFT of length a.n through the plan's stages, which come
 // in a fixed order (16s, one 8 / 4 / 2, then 13s, 11s, 7s, 5s, 3s): one
 // inlined copy of each stage kind in sequence (a switch inside a loop over
-// the stages makes the compiler spill).  Force-inlined: called twice per
-// kernel, the compiler otherwise emits it as a real call whose ABI costs a
-// large stack frame and much of the speed.
-template <int T>
-__device__ __forceinline__ void fft_forward(float2 *x, const FilterPlan &a, const float2 *ta, const float2 *tb) {
+// the stages makes the compiler spill).
+template <int E>
+__device__ __forceinline__ void fft_forward(float2 *x, const StagePlan &a, const float2 *ta, const float2 *tb) {
   int s = 0, Ns = 1;
   const int ns = a.nstages;
-  for (; s < ns && a.radix[s] == 16; ++s, Ns *= 16) fft_stage<16, T>(x, a, Ns, ta, tb);
-  if (s < ns && a.radix[s] == 8) { fft_stage<8, T>(x, a, Ns, ta, tb); ++s; Ns *= 8; }
-  if (s < ns && a.radix[s] == 4) { fft_stage<4, T>(x, a, Ns, ta, tb); ++s; Ns *= 4; }
-  if (s < ns && a.radix[s] == 2) { fft_stage<2, T>(x, a, Ns, ta, tb); ++s; Ns *= 2; }
-  for (; s < ns && a.radix[s] == 13; ++s, Ns *= 13) fft_stage<13, T>(x, a, Ns, ta, tb);
-  for (; s < ns && a.radix[s] == 11; ++s, Ns *= 11) fft_stage<11, T>(x, a, Ns, ta, tb);
-  for (; s < ns && a.radix[s] == 7; ++s, Ns *= 7) fft_stage<7, T>(x, a, Ns, ta, tb);
-  for (; s < ns && a.radix[s] == 5; ++s, Ns *= 5) fft_stage<5, T>(x, a, Ns, ta, tb);
-  for (; s < ns && a.radix[s] == 3; ++s, Ns *= 3) fft_stage<3, T>(x, a, Ns, ta, tb);
+  for (; s < ns && a.radix[s] == 16; ++s, Ns *= 16) fft_stage<16, E>(x, a, Ns, a.magic[s], ta, tb);
+  if (s < ns && a.radix[s] == 8) { fft_stage<8, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 8; }
+  if (s < ns && a.radix[s] == 4) { fft_stage<4, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 4; }
+  if (s < ns && a.radix[s] == 2) { fft_stage<2, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 2; }
+  for (; s < ns && a.radix[s] == 13; ++s, Ns *= 13) fft_stage<13, E>(x, a, Ns, a.magic[s], ta, tb);
+  for (; s < ns && a.radix[s] == 11; ++s, Ns *= 11) fft_stage<11, E>(x, a, Ns, a.magic[s], ta, tb);
+  for (; s < ns && a.radix[s] == 7; ++s, Ns *= 7) fft_stage<7, E>(x, a, Ns, a.magic[s], ta, tb);
+  for (; s < ns && a.radix[s] == 5; ++s, Ns *= 5) fft_stage<5, E>(x, a, Ns, a.magic[s], ta, tb);
+  for (; s < ns && a.radix[s] == 3; ++s, Ns *= 3) fft_stage<3, E>(x, a, Ns, a.magic[s], ta, tb);
 }
 
 // Block-wide reduction over T threads (op: 0 sum, 1 max, 2 min).
@@ -269,7 +287,7 @@ __device__ float2 block_reduce2(float2 v, int op, float2 *scratch) {
   if (lane == 0) scratch[warp] = v;
   __syncthreads();
   if (warp == 0) {
-    v = lane < T / 32 ? scratch[lane]
+    v = lane < (int)(blockDim.x >> 5) ? scratch[lane]
                       : (op == 0 ? make_float2(0.f, 0.f)
                                  : (op == 1 ? make_float2(-FLT_MAX, -FLT_MAX) : make_float2(FLT_MAX, FLT_MAX)));
 #pragma unroll
@@ -304,7 +322,7 @@ __device__ float2 block_select2(const float2 *x, int pad, int ncol, int rank, fl
   for (int it = 0; it < 32; ++it) {
     const unsigned m1 = lo1 + ((hi1 - lo1) >> 1), m2 = lo2 + ((hi2 - lo2) >> 1);
     float c1 = 0.f, c2 = 0.f;
-    for (int j = threadIdx.x; j < ncol; j += T) {
+    for (int j = threadIdx.x; j < ncol; j += (int)blockDim.x) {
       const float2 v = x[pidx(pad + j)];
       c1 += fkey(v.x) <= m1 ? 1.f : 0.f;
       c2 += fkey(v.y) <= m2 ? 1.f : 0.f;
@@ -316,62 +334,69 @@ __device__ float2 block_select2(const float2 *x, int pad, int ncol, int rank, fl
   return make_float2(fkey_inv(lo1), fkey_inv(lo2));
 }
 
-// Filters row pair `pair` of the rows a with the plan p (CTA-uniform).
-template <typename OutT, int T>
-__device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const FilterRows &a, int pair) {
-  extern __shared__ float2 sm[];  // n complex, padded by pidx
-  __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
-  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
-  const int M = p.n;
-  const int ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad;
-  const int tid = threadIdx.x;
-  if (N > M) return;  // not a length for these rows (CTA-uniform)
-
-  // twiddle tables: ta[u] = w^(64 u), tb[v] = w^v, w = exp(-2 pi i / n)
-  for (int u = tid; u < (M + kTwLo - 1) / kTwLo; u += T) ta[u] = __ldg(p.tw + u * kTwLo);
-  for (int v = tid; v < kTwLo; v += T) tb[v] = v < M ? __ldg(p.tw + v) : make_float2(1.f, 0.f);
-
-  // the two rows (angle, slice) of this CTA
+// The two rows (angle, slice) of row pair `pair`.
+struct PairIdx {
   int i1, k1, i2, k2;
   bool ok2;
+};
+
+__device__ __forceinline__ PairIdx pair_rows(const FilterRows &a, int pair) {
+  PairIdx r;
   if (a.pair_within_angle) {
-    i1 = pair / a.pairs_per_angle;
-    k1 = 2 * (pair % a.pairs_per_angle);
-    i2 = i1;
-    k2 = k1 + 1;
-    ok2 = k2 < a.nslice;
+    r.i1 = pair / a.pairs_per_angle;
+    r.k1 = 2 * (pair % a.pairs_per_angle);
+    r.i2 = r.i1;
+    r.k2 = r.k1 + 1;
+    r.ok2 = r.k2 < a.nslice;
   } else {
     // rows 2 pair and 2 pair + 1 in [angle][slice] order; the host caps
     // the pairs at 2^31, so the row index fits 32-bit unsigned arithmetic
     // (a 64-bit division here made the kernel spill to the stack)
     const unsigned r1 = 2u * (unsigned)pair, r2 = r1 + 1u, ns = (unsigned)a.nslice;
-    i1 = (int)(r1 / ns);
-    k1 = (int)(r1 % ns);
-    i2 = (int)(r2 / ns);
-    k2 = (int)(r2 % ns);
-    ok2 = (unsigned long long)r2 < (unsigned long long)a.nrow * (unsigned long long)a.nslice;
+    r.i1 = (int)(r1 / ns);
+    r.k1 = (int)(r1 % ns);
+    r.i2 = (int)(r2 / ns);
+    r.k2 = (int)(r2 % ns);
+    r.ok2 = (unsigned long long)r2 < (unsigned long long)a.nrow * (unsigned long long)a.nslice;
   }
-  const float *s1 = a.src + i1 * a.srs + k1 * a.sss;
-  const float *s2 = a.src + (ok2 ? i2 * a.srs + k2 * a.sss : 0);
+  return r;
+}
 
-  // 1. the two logged rows into the middle of the complex buffer
-  for (int j = tid; j < ncol; j += T) {
-    float v1 = __ldg(s1 + j);
-    float v2 = ok2 ? __ldg(s2 + j) : 0.0f;
-    if (p.apply_log) { v1 = atb::neg_log(v1); v2 = ok2 ? atb::neg_log(v2) : 0.0f; }
-    sm[pidx(pad + j)] = make_float2(v1, v2);
+// Twiddle tables ta[u] = w^(64 u), tb[v] = w^v (w = exp(-2 pi i / n)) and
+// the stage plan into shared memory, visible after the next barrier.
+__device__ __forceinline__ void load_tables(const FilterPlan &p, float2 *ta, float2 *tb, StagePlan &sp) {
+  const int M = p.n, nt = blockDim.x;
+  for (int u = threadIdx.x; u < (M + kTwLo - 1) / kTwLo; u += nt) ta[u] = __ldg(p.tw + u * kTwLo);
+  for (int v = threadIdx.x; v < kTwLo; v += nt) tb[v] = v < M ? __ldg(p.tw + v) : make_float2(1.f, 0.f);
+  for (int i = threadIdx.x; i < kMaxStages; i += nt) {
+    sp.radix[i] = p.radix[i];
+    sp.magic[i] = p.magic[i];
   }
-  for (int m = N + tid; m < M; m += T) sm[pidx(m)] = make_float2(0.f, 0.f);
-  __syncthreads();
+  for (int i = threadIdx.x; i < 30; i += nt) sp.rc[i / 6][i % 6] = p.rc[i / 6][i % 6];
+  if (threadIdx.x == 0) {
+    sp.n = p.n;
+    sp.nstages = p.nstages;
+  }
+}
 
-  // 2. padding (numpy.pad semantics along the row)
+// Padding, transforms and store for one row pair whose (logged) rows sit
+// in sm[pad .. pad + ncol) with zeros in [N, n): the padding, the forward
+// transform, the product with spec (global or shared memory), the
+// conjugated inverse, crop and store.  Starts after a barrier; its last
+// reads of sm are not followed by one.
+template <typename OutT, int T, int E>
+__device__ __forceinline__ void pad_transform_store(const FilterPlan &p, const StagePlan &sp, const FilterRows &a,
+                                                    float2 *sm, const float2 *spec, const float2 *ta,
+                                                    const float2 *tb, float2 *scratch, const PairIdx &r) {
+  const int M = p.n, ncol = a.ncol, pad = a.pad, tid = threadIdx.x;
+  // padding (numpy.pad semantics along the row)
   if (pad > 0) {
     float2 stat = make_float2(0.f, 0.f);
     if (p.mode == ATB_PAD_MEAN || p.mode == ATB_PAD_MAXIMUM || p.mode == ATB_PAD_MINIMUM) {
       const int op = p.mode == ATB_PAD_MEAN ? 0 : (p.mode == ATB_PAD_MAXIMUM ? 1 : 2);
       float2 acc = op == 0 ? make_float2(0.f, 0.f)
                            : (op == 1 ? make_float2(-FLT_MAX, -FLT_MAX) : make_float2(FLT_MAX, FLT_MAX));
-      for (int j = tid; j < ncol; j += T) {
+      for (int j = tid; j < ncol; j += (int)blockDim.x) {
         const float2 v = sm[pidx(pad + j)];
         if (op == 0) { acc.x += v.x; acc.y += v.y; }
         else if (op == 1) { acc.x = fmaxf(acc.x, v.x); acc.y = fmaxf(acc.y, v.y); }
@@ -388,7 +413,7 @@ __device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const Filt
         stat = make_float2(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y));
       }
     }
-    for (int t = tid; t < 2 * pad; t += T) {
+    for (int t = tid; t < 2 * pad; t += (int)blockDim.x) {
       const bool left = t < pad;
       const int m = left ? t : ncol + t;   // position in the padded row
       const int q = m - pad;               // position relative to the row
@@ -428,38 +453,168 @@ __device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const Filt
   }
   __syncthreads();
 
-  // 3. forward transform, spectral product (conjugated), second forward
-  //    transform = conjugated inverse
-  fft_forward<T>(sm, p, ta, tb);
-  const float2 *spec = a.spec + (a.spec_rows > 1 ? (long long)i1 * M : 0LL);
-  for (int k = tid; k < M; k += T) {
-    const float2 y = cmul(sm[pidx(k)], __ldg(spec + k));
-    sm[pidx(k)] = make_float2(y.x, -y.y);
+  // forward transform, spectral product (conjugated), second forward
+  // transform = conjugated inverse, from one call site (two inlined copies
+  // would double the code the SMs fetch)
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    fft_forward<E>(sm, sp, ta, tb);
+    if (pass == 1) break;
+    for (int k = tid; k < M; k += (int)blockDim.x) {
+      const float2 y = cmul(sm[pidx(k)], spec[k]);
+      sm[pidx(k)] = make_float2(y.x, -y.y);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  fft_forward<T>(sm, p, ta, tb);
 
-  // 4. crop: real part -> row 1, -imag part -> row 2
-  OutT *d1 = reinterpret_cast<OutT *>(a.dst) + i1 * a.drs + k1 * a.dss;
-  OutT *d2 = reinterpret_cast<OutT *>(a.dst) + (ok2 ? i2 * a.drs + k2 * a.dss : 0);
-  for (int j = tid; j < ncol; j += T) {
+  // crop: real part -> row 1, -imag part -> row 2
+  OutT *d1 = reinterpret_cast<OutT *>(a.dst) + r.i1 * a.drs + r.k1 * a.dss;
+  OutT *d2 = reinterpret_cast<OutT *>(a.dst) + (r.ok2 ? r.i2 * a.drs + r.k2 * a.dss : 0);
+  for (int j = tid; j < ncol; j += (int)blockDim.x) {
     const float2 w = sm[pidx(pad + j)];
     atb::store_from_float(d1 + j, w.x);
-    if (ok2) atb::store_from_float(d2 + j, -w.y);
+    if (r.ok2) atb::store_from_float(d2 + j, -w.y);
   }
 }
 
-template <typename OutT, int T>
-__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
-    filter_rows_kernel(const __grid_constant__ FilterPlan p, const __grid_constant__ FilterRows a) {
-  filter_rows_body<OutT, T>(p, a, (int)blockIdx.x);
+// Filters row pair `pair` of the rows a with the plan p (CTA-uniform),
+// reading the rows straight from global memory.
+template <typename OutT, int T, int E>
+__device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const FilterRows &a, int pair) {
+  extern __shared__ float2 sm[];  // n complex
+  __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
+  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
+  __shared__ StagePlan sp;
+  const int M = p.n;
+  const int ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (N > M) return;  // not a length for these rows (CTA-uniform)
+  load_tables(p, ta, tb, sp);
+  const PairIdx r = pair_rows(a, pair);
+  const float *s1 = a.src + r.i1 * a.srs + r.k1 * a.sss;
+  const float *s2 = a.src + (r.ok2 ? r.i2 * a.srs + r.k2 * a.sss : 0);
+  for (int j = tid; j < ncol; j += nt) {
+    float v1 = __ldg(s1 + j);
+    float v2 = r.ok2 ? __ldg(s2 + j) : 0.0f;
+    if (p.apply_log) { v1 = atb::neg_log(v1); v2 = r.ok2 ? atb::neg_log(v2) : 0.0f; }
+    sm[pidx(pad + j)] = make_float2(v1, v2);
+  }
+  for (int m = N + tid; m < M; m += nt) sm[pidx(m)] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float2 *spec = a.spec + (a.spec_rows > 1 ? (long long)r.i1 * M : 0LL);
+  pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, ta, tb, scratch, r);
+}
+
+// ---- asynchronous copies global -> shared (cp.async; completion is waited
+// for with cp.async.wait_all, a hardware wait)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// the rows of pair r into stage[0 .. ncol) and stage[ncol4 .. ncol4 + ncol)
+__device__ __forceinline__ void stage_rows(const FilterRows &a, const PairIdx &r, float *stage, int ncol4) {
+  const int ncol = a.ncol, nt = blockDim.x;
+  const float *s1 = a.src + r.i1 * a.srs + r.k1 * a.sss;
+  const float *s2 = a.src + (r.ok2 ? r.i2 * a.srs + r.k2 * a.sss : 0);
+  const bool vec = (ncol & 3) == 0 && ((reinterpret_cast<uintptr_t>(s1) | reinterpret_cast<uintptr_t>(s2)) & 15) == 0;
+  if (vec) {
+    const int q = ncol >> 2;
+    for (int t = threadIdx.x; t < 2 * q; t += nt) {
+      const int row = t >= q, c = (t - row * q) << 2;
+      if (row == 0) cp_async16(stage + c, s1 + c);
+      else if (r.ok2) cp_async16(stage + ncol4 + c, s2 + c);
+    }
+  } else {
+    for (int t = threadIdx.x; t < 2 * ncol; t += nt) {
+      const int row = t >= ncol, c = t - row * ncol;
+      if (row == 0) cp_async4(stage + c, s1 + c);
+      else if (r.ok2) cp_async4(stage + ncol4 + c, s2 + c);
+    }
+  }
+  cp_async_commit();
+}
+
+// CTAs per SM the register budget aims at (T: the most threads a launch of
+// the instantiation uses): 3 for the 16-value budget at up to 256
+// threads, 2 up to 384, else 1
+constexpr int min_blocks(int t, int e) { return t > 384 ? 1 : (t > 256 || e > 16 ? 2 : 3); }
+
+// Shared-memory layout of the persistent kernel (bytes): the transform
+// buffer, the staged rows of the next pair, the spectrum (one kernel for
+// every row only).
+__host__ __device__ constexpr size_t buf_bytes(int n) { return sizeof(float2) * (size_t)((n + 1) & ~1); }
+__host__ __device__ constexpr int ncol4_of(int ncol) { return (ncol + 3) & ~3; }
+__host__ __device__ constexpr size_t stage_bytes(int ncol) { return sizeof(float) * 2 * (size_t)ncol4_of(ncol); }
+
+// Persistent: CTA b filters pairs b, b + grid, ...  While a pair is
+// transformed, the next pair's rows are already on their way into shared
+// memory, so row loads do not stall the transforms; a shared spectrum is
+// read once per CTA.
+template <typename OutT, int T, int E>
+__global__ void __launch_bounds__(T, min_blocks(T, E))
+    filter_rows_kernel(const __grid_constant__ FilterPlan p, const __grid_constant__ FilterRows a, int npairs,
+                       int spec_in_smem) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
+  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
+  __shared__ StagePlan sp;
+  const int M = p.n, ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad, ncol4 = ncol4_of(ncol);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  float2 *sm = reinterpret_cast<float2 *>(smraw);
+  float *stage = reinterpret_cast<float *>(smraw + buf_bytes(M));
+  float2 *spec_s = reinterpret_cast<float2 *>(smraw + buf_bytes(M) + stage_bytes(ncol));
+  const bool shared_spec = spec_in_smem && a.spec_rows == 1;
+  load_tables(p, ta, tb, sp);
+  if (shared_spec)
+    for (int k = tid; k < M; k += nt) cp_async8(spec_s + k, a.spec + k);
+  int pair = blockIdx.x;
+  if (pair < npairs) stage_rows(a, pair_rows(a, pair), stage, ncol4);
+  for (; pair < npairs; pair += gridDim.x) {
+    const PairIdx r = pair_rows(a, pair);
+    cp_async_wait_all();
+    __syncthreads();  // the staged rows (and the spectrum) are visible; sm is free
+    for (int j = tid; j < ncol; j += nt) {
+      float v1 = stage[j];
+      float v2 = r.ok2 ? stage[ncol4 + j] : 0.0f;
+      if (p.apply_log) { v1 = atb::neg_log(v1); v2 = r.ok2 ? atb::neg_log(v2) : 0.0f; }
+      sm[pidx(pad + j)] = make_float2(v1, v2);
+    }
+    for (int m = N + tid; m < M; m += nt) sm[pidx(m)] = make_float2(0.f, 0.f);
+    __syncthreads();  // stage is consumed
+    const int next = pair + gridDim.x;
+    if (next < npairs) stage_rows(a, pair_rows(a, next), stage, ncol4);
+    const float2 *spec = shared_spec ? spec_s : a.spec + (a.spec_rows > 1 ? (long long)r.i1 * M : 0LL);
+    pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, ta, tb, scratch, r);
+  }
+}
+
+// One CTA per pair, rows read straight from global memory: rows too long
+// for the persistent kernel's staging buffer.
+template <typename OutT, int T, int E>
+__global__ void __launch_bounds__(T, min_blocks(T, E))
+    filter_rows_direct_kernel(const __grid_constant__ FilterPlan p, const __grid_constant__ FilterRows a) {
+  filter_rows_body<OutT, T, E>(p, a, (int)blockIdx.x);
 }
 
 // One launch over the row pairs of several single-slice sinograms that
 // share the transform length: CTA q finds the item whose pair range holds q
 // (binary search on pair_offset) and filters that pair.
-template <typename OutT, int T>
-__global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
+template <typename OutT, int T, int E>
+__global__ void __launch_bounds__(T, min_blocks(T, E))
     filter_batch_kernel(const __grid_constant__ FilterPlan p, const atb_filter_item *items, int nitems) {
   const int q = blockIdx.x;
   int lo = 0, hi = nitems - 1;
@@ -477,7 +632,7 @@ __global__ void __launch_bounds__(T, T <= 256 ? 2 : 1)
   b.dst = it.dst; b.drs = it.dst_row_stride; b.dss = 0;
   b.pair_within_angle = 0;
   b.pairs_per_angle = 0;
-  filter_rows_body<OutT, T>(p, b, pair);
+  filter_rows_body<OutT, T, E>(p, b, pair);
 }
 
 __global__ void neg_log_kernel(const float *__restrict__ src, long long srs, long long sss, int nrow,
@@ -545,18 +700,26 @@ double transform_cost(int n) {
   return c * n;
 }
 
-// threads per CTA: the fewest (a multiple of 32, at least 64) for which
-// every stage's butterflies fit the per-thread register budget
-int threads_for(int n, const int *radix, int ns) {
-  int need = 64;
-  for (int k = 0; k < ns; ++k) {
-    const int q = n / radix[k], b = max_butterflies(radix[k]);
-    const int t = (q + b - 1) / b;
-    if (t > need) need = t;
+// Launch shape of a plan: threads per CTA and per-thread value budget:
+// the fewest of 64, 128, 256 or 512 threads for which every stage's
+// butterflies fit a budget of 16 values, else 512 threads with a budget of
+// 32.  (In between counts that waste fewer butterfly slots cost more in
+// residency: 288 threads for 2860 points, two CTAs per SM, took 0.90 ms
+// per 16-slice launch against 0.78 ms for 256 threads, three per SM.)
+bool threads_for(int n, const int *radix, int ns, int &threads, int &budget) {
+  for (int e : {16, 32}) {
+    for (int t : {64, 128, 256, 512}) {
+      if (e == 32 && t != 512) continue;
+      bool ok = true;
+      for (int k = 0; k < ns && ok; ++k) ok = (n / radix[k] + t - 1) / t <= butterflies(radix[k], e);
+      if (ok) {
+        threads = t;
+        budget = e;
+        return true;
+      }
+    }
   }
-  for (int t : {64, 128, 256, 512})
-    if (t >= need) return t;
-  return -1;
+  return false;
 }
 
 int filter_length(int ncol, int pad) {
@@ -591,7 +754,7 @@ bool valid_length(int n, int ncol, int pad) {
 }
 
 // the plan of length n (false: no radix plan or thread count for it)
-bool make_plan(int n, int mode, int apply_log, const void *twiddle, FilterPlan &p, int &threads) {
+bool make_plan(int n, int mode, int apply_log, const void *twiddle, FilterPlan &p, int &threads, int &budget) {
   if (n < 2 || n > kMaxLen) return false;
   p.mode = mode;
   p.apply_log = apply_log ? 1 : 0;
@@ -604,49 +767,81 @@ bool make_plan(int n, int mode, int apply_log, const void *twiddle, FilterPlan &
       const double ang = 2.0 * M_PI * (double)(q + 1) / (double)op[k];
       p.rc[k][q] = q < (op[k] - 1) / 2 ? make_float2((float)std::cos(ang), (float)std::sin(ang)) : make_float2(0.f, 0.f);
     }
-  threads = threads_for(n, p.radix, p.nstages);
-  return threads > 0;
+  for (int k = 0, ns = 1; k < p.nstages; ns *= p.radix[k], ++k)
+    p.magic[k] = ns == 1 ? 0u : (unsigned)((0x100000000ULL + (unsigned long long)ns - 1) / (unsigned long long)ns);
+  return threads_for(n, p.radix, p.nstages, threads, budget);
 }
 
-size_t smem_bytes(int n) { return sizeof(float2) * (size_t)(n + (n >> 4) + 1); }
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return n;
+}
 
-template <typename OutT, int T>
-int launch_filter_t(const FilterPlan &p, const FilterRows &a, long long npairs, cudaStream_t st) {
-  const size_t smem = smem_bytes(p.n);
-  const int rc = atb::ensure_smem(filter_rows_kernel<OutT, T>, smem, "atb_filter_rows");
+int max_smem() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 227 * 1024;
+  return v;
+}
+
+template <typename OutT, int T, int E>
+int launch_filter_t(const FilterPlan &p, const FilterRows &a, int nt, long long npairs, cudaStream_t st) {
+  // shared memory besides the dynamic part: twiddle tables, plan, scratch
+  const size_t fixed = sizeof(float2) * (kMaxLen / kTwLo + kTwLo + 32) + sizeof(StagePlan);
+  const size_t limit = (size_t)max_smem() - fixed;
+  const size_t base = buf_bytes(p.n) + stage_bytes(a.ncol), spec = sizeof(float2) * p.n;
+  if (base > limit) {  // no room to stage rows: one CTA per pair
+    const size_t smem = buf_bytes(p.n);
+    const int rc = atb::ensure_smem(filter_rows_direct_kernel<OutT, T, E>, smem, "atb_filter_rows");
+    if (rc != ATB_OK) return rc;
+    filter_rows_direct_kernel<OutT, T, E><<<(unsigned)npairs, nt, smem, st>>>(p, a);
+    return atb::check_launch("atb_filter_rows");
+  }
+  const int spec_in_smem = a.spec_rows == 1 && base + spec <= limit;
+  const size_t smem = base + (spec_in_smem ? spec : 0);
+  const int rc = atb::ensure_smem(filter_rows_kernel<OutT, T, E>, smem, "atb_filter_rows");
   if (rc != ATB_OK) return rc;
-  filter_rows_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(p, a);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, filter_rows_kernel<OutT, T, E>, nt, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long grid = std::min<long long>(npairs, (long long)per_sm * sm_count());
+  filter_rows_kernel<OutT, T, E><<<(unsigned)grid, nt, smem, st>>>(p, a, (int)npairs, spec_in_smem);
   return atb::check_launch("atb_filter_rows");
 }
 
 template <typename OutT>
-int launch_filter(const FilterPlan &p, const FilterRows &a, int threads, long long npairs, cudaStream_t st) {
-  switch (threads) {
-    case 512: return launch_filter_t<OutT, 512>(p, a, npairs, st);
-    case 256: return launch_filter_t<OutT, 256>(p, a, npairs, st);
-    case 128: return launch_filter_t<OutT, 128>(p, a, npairs, st);
-    default: return launch_filter_t<OutT, 64>(p, a, npairs, st);
-  }
+int launch_filter(const FilterPlan &p, const FilterRows &a, int threads, int budget, long long npairs,
+                  cudaStream_t st) {
+  if (budget > 16) return launch_filter_t<OutT, 512, 32>(p, a, threads, npairs, st);
+  if (threads <= 128) return launch_filter_t<OutT, 128, 16>(p, a, threads, npairs, st);
+  if (threads <= 256) return launch_filter_t<OutT, 256, 16>(p, a, threads, npairs, st);
+  if (threads <= 384) return launch_filter_t<OutT, 384, 16>(p, a, threads, npairs, st);
+  return launch_filter_t<OutT, 512, 16>(p, a, threads, npairs, st);
 }
 
-template <typename OutT, int T>
-int launch_batch_t(const FilterPlan &p, const atb_filter_item *items, int nitems, int npairs, cudaStream_t st) {
-  const size_t smem = smem_bytes(p.n);
-  const int rc = atb::ensure_smem(filter_batch_kernel<OutT, T>, smem, "atb_filter_rows_batch");
+template <typename OutT, int T, int E>
+int launch_batch_t(const FilterPlan &p, const atb_filter_item *items, int nitems, int nt, int npairs,
+                   cudaStream_t st) {
+  const size_t smem = buf_bytes(p.n);
+  const int rc = atb::ensure_smem(filter_batch_kernel<OutT, T, E>, smem, "atb_filter_rows_batch");
   if (rc != ATB_OK) return rc;
-  filter_batch_kernel<OutT, T><<<(unsigned)npairs, T, smem, st>>>(p, items, nitems);
+  filter_batch_kernel<OutT, T, E><<<(unsigned)npairs, nt, smem, st>>>(p, items, nitems);
   return atb::check_launch("atb_filter_rows_batch");
 }
 
 template <typename OutT>
-int launch_batch(const FilterPlan &p, int threads, const atb_filter_item *items, int nitems, int npairs,
-                 cudaStream_t st) {
-  switch (threads) {
-    case 512: return launch_batch_t<OutT, 512>(p, items, nitems, npairs, st);
-    case 256: return launch_batch_t<OutT, 256>(p, items, nitems, npairs, st);
-    case 128: return launch_batch_t<OutT, 128>(p, items, nitems, npairs, st);
-    default: return launch_batch_t<OutT, 64>(p, items, nitems, npairs, st);
-  }
+int launch_batch(const FilterPlan &p, int threads, int budget, const atb_filter_item *items, int nitems,
+                 int npairs, cudaStream_t st) {
+  if (budget > 16) return launch_batch_t<OutT, 512, 32>(p, items, nitems, threads, npairs, st);
+  if (threads <= 128) return launch_batch_t<OutT, 128, 16>(p, items, nitems, threads, npairs, st);
+  if (threads <= 256) return launch_batch_t<OutT, 256, 16>(p, items, nitems, threads, npairs, st);
+  if (threads <= 384) return launch_batch_t<OutT, 384, 16>(p, items, nitems, threads, npairs, st);
+  return launch_batch_t<OutT, 512, 16>(p, items, nitems, threads, npairs, st);
 }
 
 }  // namespace
@@ -675,8 +870,8 @@ int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_
   if (spec_rows != 1 && spec_rows != nrow)
     return atb::fail(ATB_EINVAL, "atb_filter_rows: spec_rows=%d must be 1 or nrow=%d", spec_rows, nrow);
   FilterPlan p;
-  int threads = 0;
-  if (!valid_length(fft_len, ncol, pad) || !make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads))
+  int threads = 0, budget = 0;
+  if (!valid_length(fft_len, ncol, pad) || !make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads, budget))
     return atb::fail(ATB_EINVAL, "atb_filter_rows: fft_len=%d is not a transform length for ncol=%d pad=%d "
                      "(atb_filter_length gives one)", fft_len, ncol, pad);
   FilterRows a;
@@ -697,9 +892,9 @@ int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_
   if (npairs > 0x7fffffffLL) return atb::fail(ATB_ERANGE, "atb_filter_rows: too many rows");
   cudaStream_t st = atb::as_stream(stream);
   switch (dst_dtype) {
-    case ATB_F32: return launch_filter<float>(p, a, threads, npairs, st);
-    case ATB_F16: return launch_filter<__half>(p, a, threads, npairs, st);
-    case ATB_BF16: return launch_filter<__nv_bfloat16>(p, a, threads, npairs, st);
+    case ATB_F32: return launch_filter<float>(p, a, threads, budget, npairs, st);
+    case ATB_F16: return launch_filter<__half>(p, a, threads, budget, npairs, st);
+    case ATB_BF16: return launch_filter<__nv_bfloat16>(p, a, threads, budget, npairs, st);
     default: return atb::fail(ATB_EINVAL, "atb_filter_rows: unknown dst_dtype %d", dst_dtype);
   }
 }
@@ -711,16 +906,16 @@ int atb_filter_rows_batch(const atb_filter_item *items, int nitems, int npairs, 
   if (pad_mode < ATB_PAD_EDGE || pad_mode > ATB_PAD_MEDIAN)
     return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown pad_mode %d", pad_mode);
   FilterPlan p;
-  int threads = 0;
+  int threads = 0, budget = 0;
   // every item needs fft_len == its N or fft_len >= N + ncol - 1; the
   // kernel skips items longer than fft_len
-  if (!make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads))
+  if (!make_plan(fft_len, pad_mode, apply_log, twiddle, p, threads, budget))
     return atb::fail(ATB_ERANGE, "atb_filter_rows_batch: fft_len=%d has no plan", fft_len);
   cudaStream_t st = atb::as_stream(stream);
   switch (dst_dtype) {
-    case ATB_F32: return launch_batch<float>(p, threads, items, nitems, npairs, st);
-    case ATB_F16: return launch_batch<__half>(p, threads, items, nitems, npairs, st);
-    case ATB_BF16: return launch_batch<__nv_bfloat16>(p, threads, items, nitems, npairs, st);
+    case ATB_F32: return launch_batch<float>(p, threads, budget, items, nitems, npairs, st);
+    case ATB_F16: return launch_batch<__half>(p, threads, budget, items, nitems, npairs, st);
+    case ATB_BF16: return launch_batch<__nv_bfloat16>(p, threads, budget, items, nitems, npairs, st);
     default: return atb::fail(ATB_EINVAL, "atb_filter_rows_batch: unknown dst_dtype %d", dst_dtype);
   }
 }
