@@ -12,7 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libalgotom_b200.so")
 
 # every symbol include/algotom_b200.h declares
-EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_length",
+EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_length", "atb_filter_twiddles",
            "atb_filter_rows", "atb_neg_log", "atb_backproject",
            "atb_backproject_status", "atb_backproject_centers",
            "atb_radon_workspace", "atb_radon_adjoint", "atb_bp_batch_plan",
@@ -65,6 +65,7 @@ _SIGS = {
     "atb_version": (ctypes.c_int, []),
     "atb_last_error": (ctypes.c_char_p, []),
     "atb_filter_length": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "atb_filter_twiddles": (ctypes.c_int, [ctypes.c_int, _vp]),
     "atb_copy_2d": (ctypes.c_int, [_vp, _c_i64, _vp, _c_i64, _c_i64, _c_i64,
                                    ctypes.c_int, _vp]),
     "atb_filter_rows": (ctypes.c_int, [

@@ -246,31 +246,52 @@ __device__ __forceinline__ void load_twiddles_n(const double2 *tw, int n, double
     tws[i] = i < kTwLo ? (i < n ? __ldg(tw + i) : make_double2(1.0, 0.0)) : __ldg(tw + (i - kTwLo) * kTwLo);
 }
 
+// One in-place stage on two butterflies per thread at a time: both load
+// before either computes (a stage's butterflies touch disjoint elements),
+// which doubles the independent work in flight per thread.  The twiddles
+// of a butterfly are w, w^2, ..., w^(R-1) of one table value w by repeated
+// products (at most R - 2 extra roundings in FP64, against R - 1 table
+// lookups of two shared-memory reads each).  n and L are powers of two, so
+// the butterfly's block and offset come from a shift and a mask.
+template <int R, bool INV>
+__device__ __forceinline__ void ip_butterfly(double2 (&v)[R], int n1, int tstep, const double2 *tws) {
+  const double2 rc[6] = {};
+  if constexpr (!INV) dft<R, false>(v, rc);
+  if (n1) {
+    const double2 w = twiddle(tws, n1 * tstep);
+    double2 wk = w;
+#pragma unroll
+    for (int k = 1; k < R; ++k) {
+      v[k] = INV ? cmulc(v[k], wk) : cmul(v[k], wk);
+      if (k + 1 < R) wk = cmul(wk, w);
+    }
+  }
+  if constexpr (INV) dft<R, true>(v, rc);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void ip_stage(double2 *x, int n, int L, const double2 *tws) {
-  const int s = L / R, tstep = n / L;
-  const double2 rc[6] = {};
-  for (int q = threadIdx.x; q < n / R; q += blockDim.x) {
-    const int b = q / s, n1 = q - b * s;
-    double2 *p = x + b * L + n1;
-    double2 v[R];
+  const int s = L / R, tstep = n / L, nq = n / R, nt = blockDim.x;
+  const int sh = __ffs(s) - 1;  // s = 2^sh
+  for (int q0 = threadIdx.x; q0 < nq; q0 += 2 * nt) {
+    const int q1 = q0 + nt;
+    const bool two = q1 < nq;
+    const int n10 = q0 & (s - 1), n11 = q1 & (s - 1);
+    double2 *p0 = x + (q0 >> sh) * L + n10;
+    double2 *p1 = x + (q1 >> sh) * L + n11;
+    double2 v0[R], v1[R];
 #pragma unroll
-    for (int j = 0; j < R; ++j) v[j] = p[j * s];
-    if constexpr (!INV) {
-      dft<R, false>(v, rc);
-      if (n1) {
-#pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], twiddle(tws, k * n1 * tstep));
-      }
-    } else {
-      if (n1) {
-#pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], twiddle(tws, k * n1 * tstep));
-      }
-      dft<R, true>(v, rc);
+    for (int j = 0; j < R; ++j) {
+      v0[j] = p0[j * s];
+      v1[j] = two ? p1[j * s] : make_double2(0.0, 0.0);
     }
+    ip_butterfly<R, INV>(v0, n10, tstep, tws);
+    ip_butterfly<R, INV>(v1, n11, tstep, tws);
 #pragma unroll
-    for (int j = 0; j < R; ++j) p[j * s] = v[j];
+    for (int j = 0; j < R; ++j) {
+      p0[j * s] = v0[j];
+      if (two) p1[j * s] = v1[j];
+    }
   }
 }
 

@@ -38,7 +38,6 @@ namespace {
 
 constexpr int kMaxLen = 16384;  // 16384 complex (+1/16 padding) = 136 KiB of shared memory
 constexpr int kMaxStages = 14;
-constexpr int kTwLo = 64;       // two-level twiddle tables: w^t = ta[t / 64] tb[t % 64]
 
 // Shared-memory index of complex element i.  (A padding word every 16 or
 // 32 elements trims the bank conflicts of the first stages' strided
@@ -51,7 +50,7 @@ __device__ __forceinline__ int pidx(int i) { return i; }
 // time, so kernels take it as a __grid_constant__ parameter).
 struct FilterPlan {
   int mode, apply_log;
-  const float2 *tw;    // [n] exp(-2 pi i t / n)
+  const float2 *tw;    // [n] the stages' twiddles (atb_filter_twiddles)
   int n, nstages;      // transform length and its radices, in stage order
   int radix[kMaxStages];
   unsigned magic[kMaxStages];  // ceil(2^32 / Ns) for Ns > 1: j / Ns = umulhi(j, magic) for j, Ns < 2^14
@@ -193,19 +192,19 @@ __host__ __device__ constexpr int butterflies(int r, int e) { return (e + r - 1)
 // (k = j mod Ns, w = exp(-2 pi i / (Ns R))), does an R-point DFT and writes
 // output q to x[(j - k) R + k + q Ns].  Every thread reads all of its
 // inputs before the barrier and writes after it, so one buffer suffices.
-// Twiddles exp(-2 pi i t / n) = ta[t / 64] * tb[t % 64] come from two short
-// tables in shared memory; w^r is the product of the table values of the
-// powers 1, 2, 4, 8 in r (at most three roundings, against 2 (R - 1) table
-// reads per butterfly).  The launch's thread count is a run-time value
+// The twiddles w^(r k), r = 1 .. R-1, of butterfly k are R - 1
+// consecutive entries of the stage's table (tw + Ns - 1 + k (R - 1)),
+// computed in FP64 on the host: one read each, no index arithmetic beyond
+// the base, no products.  The launch's thread count is a run-time value
 // (blockDim.x); a thread holds up to kB butterflies of the stage.  Values
 // of butterflies a thread skips are zeroed, not left undefined: undefined
 // values on predicated paths made the compiler keep them alive across the
 // pair loop and spill.
 template <int R, int E>
 __device__ __forceinline__ void fft_stage(float2 *x, const StagePlan &a, int Ns, unsigned magic,
-                                          const float2 *ta, const float2 *tb) {
+                                          const float2 *tw) {
   constexpr int kB = butterflies(R, E);
-  const int n = a.n, Q = n / R, tstep = n / (Ns * R);
+  const int n = a.n, Q = n / R;
   const int nt = blockDim.x, nb = (Q + nt - 1) / nt;  // butterflies per thread (<= kB; CTA-uniform)
   float2 rc[6];
   if constexpr (R % 2 == 1) {
@@ -226,23 +225,9 @@ __device__ __forceinline__ void fft_stage(float2 *x, const StagePlan &a, int Ns,
     if (b < nb && j < Q) {
       const int k = Ns == 1 ? 0 : j - (int)__umulhi((unsigned)j, magic) * Ns;  // j mod Ns
       if (k) {
-        const int e = k * tstep;  // w^r = exp(-2 pi i r e / n)
-        auto tw = [&](int c) {
-          const int t = c * e;
-          return cmul(ta[t >> 6], tb[t & (kTwLo - 1)]);
-        };
-        const float2 w1 = tw(1);
-        const float2 w2 = R >= 3 ? tw(2) : w1;
-        const float2 w4 = R >= 5 ? tw(4) : w1;
-        const float2 w8 = R >= 9 ? tw(8) : w1;
+        const float2 *w = tw + (Ns - 1) + k * (R - 1);
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          float2 w = (r & 1) ? w1 : ((r & 2) ? w2 : ((r & 4) ? w4 : w8));
-          if ((r & 1) && (r & 2)) w = cmul(w, w2);
-          if ((r & 3) && (r & 4)) w = cmul(w, w4);
-          if ((r & 7) && (r & 8)) w = cmul(w, w8);
-          v[b][r] = cmul(v[b][r], w);
-        }
+        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], w[r - 1]);
       }
       dft<R>(v[b], rc);
       const int o = (j - k) * R + k;
@@ -258,18 +243,18 @@ __device__ __forceinline__ void fft_stage(float2 *x, const StagePlan &a, int Ns,
 // inlined copy of each stage kind in sequence (a switch inside a loop over
 // the stages makes the compiler spill).
 template <int E>
-__device__ __forceinline__ void fft_forward(float2 *x, const StagePlan &a, const float2 *ta, const float2 *tb) {
+__device__ __forceinline__ void fft_forward(float2 *x, const StagePlan &a, const float2 *tw) {
   int s = 0, Ns = 1;
   const int ns = a.nstages;
-  for (; s < ns && a.radix[s] == 16; ++s, Ns *= 16) fft_stage<16, E>(x, a, Ns, a.magic[s], ta, tb);
-  if (s < ns && a.radix[s] == 8) { fft_stage<8, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 8; }
-  if (s < ns && a.radix[s] == 4) { fft_stage<4, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 4; }
-  if (s < ns && a.radix[s] == 2) { fft_stage<2, E>(x, a, Ns, a.magic[s], ta, tb); ++s; Ns *= 2; }
-  for (; s < ns && a.radix[s] == 13; ++s, Ns *= 13) fft_stage<13, E>(x, a, Ns, a.magic[s], ta, tb);
-  for (; s < ns && a.radix[s] == 11; ++s, Ns *= 11) fft_stage<11, E>(x, a, Ns, a.magic[s], ta, tb);
-  for (; s < ns && a.radix[s] == 7; ++s, Ns *= 7) fft_stage<7, E>(x, a, Ns, a.magic[s], ta, tb);
-  for (; s < ns && a.radix[s] == 5; ++s, Ns *= 5) fft_stage<5, E>(x, a, Ns, a.magic[s], ta, tb);
-  for (; s < ns && a.radix[s] == 3; ++s, Ns *= 3) fft_stage<3, E>(x, a, Ns, a.magic[s], ta, tb);
+  for (; s < ns && a.radix[s] == 16; ++s, Ns *= 16) fft_stage<16, E>(x, a, Ns, a.magic[s], tw);
+  if (s < ns && a.radix[s] == 8) { fft_stage<8, E>(x, a, Ns, a.magic[s], tw); ++s; Ns *= 8; }
+  if (s < ns && a.radix[s] == 4) { fft_stage<4, E>(x, a, Ns, a.magic[s], tw); ++s; Ns *= 4; }
+  if (s < ns && a.radix[s] == 2) { fft_stage<2, E>(x, a, Ns, a.magic[s], tw); ++s; Ns *= 2; }
+  for (; s < ns && a.radix[s] == 13; ++s, Ns *= 13) fft_stage<13, E>(x, a, Ns, a.magic[s], tw);
+  for (; s < ns && a.radix[s] == 11; ++s, Ns *= 11) fft_stage<11, E>(x, a, Ns, a.magic[s], tw);
+  for (; s < ns && a.radix[s] == 7; ++s, Ns *= 7) fft_stage<7, E>(x, a, Ns, a.magic[s], tw);
+  for (; s < ns && a.radix[s] == 5; ++s, Ns *= 5) fft_stage<5, E>(x, a, Ns, a.magic[s], tw);
+  for (; s < ns && a.radix[s] == 3; ++s, Ns *= 3) fft_stage<3, E>(x, a, Ns, a.magic[s], tw);
 }
 
 // Block-wide reduction over T threads (op: 0 sum, 1 max, 2 min).
@@ -362,12 +347,9 @@ __device__ __forceinline__ PairIdx pair_rows(const FilterRows &a, int pair) {
   return r;
 }
 
-// Twiddle tables ta[u] = w^(64 u), tb[v] = w^v (w = exp(-2 pi i / n)) and
-// the stage plan into shared memory, visible after the next barrier.
-__device__ __forceinline__ void load_tables(const FilterPlan &p, float2 *ta, float2 *tb, StagePlan &sp) {
-  const int M = p.n, nt = blockDim.x;
-  for (int u = threadIdx.x; u < (M + kTwLo - 1) / kTwLo; u += nt) ta[u] = __ldg(p.tw + u * kTwLo);
-  for (int v = threadIdx.x; v < kTwLo; v += nt) tb[v] = v < M ? __ldg(p.tw + v) : make_float2(1.f, 0.f);
+// The stage plan into shared memory, visible after the next barrier.
+__device__ __forceinline__ void load_tables(const FilterPlan &p, StagePlan &sp) {
+  const int nt = blockDim.x;
   for (int i = threadIdx.x; i < kMaxStages; i += nt) {
     sp.radix[i] = p.radix[i];
     sp.magic[i] = p.magic[i];
@@ -386,8 +368,8 @@ __device__ __forceinline__ void load_tables(const FilterPlan &p, float2 *ta, flo
 // reads of sm are not followed by one.
 template <typename OutT, int T, int E>
 __device__ __forceinline__ void pad_transform_store(const FilterPlan &p, const StagePlan &sp, const FilterRows &a,
-                                                    float2 *sm, const float2 *spec, const float2 *ta,
-                                                    const float2 *tb, float2 *scratch, const PairIdx &r) {
+                                                    float2 *sm, const float2 *spec, const float2 *tw,
+                                                    float2 *scratch, const PairIdx &r) {
   const int M = p.n, ncol = a.ncol, pad = a.pad, tid = threadIdx.x;
   // padding (numpy.pad semantics along the row)
   if (pad > 0) {
@@ -458,7 +440,7 @@ __device__ __forceinline__ void pad_transform_store(const FilterPlan &p, const S
   // would double the code the SMs fetch)
 #pragma unroll 1
   for (int pass = 0; pass < 2; ++pass) {
-    fft_forward<E>(sm, sp, ta, tb);
+    fft_forward<E>(sm, sp, tw);
     if (pass == 1) break;
     for (int k = tid; k < M; k += (int)blockDim.x) {
       const float2 y = cmul(sm[pidx(k)], spec[k]);
@@ -483,13 +465,12 @@ template <typename OutT, int T, int E>
 __device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const FilterRows &a, int pair) {
   extern __shared__ float2 sm[];  // n complex
   __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
-  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
   __shared__ StagePlan sp;
   const int M = p.n;
   const int ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad;
   const int tid = threadIdx.x, nt = blockDim.x;
   if (N > M) return;  // not a length for these rows (CTA-uniform)
-  load_tables(p, ta, tb, sp);
+  load_tables(p, sp);
   const PairIdx r = pair_rows(a, pair);
   const float *s1 = a.src + r.i1 * a.srs + r.k1 * a.sss;
   const float *s2 = a.src + (r.ok2 ? r.i2 * a.srs + r.k2 * a.sss : 0);
@@ -502,7 +483,7 @@ __device__ __forceinline__ void filter_rows_body(const FilterPlan &p, const Filt
   for (int m = N + tid; m < M; m += nt) sm[pidx(m)] = make_float2(0.f, 0.f);
   __syncthreads();
   const float2 *spec = a.spec + (a.spec_rows > 1 ? (long long)r.i1 * M : 0LL);
-  pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, ta, tb, scratch, r);
+  pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, p.tw, scratch, r);  // twiddles through L1
 }
 
 // ---- asynchronous copies global -> shared (cp.async; completion is waited
@@ -554,8 +535,9 @@ __device__ __forceinline__ void stage_rows(const FilterRows &a, const PairIdx &r
 constexpr int min_blocks(int t, int e) { return t > 384 ? 1 : (t > 256 || e > 16 ? 2 : 3); }
 
 // Shared-memory layout of the persistent kernel (bytes): the transform
-// buffer, the staged rows of the next pair, the spectrum (one kernel for
-// every row only).
+// buffer, the staged rows of the next pair, the twiddle table, the
+// spectrum (one kernel for every row, when it fits without costing a CTA
+// per SM).
 __host__ __device__ constexpr size_t buf_bytes(int n) { return sizeof(float2) * (size_t)((n + 1) & ~1); }
 __host__ __device__ constexpr int ncol4_of(int ncol) { return (ncol + 3) & ~3; }
 __host__ __device__ constexpr size_t stage_bytes(int ncol) { return sizeof(float) * 2 * (size_t)ncol4_of(ncol); }
@@ -570,15 +552,16 @@ __global__ void __launch_bounds__(T, min_blocks(T, E))
                        int spec_in_smem) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ float2 scratch[T / 32 > 0 ? T / 32 : 1];
-  __shared__ float2 ta[kMaxLen / kTwLo], tb[kTwLo];
   __shared__ StagePlan sp;
   const int M = p.n, ncol = a.ncol, pad = a.pad, N = ncol + 2 * pad, ncol4 = ncol4_of(ncol);
   const int tid = threadIdx.x, nt = blockDim.x;
   float2 *sm = reinterpret_cast<float2 *>(smraw);
   float *stage = reinterpret_cast<float *>(smraw + buf_bytes(M));
-  float2 *spec_s = reinterpret_cast<float2 *>(smraw + buf_bytes(M) + stage_bytes(ncol));
+  float2 *tw_s = reinterpret_cast<float2 *>(smraw + buf_bytes(M) + stage_bytes(ncol));
+  float2 *spec_s = tw_s + ((M + 1) & ~1);
   const bool shared_spec = spec_in_smem && a.spec_rows == 1;
-  load_tables(p, ta, tb, sp);
+  load_tables(p, sp);
+  for (int k = tid; k < M; k += nt) cp_async8(tw_s + k, p.tw + k);
   if (shared_spec)
     for (int k = tid; k < M; k += nt) cp_async8(spec_s + k, a.spec + k);
   int pair = blockIdx.x;
@@ -598,7 +581,7 @@ __global__ void __launch_bounds__(T, min_blocks(T, E))
     const int next = pair + gridDim.x;
     if (next < npairs) stage_rows(a, pair_rows(a, next), stage, ncol4);
     const float2 *spec = shared_spec ? spec_s : a.spec + (a.spec_rows > 1 ? (long long)r.i1 * M : 0LL);
-    pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, ta, tb, scratch, r);
+    pad_transform_store<OutT, T, E>(p, sp, a, sm, spec, tw_s, scratch, r);
   }
 }
 
@@ -789,10 +772,10 @@ int max_smem() {
 
 template <typename OutT, int T, int E>
 int launch_filter_t(const FilterPlan &p, const FilterRows &a, int nt, long long npairs, cudaStream_t st) {
-  // shared memory besides the dynamic part: twiddle tables, plan, scratch
-  const size_t fixed = sizeof(float2) * (kMaxLen / kTwLo + kTwLo + 32) + sizeof(StagePlan);
+  // shared memory besides the dynamic part: plan, scratch
+  const size_t fixed = sizeof(float2) * 32 + sizeof(StagePlan);
   const size_t limit = (size_t)max_smem() - fixed;
-  const size_t base = buf_bytes(p.n) + stage_bytes(a.ncol), spec = sizeof(float2) * p.n;
+  const size_t base = buf_bytes(p.n) + stage_bytes(a.ncol) + buf_bytes(p.n), spec = sizeof(float2) * p.n;
   if (base > limit) {  // no room to stage rows: one CTA per pair
     const size_t smem = buf_bytes(p.n);
     const int rc = atb::ensure_smem(filter_rows_direct_kernel<OutT, T, E>, smem, "atb_filter_rows");
@@ -800,15 +783,20 @@ int launch_filter_t(const FilterPlan &p, const FilterRows &a, int nt, long long 
     filter_rows_direct_kernel<OutT, T, E><<<(unsigned)npairs, nt, smem, st>>>(p, a);
     return atb::check_launch("atb_filter_rows");
   }
-  const int spec_in_smem = a.spec_rows == 1 && base + spec <= limit;
+  // the spectrum in shared memory only if that costs no CTA per SM
+  auto resident = [&](size_t bytes) {
+    int n = 0;
+    if (atb::ensure_smem(filter_rows_kernel<OutT, T, E>, bytes, "atb_filter_rows") != ATB_OK ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, filter_rows_kernel<OutT, T, E>, nt, bytes) != cudaSuccess)
+      return 0;
+    return n;
+  };
+  int per_sm = resident(base);
+  if (per_sm < 1) return atb::fail(ATB_ECUDA, "atb_filter_rows: no CTA of %d bytes fits an SM", (int)base);
+  const int spec_in_smem = a.spec_rows == 1 && base + spec <= limit && resident(base + spec) >= per_sm;
   const size_t smem = base + (spec_in_smem ? spec : 0);
   const int rc = atb::ensure_smem(filter_rows_kernel<OutT, T, E>, smem, "atb_filter_rows");
   if (rc != ATB_OK) return rc;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, filter_rows_kernel<OutT, T, E>, nt, smem) !=
-          cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
   const long long grid = std::min<long long>(npairs, (long long)per_sm * sm_count());
   filter_rows_kernel<OutT, T, E><<<(unsigned)grid, nt, smem, st>>>(p, a, (int)npairs, spec_in_smem);
   return atb::check_launch("atb_filter_rows");
@@ -855,6 +843,33 @@ int atb_filter_length(int ncol, int pad) {
     return atb::fail(ATB_ERANGE, "atb_filter_length: ncol=%d pad=%d needs a transform longer than %d", ncol, pad,
                      kMaxLen);
   return n;
+}
+
+int atb_filter_twiddles(int n, void *host_out) {
+  if (!host_out) return atb::fail(ATB_EINVAL, "atb_filter_twiddles: null pointer");
+  int radix[kMaxStages], ns = 0;
+  if (n < 2 || n > kMaxLen || !make_radices(n, radix, ns))
+    return atb::fail(ATB_EINVAL, "atb_filter_twiddles: %d is not a transform length of the filter", n);
+  float *out = static_cast<float *>(host_out);
+  // stage s of radix R after sub-transforms of length Ns: entries
+  // Ns - 1 + k (R - 1) + (r - 1) = exp(-2 pi i r k / (Ns R)), k < Ns, 0 < r < R
+  // (the stages' Ns (R - 1) add up to n - 1; entry n - 1 is unused)
+  int Ns = 1;
+  for (int st = 0; st < ns; ++st) {
+    const int R = radix[st];
+    for (int k = 0; k < Ns; ++k)
+      for (int r = 1; r < R; ++r) {
+        const long long e = (long long)r * k;
+        const double ang = -2.0 * M_PI * (double)e / (double)(Ns * R);
+        float *o = out + 2 * (Ns - 1 + k * (R - 1) + (r - 1));
+        o[0] = (float)std::cos(ang);
+        o[1] = (float)std::sin(ang);
+      }
+    Ns *= R;
+  }
+  out[2 * (n - 1)] = 1.0f;
+  out[2 * (n - 1) + 1] = 0.0f;
+  return ATB_OK;
 }
 
 int atb_filter_rows(const float *src, int64_t src_row_stride, int64_t src_slice_stride, int nrow, int nslice,

@@ -90,11 +90,15 @@ def _trig(angles, device):
 
 
 def _twiddle(m, device):
+    """Device twiddle table of the row filter's length-m transforms
+    (``atb_filter_twiddles``: each FFT stage's twiddles in the order the
+    kernel reads them, FP64-computed), cached per (m, device)."""
     key = (m, device)
     t = _tw_cache.get(key)
     if t is None:
-        tw = win.twiddles(m)
-        t = torch.from_numpy(tw.view(np.float32).copy()).to(device)
+        tw = np.empty(2 * m, dtype=np.float32)
+        nat.call("atb_filter_twiddles", int(m), tw.ctypes.data)
+        t = torch.from_numpy(tw).to(device)
         _tw_cache[key] = t
     return t
 

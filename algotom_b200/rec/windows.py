@@ -21,7 +21,6 @@ positions.  Taking ``real`` of the inverse transform keeps only the
 Hermitian part of ``H``, which this construction inherits automatically.
 """
 import math
-from functools import lru_cache
 
 import numpy as np
 import scipy.ndimage as ndi
@@ -88,13 +87,6 @@ def row_filter_spectrum(window_rows, ncol, pad, m):
         b = np.zeros((w.shape[0], m))
         b[:, lags % m] = kappa[:, lags % n]
     return (np.fft.fft(b, axis=1) / m).astype(np.complex64)
-
-
-@lru_cache(maxsize=16)
-def twiddles(m):
-    """exp(-2 pi i t / m), t in [0, m), complex64 from FP64."""
-    t = np.arange(m, dtype=np.float64)
-    return np.exp(-2j * np.pi * t / m).astype(np.complex64)
 
 
 def make_circular_ramp_window(width, filter_name=None):

@@ -84,6 +84,16 @@ int atb_copy_2d(void *dst, int64_t dst_pitch, const void *src,
 int atb_filter_length(int ncol, int pad);
 
 /*
+ * The twiddle table of the row filter's transforms of length n (a length
+ * atb_filter_length returns), written to HOST memory: n complex64 values,
+ * the twiddles of each FFT stage in the order the kernel reads them
+ * (exp(-2 pi i r k / (Ns R)) for stage radix R after sub-transforms of
+ * length Ns), computed in FP64.  The caller copies it to the device once
+ * per length and passes it as `twiddle`.
+ */
+int atb_filter_twiddles(int n, void *host_out);
+
+/*
  * Padded ramp-and-window filter of every row of a sinogram stack, with the
  * optional -log folded in; replaces apply_ramp_filter
  * (algotom/rec/reconstruction.py:118-153) and the -log pre-step
@@ -95,7 +105,7 @@ int atb_filter_length(int ncol, int pad);
  *            real kernel, already scaled by 1 / fft_len.  spec_rows = 1 (one
  *            kernel for every row) or nrow (one kernel per angle; then two
  *            slices of one angle share a transform)
- *   twiddle  complex64 [fft_len]: exp(-2 pi i t / fft_len)
+ *   twiddle  complex64 [fft_len]: atb_filter_twiddles(fft_len) on the device
  *   fft_len  a length with fft_len == ncol + 2 pad (no prime factor above
  *            13) or fft_len >= 2 ncol + 2 pad - 1 (7-smooth), at most 16384;
  *            atb_filter_length gives the cheapest

@@ -71,11 +71,41 @@ def test_spectrum_rejects_short_fft():
         W.row_filter_spectrum(W.ramp_window_row(100, "hann"), 80, 10, 101)
 
 
-def test_twiddles():
-    for m in (64, 60, 2860):
-        t = W.twiddles(m)
-        np.testing.assert_allclose(
-            t, np.exp(-2j * np.pi * np.arange(m) / m), atol=1e-7)
+def test_filter_twiddles():
+    """atb_filter_twiddles: each stage's exp(-2 pi i r k / (Ns R)) at
+    Ns - 1 + k (R - 1) + r - 1, the stages in the kernel's radix order."""
+    def radices(n):
+        out, m = [], n
+        while m % 16 == 0:
+            out.append(16)
+            m //= 16
+        for q in (8, 4, 2):
+            if m % q == 0:
+                out.append(q)
+                m //= q
+        for q in (13, 11, 7, 5, 3):
+            while m % q == 0:
+                out.append(q)
+                m //= q
+        return out
+    for n in (64, 60, 2860, 2560, 4410):
+        t = np.empty(2 * n, np.float32)
+        nat.call("atb_filter_twiddles", n, t.ctypes.data)
+        t = t.view(np.complex64)
+        ref = np.zeros(n, np.complex128)
+        ns = 1
+        for r_ in radices(n):
+            for k in range(ns):
+                for r in range(1, r_):
+                    ref[ns - 1 + k * (r_ - 1) + r - 1] = np.exp(
+                        -2j * np.pi * r * k / (ns * r_))
+            ns *= r_
+        ref[n - 1] = 1.0
+        np.testing.assert_allclose(t, ref, atol=1e-7)
+    lib = nat.load()
+    t = np.empty(2 * 17, np.float32)
+    assert lib.atb_filter_twiddles(17, t.ctypes.data) == -1  # no plan for 17
+    assert lib.atb_filter_twiddles(16, None) == -1
 
 
 def test_phantom_sinogram_is_exact_line_integral():
