@@ -25,6 +25,8 @@
 
 namespace {
 
+using atb::spline::fir_block;
+using atb::spline::fir_pad;
 using atb::spline::make_taps;
 using atb::spline::sym_index;
 using atb::spline::Taps;
@@ -32,6 +34,8 @@ using atb::spline::Taps;
 constexpr int kPad = 12;       // end samples replicated on each side
 constexpr int kThreads = 256;
 constexpr int kMaxCols = 16384;
+constexpr int kTaps = 32;      // the cubic prefilter's taps (make_taps(3).ntaps)
+constexpr int kBlk = 8;        // coefficients per thread and window
 
 struct RowArgs {
   const float *src;
@@ -49,7 +53,7 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.ncol, big = n + 2 * kPad;
   double *c = reinterpret_cast<double *>(smem);  // [big] spline coefficients
-  float *x = reinterpret_cast<float *>(c + big);  // [big] the padded row
+  float *x = reinterpret_cast<float *>(c + big);  // [fir_pad(big)] the padded row, padded layout
   float *y;                                       // [n] the (shifted) row
   const int row = blockIdx.x;
   const float *src = a.src + row * a.srs;
@@ -57,15 +61,19 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
     const int col = min(max(k - kPad, 0), n - 1);
     float v = src[min(a.flip ? n - 1 - col : col, a.ncol_src - 1)];
     if (a.apply_log) v = -logf(v);
-    x[k] = v;
+    x[fir_pad(k)] = v;
   }
   __syncthreads();
   if (a.shift != 0.0) {
-    for (int k = threadIdx.x; k < big; k += kThreads) {
-      double acc = taps.h[0] * (double)x[k];
-      for (int m = 1; m <= taps.ntaps; ++m)
-        acc += taps.h[m] * ((double)x[sym_index(k - m, big, 0)] + (double)x[sym_index(k + m, big, 0)]);
-      c[k] = acc;
+    // kBlk consecutive coefficients per thread from one sliding window
+    // (each staged value read once per window, not once per tap)
+    for (int k0 = threadIdx.x * kBlk; k0 < big; k0 += kThreads * kBlk) {
+      double acc[kBlk];
+      fir_block<kTaps, kBlk>(
+          taps, [&](int t) { return (double)x[fir_pad(sym_index(k0 + t - kTaps, big, 0))]; }, acc);
+#pragma unroll
+      for (int r = 0; r < kBlk; ++r)
+        if (k0 + r < big) c[k0 + r] = acc[r];
     }
     __syncthreads();
     y = x;  // the padded row is no longer read
@@ -88,7 +96,7 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
     }
   } else {
     y = reinterpret_cast<float *>(c);  // no coefficients needed
-    for (int k = threadIdx.x; k < n; k += kThreads) y[k] = x[k + kPad];
+    for (int k = threadIdx.x; k < n; k += kThreads) y[k] = x[fir_pad(k + kPad)];
   }
   __syncthreads();
   float *dst = a.dst + row * a.drs;
@@ -122,7 +130,8 @@ __global__ void __launch_bounds__(kThreads) row_kernel(RowArgs a, Taps taps) {
 
 int launch_rows(const RowArgs &a, const char *what, void *stream) {
   static const Taps taps = make_taps(3);
-  const size_t smem = (sizeof(double) + sizeof(float)) * (a.ncol + 2 * kPad);
+  const int big = a.ncol + 2 * kPad;
+  const size_t smem = sizeof(double) * big + sizeof(float) * (big + (big >> 3) + 1);
   int rc = atb::ensure_smem(row_kernel, smem, what);
   if (rc != ATB_OK) return rc;
   row_kernel<<<a.nrow, kThreads, smem, atb::as_stream(stream)>>>(a, taps);

@@ -30,6 +30,8 @@ namespace {
 
 constexpr int kFirThreads = 256;
 constexpr int kGridThreads = 256;
+using atb::spline::fir_block;
+using atb::spline::fir_pad;
 using atb::spline::sym_index;
 using atb::spline::Taps;
 using atb::spline::make_taps;
@@ -64,61 +66,70 @@ __global__ void __launch_bounds__(kFirThreads)
 }
 
 // Tiled forms: the strip a CTA filters, plus its 2 x ntaps halo (symmetric
-// extension resolved while staging), is staged in shared memory once, so
-// each output's 2 ntaps + 1 reads hit shared memory instead of L2 (the
-// untiled kernel above reads every tap through the cache hierarchy).  Same
-// taps and summation order: the same results bit for bit.
+// extension resolved while staging), is staged in shared memory once, and
+// every thread computes kFirBlk consecutive outputs of one line from one
+// sliding window of kFirBlk + 2 ntaps staged values held in turn in a
+// register: each value is read from shared memory once and feeds up to
+// kFirBlk outputs, against 2 ntaps + 1 reads per output (the untiled
+// kernel above, and a first tiled form, read every tap per output: shared-
+// memory bandwidth bound them).  The tap count is a template parameter, so
+// the window loop unrolls with its taps as constants.
+constexpr int kFirBlk = 8;      // consecutive outputs per thread
 constexpr int kFirLines = 32;   // lines per CTA (filter axis strided)
-constexpr int kFirRows = 64;    // outputs per line per CTA (filter axis strided)
-constexpr int kFirSeg = 128;    // positions per CTA (filter axis contiguous)
+constexpr int kFirRows = kFirBlk * (kFirThreads / 32);  // 64 outputs per line per CTA
+constexpr int kFirSeg = kFirBlk * kFirThreads;          // outputs per CTA (filter axis contiguous)
 
 // filter axis strided, lines contiguous: element (i, l) at src[i * es + l],
-// l < nl; CTA = 32 consecutive l x 64 consecutive i
+// l < nl; CTA = 32 consecutive l x 64 consecutive i, warp w computing
+// positions [8 w, 8 w + 8) of its lane's line
+template <int NT>
 __global__ void __launch_bounds__(kFirThreads)
     prefilter_cols_kernel(const double *__restrict__ src, double *__restrict__ dst, long long es, int nl, int n,
                           int boundary, Taps taps) {
-  extern __shared__ double xs[];  // [kFirRows + 2 ntaps][kFirLines]
+  extern __shared__ double xs[];  // [kFirRows + 2 NT][kFirLines]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int l = blockIdx.x * kFirLines + lane;
   const int i0 = blockIdx.y * kFirRows;
-  const int nt = taps.ntaps, span = kFirRows + 2 * nt;
+  constexpr int span = kFirRows + 2 * NT;
   for (int q = warp; q < span; q += kFirThreads / 32)
-    xs[q * kFirLines + lane] = l < nl ? src[(long long)sym_index(i0 - nt + q, n, boundary) * es + l] : 0.0;
+    xs[q * kFirLines + lane] = l < nl ? src[(long long)sym_index(i0 - NT + q, n, boundary) * es + l] : 0.0;
   __syncthreads();
-  if (l >= nl) return;
-  for (int k0 = warp; k0 < kFirRows; k0 += kFirThreads / 32) {
-    const int i = i0 + k0;
-    if (i >= n) break;
-    const double *c = xs + (nt + k0) * kFirLines + lane;
-    double acc = taps.h[0] * c[0];
-    for (int k = 1; k <= nt; ++k) acc += taps.h[k] * (c[-k * kFirLines] + c[k * kFirLines]);
-    dst[(long long)i * es + l] = acc;
-  }
+  const int r0 = warp * kFirBlk;
+  if (l >= nl || i0 + r0 >= n) return;
+  double acc[kFirBlk];
+  const double *c = xs + r0 * kFirLines + lane;
+  fir_block<NT, kFirBlk>(taps, [&](int t) { return c[t * kFirLines]; }, acc);
+#pragma unroll
+  for (int r = 0; r < kFirBlk; ++r)
+    if (i0 + r0 + r < n) dst[(long long)(i0 + r0 + r) * es + l] = acc[r];
 }
 
 // filter axis contiguous: element (line, i, comp) at
-// src[line * ls + i * ncomp + comp]; CTA = one line x 128 positions
+// src[line * ls + i * ncomp + comp]; CTA = one line x kFirSeg / ncomp
+// positions, thread = one component x kFirBlk consecutive positions
+template <int NT>
 __global__ void __launch_bounds__(kFirThreads)
     prefilter_rows_kernel(const double *__restrict__ src, double *__restrict__ dst, long long ls, int ncomp, int n,
                           int boundary, Taps taps) {
-  extern __shared__ double xs[];  // [(kFirSeg + 2 ntaps) * ncomp]
+  extern __shared__ double xs[];  // per component: fir_pad(kSeg / ncomp + 2 NT) values
   const long long line = blockIdx.y;
-  const int i0 = blockIdx.x * kFirSeg;
-  const int nt = taps.ntaps, span = (kFirSeg + 2 * nt) * ncomp;
+  const int seg = kFirSeg / ncomp, i0 = blockIdx.x * seg;
+  const int span = seg + 2 * NT, stride = fir_pad(span) + 1;
   const double *in = src + line * ls;
-  for (int e = threadIdx.x; e < span; e += kFirThreads) {
+  for (int e = threadIdx.x; e < span * ncomp; e += kFirThreads) {
     const int q = e / ncomp, comp = e - q * ncomp;
-    xs[e] = in[(long long)sym_index(i0 - nt + q, n, boundary) * ncomp + comp];
+    xs[comp * stride + fir_pad(q)] = in[(long long)sym_index(i0 - NT + q, n, boundary) * ncomp + comp];
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < kFirSeg * ncomp; e += kFirThreads) {
-    const int q = e / ncomp, comp = e - q * ncomp, i = i0 + q;
-    if (i >= n) break;
-    const double *c = xs + (nt + q) * ncomp + comp;
-    double acc = taps.h[0] * c[0];
-    for (int k = 1; k <= nt; ++k) acc += taps.h[k] * (c[-k * ncomp] + c[k * ncomp]);
-    dst[line * ls + (long long)i * ncomp + comp] = acc;
-  }
+  const int per = kFirThreads / ncomp, comp = threadIdx.x / per;
+  const int q0 = (threadIdx.x - comp * per) * kFirBlk;
+  if (i0 + q0 >= n) return;
+  double acc[kFirBlk];
+  const double *c = xs + comp * stride;
+  fir_block<NT, kFirBlk>(taps, [&](int t) { return c[fir_pad(q0 + t)]; }, acc);
+#pragma unroll
+  for (int r = 0; r < kFirBlk; ++r)
+    if (i0 + q0 + r < n) dst[line * ls + (long long)(i0 + q0 + r) * ncomp + comp] = acc[r];
 }
 
 __global__ void __launch_bounds__(kGridThreads)
@@ -229,24 +240,36 @@ extern "C" int atb_spline_prefilter(const double *src, double *dst, int64_t line
   static const Taps taps3 = make_taps(3), taps5 = make_taps(5);
   const Taps &taps = order == 5 ? taps5 : taps3;
   cudaStream_t st = atb::as_stream(stream);
+  const int nt = taps.ntaps;
   if (line_stride == ncomp && (long long)nlines * ncomp <= 2147483647LL && (n + kFirRows - 1) / kFirRows <= 65535) {
     // lines contiguous: tiles of 32 lines x 64 positions
     const int nl = nlines * ncomp;
-    const size_t smem = sizeof(double) * kFirLines * (kFirRows + 2 * taps.ntaps);
-    int rc = atb::ensure_smem(prefilter_cols_kernel, smem, "atb_spline_prefilter");
-    if (rc != ATB_OK) return rc;
+    const size_t smem = sizeof(double) * kFirLines * (kFirRows + 2 * nt);
     const dim3 grid((nl + kFirLines - 1) / kFirLines, (n + kFirRows - 1) / kFirRows);
-    prefilter_cols_kernel<<<grid, kFirThreads, smem, st>>>(src, dst, elem_stride, nl, n, boundary, taps);
-    return atb::check_launch("atb_spline_prefilter");
+    int rc;
+    if (nt == 48) {
+      rc = atb::ensure_smem(prefilter_cols_kernel<48>, smem, "atb_spline_prefilter");
+      if (rc == ATB_OK) prefilter_cols_kernel<48><<<grid, kFirThreads, smem, st>>>(src, dst, elem_stride, nl, n, boundary, taps);
+    } else {
+      rc = atb::ensure_smem(prefilter_cols_kernel<32>, smem, "atb_spline_prefilter");
+      if (rc == ATB_OK) prefilter_cols_kernel<32><<<grid, kFirThreads, smem, st>>>(src, dst, elem_stride, nl, n, boundary, taps);
+    }
+    return rc != ATB_OK ? rc : atb::check_launch("atb_spline_prefilter");
   }
   if (elem_stride == ncomp && nlines <= 65535) {
-    // elements contiguous: one line segment of 128 positions per CTA
-    const size_t smem = sizeof(double) * ncomp * (kFirSeg + 2 * taps.ntaps);
-    int rc = atb::ensure_smem(prefilter_rows_kernel, smem, "atb_spline_prefilter");
-    if (rc != ATB_OK) return rc;
-    const dim3 grid((n + kFirSeg - 1) / kFirSeg, nlines);
-    prefilter_rows_kernel<<<grid, kFirThreads, smem, st>>>(src, dst, line_stride, ncomp, n, boundary, taps);
-    return atb::check_launch("atb_spline_prefilter");
+    // elements contiguous: one line segment of kFirSeg / ncomp positions per CTA
+    const int seg = kFirSeg / ncomp;
+    const size_t smem = sizeof(double) * ncomp * (size_t)((seg + 2 * nt) + ((seg + 2 * nt) >> 3) + 1);
+    const dim3 grid((n + seg - 1) / seg, nlines);
+    int rc;
+    if (nt == 48) {
+      rc = atb::ensure_smem(prefilter_rows_kernel<48>, smem, "atb_spline_prefilter");
+      if (rc == ATB_OK) prefilter_rows_kernel<48><<<grid, kFirThreads, smem, st>>>(src, dst, line_stride, ncomp, n, boundary, taps);
+    } else {
+      rc = atb::ensure_smem(prefilter_rows_kernel<32>, smem, "atb_spline_prefilter");
+      if (rc == ATB_OK) prefilter_rows_kernel<32><<<grid, kFirThreads, smem, st>>>(src, dst, line_stride, ncomp, n, boundary, taps);
+    }
+    return rc != ATB_OK ? rc : atb::check_launch("atb_spline_prefilter");
   }
   const long long total = (long long)nlines * ncomp * n;
   const long long blocks = (total + kFirThreads - 1) / kFirThreads;

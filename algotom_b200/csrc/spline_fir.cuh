@@ -74,5 +74,28 @@ __device__ __forceinline__ int sym_index(int i, int n, int boundary) {
   return r >= n ? p - r : r;
 }
 
+// Register-blocked FIR: acc[r] = sum_k h[|k|] x(r + k + NT), |k| <= NT,
+// for BLK consecutive outputs from one sliding window of BLK + 2 NT values
+// x(0), x(1), ... (each read once, feeding up to BLK outputs).  NT is a
+// template parameter, so the loops unroll with the taps as constants.
+template <int NT, int BLK, typename Load>
+__device__ __forceinline__ void fir_block(const Taps &taps, Load load, double (&acc)[BLK]) {
+#pragma unroll
+  for (int r = 0; r < BLK; ++r) acc[r] = 0.0;
+#pragma unroll
+  for (int t = 0; t < BLK + 2 * NT; ++t) {
+    const double x = load(t);
+#pragma unroll
+    for (int r = 0; r < BLK; ++r) {
+      const int k = t - NT - r;
+      if (k >= -NT && k <= NT) acc[r] = fma(taps.h[k < 0 ? -k : k], x, acc[r]);
+    }
+  }
+}
+
+// index of value q in a strip padded by one word every 8 (threads 8 values
+// apart then hit distinct shared-memory banks)
+__device__ __forceinline__ int fir_pad(int q) { return q + (q >> 3); }
+
 }  // namespace spline
 }  // namespace atb
