@@ -94,9 +94,31 @@ def test_filter_limits(cuda):
     # N = 9300 = 2^2 3 5^2 31 and N + ncol - 1 > 16384: no exact length
     with pytest.raises(nat.NativeLibraryError, match="16384"):
         R.apply_ramp_filter(x, None, "hann", 150)
-    got = R.apply_ramp_filter(np.ones((2, 8000), np.float32), None, "hann",
-                              150)
-    assert np.all(np.isfinite(got))
+    # 8000 columns: length 16384, too long to stage rows in shared memory,
+    # so one CTA per row pair reads them from global memory
+    x = np.random.default_rng(2).standard_normal((3, 8000)).astype(np.float32)
+    got = R.apply_ramp_filter(x, None, "hann", 150)
+    assert O.rel_l2(got, O.apply_ramp_filter(x, None, "hann", 150)) < 1e-6
+
+
+@pytest.mark.parametrize("ncol", [2560, 2557])
+def test_filter_persistent_many_pairs(cuda, ncol):
+    """The persistent filter at the benchmark's width: many row pairs per
+    CTA, the next pair's rows prefetched; 16-byte row copies (2560) and
+    4-byte copies (2557, rows not 16-byte aligned), a strided slice view,
+    a pair split across two angles (odd slice count); checked rows against
+    the FP64 oracle."""
+    rng = np.random.default_rng(ncol)
+    nrow, nslice = 451, 5
+    x = torch.from_numpy(rng.standard_normal((nrow, nslice + 1, ncol))
+                         .astype(np.float32)).cuda()[:, 1:, :]  # a view
+    f = R.filter_sinograms(x, 150, "edge", False, None, "hann").cpu().numpy()
+    xs = x.cpu().numpy()
+    for k in (0, 2, 4):
+        rows = [0, 1, 226, 449, 450]
+        got = f[rows, k, :]
+        ref = O.apply_ramp_filter(xs[rows, k, :], None, "hann", 150, "edge")
+        assert O.rel_l2(got, ref) < 1e-6
 
 
 # ---------------------------------------------------------- back-projection
