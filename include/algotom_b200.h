@@ -736,6 +736,32 @@ int atb_dfi_inverse(const void *coef, int64_t coef_row_stride,
                     int64_t out_slice_stride, int out_f32, void *workspace,
                     int64_t workspace_bytes, void *stream);
 
+/* ---------------------------------------------------------------------- */
+/* Total variation of the sparse-view model-based reconstruction          */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * Smoothed isotropic total variation of a float32 [ny][nx] image (rows
+ * row_stride apart), TV = sum over i < ny-1, j < nx-1 of
+ * sqrt(dx^2 + dy^2 + eps) with dx = x[i][j+1] - x[i][j],
+ * dy = x[i+1][j] - x[i][j], and its gradient.  No counterpart in the
+ * reference (it has no iterative reconstruction on this path); it is the
+ * regulariser of the least-squares + TV descent that drives the
+ * differentiable back-projection.
+ *
+ * atb_tv_value: *out (device float32) = TV, summed in FP64 in a fixed
+ *   order; workspace: atb_tv_workspace() bytes of device memory.
+ * atb_tv_grad: grad = (weight * *scale) dTV/dx (scale a device float32, or
+ *   null for 1), added to grad when accumulate is nonzero.
+ */
+int64_t atb_tv_workspace(void);
+int atb_tv_value(const float *img, int64_t row_stride, int ny, int nx,
+                 double eps, void *workspace, int64_t workspace_bytes,
+                 float *out, void *stream);
+int atb_tv_grad(const float *img, int64_t row_stride, int ny, int nx,
+                double eps, const float *scale, float weight, float *grad,
+                int64_t grad_row_stride, int accumulate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -192,3 +192,27 @@ def test_iterative_reconstruction_with_center_refinement(cuda):
     truth = _blob_image(n)
     assert O.rel_l2(x.cpu().numpy(), truth) < 0.25
 
+
+
+def test_total_variation_matches_tensor_form(cuda):
+    """The fused TV value and gradient (atb_tv_value / atb_tv_grad) against
+    the same formula as FP64 tensor operations through autograd, with a
+    non-unit upstream gradient; odd shapes and a strided view."""
+    rng = np.random.default_rng(11)
+    for ny, nx in ((257, 130), (1, 9), (5, 1), (64, 64)):
+        base = torch.from_numpy(rng.standard_normal((ny, nx + 3))
+                                .astype(np.float32)).cuda()
+        x = base[:, 1:nx + 1].clone().requires_grad_(True)
+        view = base[:, 1:nx + 1]  # strided rows
+        x64 = x.detach().double().requires_grad_(True)
+        dx = x64[:, 1:] - x64[:, :-1]
+        dy = x64[1:, :] - x64[:-1, :]
+        ref = torch.sqrt(dx[:-1, :] ** 2 + dy[:, :-1] ** 2 + 1e-8).sum()
+        (2.5 * ref).backward()
+        got = AG.total_variation(x)
+        (2.5 * got).backward()
+        assert abs(got.item() - ref.item()) <= 1e-6 * max(1.0, ref.item())
+        g_ref = x64.grad.float()
+        assert torch.allclose(x.grad, g_ref, rtol=1e-5, atol=1e-5)
+        v = AG.total_variation(view)
+        assert abs(v.item() - ref.item()) <= 1e-6 * max(1.0, ref.item())
