@@ -202,6 +202,62 @@ __global__ void __launch_bounds__(kThreads) bpf_out_kernel(BpfArgs a, const __gr
   }
 }
 
+// ---- FP64 row filter: the ramp filter a vertical reconstruction applies
+// after its back-projection (algotom/rec/vertrec.py:677-684, 697-706),
+// real(ifft(fft(pad(row)) * ifftshift(|W|))) cropped to [pad, pad + ncol),
+// on FP64 rows, with the same transform lengths and FP64 Stockham FFT as the
+// 2-D filter above.  One row per transform (imaginary part zero): packing two
+// rows into one complex transform would give equal rows unequal round-off
+// (the real and the imaginary slot round differently), and the centre
+// search normalises by a maximum that such equal rows reach exactly.
+struct Row64Args {
+  const double *src;
+  long long srs;
+  int nrows, ncol, pad, n, mode;
+  const double *rowstat;  // [nrows] statistic of each row (statistic modes)
+  const double2 *spec;    // [T] spectrum of the embedded kernel, / T
+  double *dst;
+  long long drs;
+};
+
+__device__ __forceinline__ double row64_value(const Row64Args &a, const double *x, double stat, int rx) {
+  const int n = a.ncol, i = rx - a.pad;
+  if (i >= 0 && i < n) return __ldg(x + i);
+  switch (a.mode) {
+    case ATB_PAD_EDGE:
+    case ATB_PAD_REFLECT:
+    case ATB_PAD_SYMMETRIC:
+    case ATB_PAD_WRAP: return __ldg(x + index_map(i, n, a.mode));
+    case ATB_PAD_CONSTANT: return 0.0;
+    case ATB_PAD_LINEAR_RAMP: {  // k (edge / pad), endpoint excluded, reversed on the right
+      const double w = (double)a.pad;
+      return i < 0 ? (double)rx * (__ldg(x) / w) : (double)(a.pad - 1 - (i - n)) * (__ldg(x + n - 1) / w);
+    }
+    default: return stat;  // mean, maximum, minimum, median of the row
+  }
+}
+
+// row blockIdx.x
+__global__ void __launch_bounds__(kThreads) row64_kernel(const __grid_constant__ Row64Args a,
+                                                         const __grid_constant__ Plan pl) {
+  extern __shared__ double2 sm[];
+  const int T = pl.n, r = blockIdx.x;
+  double2 *tws = sm + 2 * T;
+  atb::fft::load_twiddles(pl, tws);
+  const double *x = a.src + (long long)r * a.srs;
+  const double st = a.rowstat ? a.rowstat[r] : 0.0;
+  for (int rx = threadIdx.x; rx < T; rx += blockDim.x)
+    sm[rx] = make_double2(rx < a.n ? row64_value(a, x, st, rx) : 0.0, 0.0);
+  __syncthreads();
+  double2 *res = atb::fft::run<false>(sm, sm + T, pl, tws);
+  double2 *other = res == sm ? sm + T : sm;
+  for (int k = threadIdx.x; k < T; k += blockDim.x) res[k] = atb::fft::cmul(res[k], __ldg(a.spec + k));
+  __syncthreads();
+  const double2 *out = atb::fft::run<true>(res, other, pl, tws);
+  double *d = a.dst + (long long)r * a.drs;
+  for (int j = threadIdx.x; j < a.ncol; j += blockDim.x) d[j] = out[a.pad + j].x;
+}
+
 // ---- statistics of the statistic pad modes (mean, maximum, minimum, median)
 
 template <typename K>
@@ -448,4 +504,42 @@ extern "C" int atb_bpf_filter2d(const float *src, int64_t src_row_stride, int64_
     if (rc != ATB_OK) return rc;
   }
   return ATB_OK;
+}
+
+extern "C" int atb_filter_rows64_length(int ncol, int pad) {
+  if (ncol < 1 || pad < 0) return atb::fail(ATB_EINVAL, "atb_filter_rows64_length: ncol=%d pad=%d", ncol, pad);
+  const int t = transform_length(ncol, pad);
+  if (t < 0)
+    return atb::fail(ATB_ERANGE, "atb_filter_rows64_length: no transform length <= %d for ncol=%d pad=%d", kMaxLen,
+                     ncol, pad);
+  return t;
+}
+
+extern "C" int atb_filter_rows64(const double *src, int64_t src_row_stride, int nrows, int ncol, int pad,
+                                 int pad_mode, const double *rowstat, const void *spectrum, const void *twiddle,
+                                 int fft_len, double *dst, int64_t dst_row_stride, void *stream) {
+  if (!src || !spectrum || !twiddle || !dst) return atb::fail(ATB_EINVAL, "atb_filter_rows64: null pointer");
+  if (nrows < 1 || ncol < 1 || pad < 0)
+    return atb::fail(ATB_EINVAL, "atb_filter_rows64: bad shape nrows=%d ncol=%d pad=%d", nrows, ncol, pad);
+  if (pad_mode < ATB_PAD_EDGE || pad_mode > ATB_PAD_MEDIAN)
+    return atb::fail(ATB_EINVAL, "atb_filter_rows64: unknown pad mode %d", pad_mode);
+  if (pad_mode >= ATB_PAD_MEAN && pad > 0 && !rowstat)
+    return atb::fail(ATB_EINVAL, "atb_filter_rows64: statistic pad modes need the row statistics");
+  if (pad_mode == ATB_PAD_LINEAR_RAMP && pad == 0) pad_mode = ATB_PAD_CONSTANT;
+  const int t = atb_filter_rows64_length(ncol, pad);
+  if (t < 0) return t;
+  if (fft_len != t)
+    return atb::fail(ATB_EINVAL, "atb_filter_rows64: fft_len=%d, atb_filter_rows64_length gives %d", fft_len, t);
+  Plan pl;
+  if (!make_plan(t, static_cast<const double2 *>(twiddle), pl))
+    return atb::fail(ATB_ERANGE, "atb_filter_rows64: no radix plan for length %d", t);
+  const size_t smem = (2 * (size_t)t + atb::fft::twiddle_entries(t)) * sizeof(double2);
+  const int rc = atb::ensure_smem(row64_kernel, smem, "atb_filter_rows64");
+  if (rc != ATB_OK) return rc;
+  Row64Args a;
+  a.src = src; a.srs = src_row_stride; a.nrows = nrows; a.ncol = ncol; a.pad = pad; a.n = ncol + 2 * pad;
+  a.mode = pad_mode; a.rowstat = rowstat; a.spec = static_cast<const double2 *>(spectrum);
+  a.dst = dst; a.drs = dst_row_stride;
+  row64_kernel<<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
+  return atb::check_launch("atb_filter_rows64");
 }

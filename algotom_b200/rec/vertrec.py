@@ -15,7 +15,7 @@ kernels of ``libalgotom_b200.so``:
   accumulated in FP64 across chunks.
 
 The ramp filter applied after the back-projection (``"after"``) runs in
-FP64 on the device through the library FFT (see :func:`_after_filter64`).
+FP64 on the device (``atb_filter_rows64``, see :func:`_after_filter64`).
 
 Projections may be NumPy arrays, array-likes with NumPy slicing (e.g. HDF5
 datasets) or torch tensors; the reference's chunks of ``chunk_size``
@@ -37,7 +37,6 @@ from .. import _native as nat
 from . import reconstruction as R
 from . import windows as win
 from .center import _gaussian_weights, _integer_input, slice_metrics
-from .padding import pad_rows
 
 _WARN_FULL = ("!!! Applying logarithm is enabled but there are values <= 0.0"
               " in the data !!!")
@@ -175,25 +174,73 @@ def _filter_rows(x3, pad, pad_mode, spec, flen, out3):
              R._stream_ptr(dev))
 
 
-def _after_filter64(ver, filter_name, pad, pad_mode, slab_bytes=1 << 30):
+_AFTER_CACHE = {}
+
+
+def _after_spectrum(filter_name, width, pad, device):
+    """(spectrum, twiddle, T) of ``atb_filter_rows64`` for the after filter:
+    the kernel real(ifft(ifftshift(|W|))) of the padded width N, laid on
+    the length-T circle at the lags [pad - N + 1, pad + width - 1] the crop
+    uses (the kernel itself when T = N), transformed and scaled by 1 / T;
+    FP64, cached per (filter, width, pad, device)."""
+    key = (filter_name, width, pad, str(device))
+    hit = _AFTER_CACHE.get(key)
+    if hit is not None:
+        return hit
+    n = width + 2 * pad
+    t = nat.call("atb_filter_rows64_length", int(width), int(pad))
+    h = np.fft.ifftshift(np.abs(win.ramp_window_row(n, filter_name)))
+    kappa = np.real(np.fft.ifft(h))
+    if t == n:
+        b = kappa
+    else:
+        lags = np.arange(pad - n + 1, pad + width)
+        b = np.zeros(t)
+        b[lags % t] = kappa[lags % n]
+    spec = torch.from_numpy(np.fft.fft(b) / t).to(device, torch.complex128)
+    tw = torch.from_numpy(np.exp(-2j * np.pi * np.arange(t) / t)).to(
+        device, torch.complex128)
+    if len(_AFTER_CACHE) > 8:
+        _AFTER_CACHE.clear()
+    hit = _AFTER_CACHE[key] = (spec, tw, t)
+    return hit
+
+
+def _after_filter64(ver, filter_name, pad, pad_mode):
     """The ramp filter applied to every row of the vertical slices after
     the back-projection (``vertrec.py:684-688``, ``:698-706``):
     ``real(ifft(ifftshift(fftshift(fft(pad(row))) * |W|)))`` cropped, in
-    FP64 on the device (library FFT) from the FP64 back-projection sums.
-    The ramp filter removes the large smooth part of those sums, so a
-    float32 transform (or float32 input) would lose ~1e-4 of the result.
-    ``ver``: float64 [nline, height, width]; returns float64."""
+    FP64 (``atb_filter_rows64``: padding in NumPy's modes, one row per
+    transform, so equal rows give equal results as NumPy's do) from the
+    FP64 back-projection sums.  The ramp filter
+    removes the large smooth part of those sums, so a float32 transform (or
+    float32 input) would lose ~1e-4 of the result.  ``ver``: float64
+    [nline, height, width]; returns float64."""
     nline, height, width = ver.shape
-    n = width + 2 * pad
-    h = np.fft.ifftshift(np.abs(win.ramp_window_row(n, filter_name)))
-    hd = torch.from_numpy(h).to(ver.device)
+    if pad_mode not in nat.PAD_MODES:
+        raise ValueError("pad_mode %r is not supported" % (pad_mode,))
+    spec, tw, t = _after_spectrum(filter_name, width, pad, ver.device)
     rows = ver.reshape(-1, width)
+    if rows.stride(-1) != 1:
+        rows = rows.contiguous()
+    stat = None
+    if pad > 0 and nat.PAD_MODES[pad_mode] >= nat.PAD_MODES["mean"]:
+        if pad_mode == "mean":
+            stat = rows.mean(dim=1)
+        elif pad_mode == "maximum":
+            stat = rows.amax(dim=1)
+        elif pad_mode == "minimum":
+            stat = rows.amin(dim=1)
+        else:
+            srt = torch.sort(rows, dim=1).values
+            stat = 0.5 * (srt[:, (width - 1) // 2] + srt[:, width // 2])
+        stat = stat.contiguous()
     out = torch.empty_like(rows)
-    step = max(1, int(slab_bytes // (16 * n)))
-    for r0 in range(0, rows.shape[0], step):
-        xp = pad_rows(rows[r0:r0 + step], pad, pad_mode)
-        y = torch.fft.ifft(torch.fft.fft(xp, dim=1) * hd, dim=1).real
-        out[r0:r0 + step] = y[:, pad:pad + width]
+    nat.call("atb_filter_rows64", rows.data_ptr(), rows.stride(0),
+             rows.shape[0], width, int(pad), nat.PAD_MODES[pad_mode],
+             stat.data_ptr() if stat is not None else None, spec.data_ptr(),
+             tw.data_ptr(), t, out.data_ptr(), out.stride(0),
+             R._stream_ptr(ver.device))
     return out.reshape(nline, height, width)
 
 

@@ -736,6 +736,31 @@ int atb_dfi_inverse(const void *coef, int64_t coef_row_stride,
                     int64_t out_slice_stride, int out_f32, void *workspace,
                     int64_t workspace_bytes, void *stream);
 
+/*
+ * FP64 ramp filter of rows, as a vertical reconstruction applies it after
+ * its back-projection (algotom/rec/vertrec.py:677-684 and
+ * __apply_ver_ramp_filter, :697-706): every float64 row of ncol samples
+ * padded with NumPy's pad_mode (end and constant values 0; the statistic
+ * modes take rowstat[r], the statistic of row r), then
+ * real(ifft(fft(row) * ifftshift(|W|))) cropped to [pad, pad + ncol).
+ * One row per transform: a row's result depends on that row alone, bit for
+ * bit (equal rows give equal results).
+ *
+ *   spectrum  complex128 [fft_len]: transform of the filter kernel laid on
+ *             the length-fft_len circle at the lags the crop uses, / fft_len
+ *   twiddle   complex128 [fft_len]: exp(-2 pi i t / fft_len)
+ *   fft_len   atb_filter_rows64_length(ncol, pad): ncol + 2 pad when it has
+ *             no prime factor above 13, else a 7-smooth length of at least
+ *             2 ncol + 2 pad - 1; at most 7168
+ * src and dst may be the same rows.
+ */
+int atb_filter_rows64_length(int ncol, int pad);
+int atb_filter_rows64(const double *src, int64_t src_row_stride, int nrows,
+                      int ncol, int pad, int pad_mode,
+                      const double *rowstat, const void *spectrum,
+                      const void *twiddle, int fft_len, double *dst,
+                      int64_t dst_row_stride, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Total variation of the sparse-view model-based reconstruction          */
 /* ---------------------------------------------------------------------- */

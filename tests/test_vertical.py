@@ -108,14 +108,23 @@ def test_row_padding_matches_numpy(mode):
                 assert np.array_equal(got, ref), (n, pad)
 
 
-def test_fp64_after_filter_matches_oracle():
+@pytest.mark.gpu
+def test_fp64_after_filter_matches_oracle(cuda):
+    """The after filter of large smooth FP64 sums (the ramp removes their
+    mean) against the oracle's, 40 + 12 = 52 = 4 x 13 points; equal rows
+    give bit-equal results, as NumPy's do (the centre search normalises by
+    a maximum that such rows reach exactly)."""
     import torch
     from algotom_b200.rec import vertrec as VR
     rng = np.random.default_rng(2)
     x = 50.0 + rng.standard_normal((2, 3, 40)).cumsum(axis=2)
-    got = VR._after_filter64(torch.from_numpy(x), "hann", 6, "edge").numpy()
+    x[1, 2] = x[1, 1] = x[0, 0]
+    got = VR._after_filter64(torch.from_numpy(x).to(cuda), "hann", 6,
+                             "edge").cpu().numpy()
     ref = np.stack([V.ver_ramp_filter(v, "hann", 6, "edge") for v in x])
     assert np.max(np.abs(got - ref)) < 1e-12 * np.max(np.abs(x))
+    assert np.array_equal(got[1, 2], got[0, 0])
+    assert np.array_equal(got[1, 1], got[0, 0])
 
 
 def test_abi_argument_errors():
@@ -326,3 +335,30 @@ def test_device_pinned_and_uint16_inputs(cuda, golden):
                                     cen, angles=ang, flat_field=flat,
                                     dark_field=dark)[0]
     assert O.rel_l2(got, ora) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["edge", "reflect", "constant", "wrap",
+                                  "linear_ramp", "mean", "median"])
+@pytest.mark.parametrize("width,pad", [(96, 14), (130, 10)])
+def test_after_filter64_matches_numpy(cuda, mode, width, pad):
+    """The FP64 after filter (atb_filter_rows64) against the reference's
+    numpy expression (vertrec.py:677-684) at an embedded transform length
+    (96 + 28 = 124 = 4 x 31 is not 13-smooth) and at the padded width
+    itself (130 + 20 = 150), for index, ramp and statistic pad modes; two
+    slices of an odd row count."""
+    import torch
+    from algotom_b200.rec import vertrec as VR
+    from algotom_b200.rec import windows as W
+    rng = np.random.default_rng(width + pad)
+    ver = rng.standard_normal((2, 7, width))
+    got = VR._after_filter64(torch.as_tensor(ver, device="cuda"), "hann",
+                             pad, mode).cpu().numpy()
+    n = width + 2 * pad
+    win = np.abs(W.ramp_window_row(n, "hann"))
+    for k in range(2):
+        xp = np.pad(ver[k], ((0, 0), (pad, pad)), mode=mode)
+        ref = np.real(np.fft.ifft(np.fft.ifftshift(
+            np.fft.fftshift(np.fft.fft(xp), axes=1) * win,
+            axes=1)))[:, pad:pad + width]
+        assert np.abs(got[k] - ref).max() <= 1e-12 * np.abs(ref).max()
