@@ -354,8 +354,7 @@ int atb_backproject_batch(const atb_bp_item *items, int nitems,
  * Limits: at most 4096 items and 1048576 tiles of 64 x 64 pixels in total;
  * larger batches are rejected with ATB_ERANGE before any device work.
  * The first call on a device looks up the array's device address (once per
- * device, with that device current); make that first call before any stream
- * capture.  Every call reuses the same array and overwrites the previous
+ * device, with that device current).  Every call reuses the same array and overwrites the previous
  * call's table: calls that overlap on the device (on different streams, or
  * from different host threads without ordering) race on it.
  */
