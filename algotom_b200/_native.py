@@ -28,7 +28,8 @@ EXPORTS = ("atb_version", "atb_last_error", "atb_copy_2d", "atb_filter_length", 
            "atb_dfi_angle_stack", "atb_wrap_shift_rows", "atb_dfi_fft_length",
            "atb_dfi_fft_setup", "atb_dfi_rows", "atb_dfi_inverse_workspace",
            "atb_dfi_inverse", "atb_tv_workspace", "atb_tv_value",
-           "atb_tv_grad", "atb_filter_rows64_length", "atb_filter_rows64")
+           "atb_tv_grad", "atb_filter_rows64_length", "atb_filter_rows64",
+           "atb_autocorr_length", "atb_autocorr_rowmax")
 
 F32, F16, BF16, U16 = 0, 1, 2, 3
 METRICS = {"entropy": 0, "sharpness": 1}
@@ -152,6 +153,10 @@ _SIGS = {
     "atb_filter_rows64": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         _vp, _vp, _vp, ctypes.c_int, _vp, _c_i64, _vp]),
+    "atb_autocorr_length": (ctypes.c_int, [ctypes.c_int]),
+    "atb_autocorr_rowmax": (ctypes.c_int, [
+        _vp, _c_i64, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, _vp,
+        _vp]),
     "atb_tv_value": (ctypes.c_int, [
         _vp, _c_i64, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp,
         _c_i64, _vp, _vp]),

@@ -206,22 +206,32 @@ __global__ void __launch_bounds__(kThreads) bpf_out_kernel(BpfArgs a, const __gr
 // after its back-projection (algotom/rec/vertrec.py:677-684, 697-706),
 // real(ifft(fft(pad(row)) * ifftshift(|W|))) cropped to [pad, pad + ncol),
 // on FP64 rows, with the same transform lengths and FP64 Stockham FFT as the
-// 2-D filter above.  One row per transform (imaginary part zero): packing two
-// rows into one complex transform would give equal rows unequal round-off
-// (the real and the imaginary slot round differently), and the centre
-// search normalises by a maximum that such equal rows reach exactly.
+// 2-D filter above.  Each row is transformed on its own: packing two rows
+// into one complex transform would give equal rows unequal round-off (the
+// real and the imaginary slot round differently), and the centre search
+// normalises by a maximum that such equal rows reach exactly.  An even
+// length T is done as a real transform: the row's even and odd samples are
+// the real and imaginary parts of one length-T/2 transform Z, split into the
+// row's spectrum X[k] = A[k] + W^k B[k] (W = exp(-2 pi i / T);
+// A[k] = (Z[k] + conj Z[-k]) / 2, B[k] = (Z[k] - conj Z[-k]) / 2i), multiplied
+// by the filter's spectrum S (Hermitian: the kernel is real), and merged back
+// into one length-T/2 inverse, U[k] = (Y[k] + conj Y[H-k])
+// + i W^-k (Y[k] - conj Y[H-k]), whose output holds y[2m] + i y[2m+1].  An
+// odd T takes one complex transform with a zero imaginary part.
 struct Row64Args {
   const double *src;
   long long srs;
   int nrows, ncol, pad, n, mode;
   const double *rowstat;  // [nrows] statistic of each row (statistic modes)
   const double2 *spec;    // [T] spectrum of the embedded kernel, / T
+  const double2 *tw;      // [T] exp(-2 pi i t / T)
   double *dst;
   long long drs;
 };
 
 __device__ __forceinline__ double row64_value(const Row64Args &a, const double *x, double stat, int rx) {
   const int n = a.ncol, i = rx - a.pad;
+  if (rx >= a.n) return 0.0;  // the embedding's zeros
   if (i >= 0 && i < n) return __ldg(x + i);
   switch (a.mode) {
     case ATB_PAD_EDGE:
@@ -237,25 +247,143 @@ __device__ __forceinline__ double row64_value(const Row64Args &a, const double *
   }
 }
 
-// row blockIdx.x
+// Twiddle table of the plan (the length-L transforms) from the length-T
+// table a.tw: every entry when L = T, every second when L = T / 2.
+template <bool HALF>
+__device__ __forceinline__ void row64_twiddles(const double2 *tw, int L, double2 *tws) {
+  constexpr int st = HALF ? 2 : 1, lo = atb::fft::kTwLo;
+  const int nhi = (L + lo - 1) / lo;
+  for (int i = threadIdx.x; i < lo + nhi; i += blockDim.x)
+    tws[i] = i < lo ? (i < L ? __ldg(tw + st * i) : make_double2(1.0, 0.0)) : __ldg(tw + st * (i - lo) * lo);
+}
+
+// Between the forward and the inverse half-length transforms of a real row
+// (res: Z, the transform of x[2m] + i x[2m+1], m < H): the row's spectrum
+// X[k], k = 0 .. H, the product Y[k] = prod(X[k], k), and U, whose inverse
+// holds y[2m] + i y[2m+1] for the real y with the Hermitian spectrum Y.
+// Pairs (k, H - k) are disjoint, so each thread works in place.
+template <class Prod>
+__device__ __forceinline__ void real_split_merge(double2 *res, int H, const double2 *tw, Prod prod) {
+  for (int k = threadIdx.x; 2 * k <= H; k += blockDim.x) {
+    const int kc = k == 0 ? 0 : H - k;
+    const double2 zk = res[k], zc = res[kc];
+    if (k == 0) {
+      // X[0] = Re Z0 + Im Z0, X[H] = Re Z0 - Im Z0; U[0] = (Y0 + conj YH) + i (Y0 - conj YH)
+      const double2 y0 = prod(make_double2(zk.x + zk.y, 0.0), 0), yh = prod(make_double2(zk.x - zk.y, 0.0), H);
+      const double2 s = make_double2(y0.x + yh.x, y0.y - yh.y), d = make_double2(y0.x - yh.x, y0.y + yh.y);
+      res[0] = make_double2(s.x - d.y, s.y + d.x);
+      continue;
+    }
+    const double2 w = __ldg(tw + k);
+    // A = (Zk + conj Zc) / 2, B = (Zk - conj Zc) / 2i, X[k] = A + W^k B, X[H-k] = conj(A - W^k B)
+    const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
+    const double2 B = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
+    const double2 wb = atb::fft::cmul(w, B);
+    const double2 yk = prod(make_double2(A.x + wb.x, A.y + wb.y), k);
+    const double2 yc = prod(make_double2(A.x - wb.x, wb.y - A.y), H - k);
+    // U[k] = (Yk + conj Yc) + i W^-k (Yk - conj Yc); U[H-k] = (Yc + conj Yk) - i W^k (Yc - conj Yk)
+    const double2 s1 = make_double2(yk.x + yc.x, yk.y - yc.y), d1 = make_double2(yk.x - yc.x, yk.y + yc.y);
+    const double2 t1 = atb::fft::cmulc(d1, w);
+    res[k] = make_double2(s1.x - t1.y, s1.y + t1.x);
+    if (kc != k) {
+      const double2 s2 = make_double2(yc.x + yk.x, yc.y - yk.y), d2 = make_double2(yc.x - yk.x, yc.y + yk.y);
+      const double2 t2 = atb::fft::cmul(d2, w);
+      res[kc] = make_double2(s2.x + t2.y, s2.y - t2.x);
+    }
+  }
+}
+
+// y[q] of the inverse's output (real transform: packed two per entry)
+template <bool HALF>
+__device__ __forceinline__ double real_out(const double2 *out, int q) {
+  return HALF ? ((q & 1) ? out[q >> 1].y : out[q >> 1].x) : out[q].x;
+}
+
+// row blockIdx.x; HALF: the plan is for H = T / 2
+template <bool HALF>
 __global__ void __launch_bounds__(kThreads) row64_kernel(const __grid_constant__ Row64Args a,
                                                          const __grid_constant__ Plan pl) {
   extern __shared__ double2 sm[];
-  const int T = pl.n, r = blockIdx.x;
-  double2 *tws = sm + 2 * T;
-  atb::fft::load_twiddles(pl, tws);
+  const int L = pl.n, r = blockIdx.x;  // L: the length of the complex transforms
+  double2 *tws = sm + 2 * L;
+  row64_twiddles<HALF>(a.tw, L, tws);
   const double *x = a.src + (long long)r * a.srs;
   const double st = a.rowstat ? a.rowstat[r] : 0.0;
-  for (int rx = threadIdx.x; rx < T; rx += blockDim.x)
-    sm[rx] = make_double2(rx < a.n ? row64_value(a, x, st, rx) : 0.0, 0.0);
+  for (int m = threadIdx.x; m < L; m += blockDim.x)
+    sm[m] = HALF ? make_double2(row64_value(a, x, st, 2 * m), row64_value(a, x, st, 2 * m + 1))
+                 : make_double2(row64_value(a, x, st, m), 0.0);
   __syncthreads();
-  double2 *res = atb::fft::run<false>(sm, sm + T, pl, tws);
-  double2 *other = res == sm ? sm + T : sm;
-  for (int k = threadIdx.x; k < T; k += blockDim.x) res[k] = atb::fft::cmul(res[k], __ldg(a.spec + k));
+  double2 *res = atb::fft::run<false>(sm, sm + L, pl, tws);
+  double2 *other = res == sm ? sm + L : sm;
+  if constexpr (HALF) {
+    real_split_merge(res, L, a.tw, [&](double2 v, int k) { return atb::fft::cmul(v, __ldg(a.spec + k)); });
+  } else {
+    for (int k = threadIdx.x; k < L; k += blockDim.x) res[k] = atb::fft::cmul(res[k], __ldg(a.spec + k));
+  }
   __syncthreads();
   const double2 *out = atb::fft::run<true>(res, other, pl, tws);
   double *d = a.dst + (long long)r * a.drs;
-  for (int j = threadIdx.x; j < a.ncol; j += blockDim.x) d[j] = out[a.pad + j].x;
+  for (int j = threadIdx.x; j < a.ncol; j += blockDim.x) d[j] = real_out<HALF>(out, a.pad + j);
+}
+
+// ---- row autocorrelation maximum of the vertical centre search's
+// "autocorrelation" metric (algotom/rec/vertrec.py:1255-1261):
+// max over lags of |ifft(|fft(row)|^2)|, the circular autocorrelation of
+// the float32 row, in FP64.  Transform length T = ncol when it has no prime
+// factor above 13; else the row is zero-padded to a 7-smooth T >= 2 ncol - 1
+// and the linear autocorrelation folded back onto the circle,
+// r[l] = y[l] + y[T - ncol + l] (l >= 1).  One row per CTA, a real transform
+// of half length when T is even.
+struct AcArgs {
+  const float *src;
+  long long srs;
+  int nrows, ncol;
+  const double2 *tw;  // [T] exp(-2 pi i t / T)
+  double *out;        // [nrows] maximum of each row
+};
+
+template <bool HALF>
+__global__ void __launch_bounds__(kThreads) autocorr_kernel(const __grid_constant__ AcArgs a,
+                                                            const __grid_constant__ Plan pl) {
+  extern __shared__ double2 sm[];
+  __shared__ double red[kThreads / 32];
+  const int L = pl.n, T = HALF ? 2 * L : L, r = blockIdx.x, n = a.ncol;
+  double2 *tws = sm + 2 * L;
+  row64_twiddles<HALF>(a.tw, L, tws);
+  const float *x = a.src + (long long)r * a.srs;
+  for (int m = threadIdx.x; m < L; m += blockDim.x) {
+    const int i0 = HALF ? 2 * m : m, i1 = i0 + 1;
+    const double v0 = i0 < n ? (double)__ldg(x + i0) : 0.0;
+    const double v1 = HALF && i1 < n ? (double)__ldg(x + i1) : 0.0;
+    sm[m] = make_double2(v0, v1);
+  }
+  __syncthreads();
+  double2 *res = atb::fft::run<false>(sm, sm + L, pl, tws);
+  double2 *other = res == sm ? sm + L : sm;
+  if constexpr (HALF) {
+    real_split_merge(res, L, a.tw, [](double2 v, int) { return make_double2(fma(v.x, v.x, v.y * v.y), 0.0); });
+  } else {
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+      const double2 v = res[k];
+      res[k] = make_double2(fma(v.x, v.x, v.y * v.y), 0.0);
+    }
+  }
+  __syncthreads();
+  const double2 *out = atb::fft::run<true>(res, other, pl, tws);
+  const double inv = 1.0 / (double)T;  // the inverse's 1 / T
+  double m = 0.0;
+  for (int l = threadIdx.x; l < n; l += blockDim.x) {
+    double v = real_out<HALF>(out, l);
+    if (T != n && l > 0) v += real_out<HALF>(out, T - n + l);
+    m = fmax(m, fabs(v * inv));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    a.out[r] = m;
+  }
 }
 
 // ---- statistics of the statistic pad modes (mean, maximum, minimum, median)
@@ -530,16 +658,60 @@ extern "C" int atb_filter_rows64(const double *src, int64_t src_row_stride, int 
   if (t < 0) return t;
   if (fft_len != t)
     return atb::fail(ATB_EINVAL, "atb_filter_rows64: fft_len=%d, atb_filter_rows64_length gives %d", fft_len, t);
+  const bool half = (t & 1) == 0;
+  const int len = half ? t / 2 : t;
   Plan pl;
-  if (!make_plan(t, static_cast<const double2 *>(twiddle), pl))
-    return atb::fail(ATB_ERANGE, "atb_filter_rows64: no radix plan for length %d", t);
-  const size_t smem = (2 * (size_t)t + atb::fft::twiddle_entries(t)) * sizeof(double2);
-  const int rc = atb::ensure_smem(row64_kernel, smem, "atb_filter_rows64");
+  if (!make_plan(len, static_cast<const double2 *>(twiddle), pl))
+    return atb::fail(ATB_ERANGE, "atb_filter_rows64: no radix plan for length %d", len);
+  const size_t smem = (2 * (size_t)len + atb::fft::twiddle_entries(len)) * sizeof(double2);
+  const int rc = half ? atb::ensure_smem(row64_kernel<true>, smem, "atb_filter_rows64")
+                      : atb::ensure_smem(row64_kernel<false>, smem, "atb_filter_rows64");
   if (rc != ATB_OK) return rc;
   Row64Args a;
   a.src = src; a.srs = src_row_stride; a.nrows = nrows; a.ncol = ncol; a.pad = pad; a.n = ncol + 2 * pad;
   a.mode = pad_mode; a.rowstat = rowstat; a.spec = static_cast<const double2 *>(spectrum);
-  a.dst = dst; a.drs = dst_row_stride;
-  row64_kernel<<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
+  a.tw = static_cast<const double2 *>(twiddle); a.dst = dst; a.drs = dst_row_stride;
+  if (half)
+    row64_kernel<true><<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
+  else
+    row64_kernel<false><<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
   return atb::check_launch("atb_filter_rows64");
+}
+
+extern "C" int atb_autocorr_length(int ncol) {
+  static const int p13[] = {2, 3, 5, 7, 11, 13};
+  static const int p7[] = {2, 3, 5, 7};
+  if (ncol < 1) return atb::fail(ATB_EINVAL, "atb_autocorr_length: ncol=%d", ncol);
+  if (ncol <= kMaxLen && smooth(ncol, p13, 6)) return ncol;
+  for (int m = 2 * ncol - 1; m <= kMaxLen; ++m)
+    if (smooth(m, p7, 4)) return m;
+  return atb::fail(ATB_ERANGE, "atb_autocorr_length: no transform length <= %d for ncol=%d", kMaxLen, ncol);
+}
+
+extern "C" int atb_autocorr_rowmax(const float *src, int64_t src_row_stride, int nrows, int ncol,
+                                   const void *twiddle, int fft_len, double *out, void *stream) {
+  if (!src || !twiddle || !out) return atb::fail(ATB_EINVAL, "atb_autocorr_rowmax: null pointer");
+  if (nrows < 1 || ncol < 1 || src_row_stride < ncol)
+    return atb::fail(ATB_EINVAL, "atb_autocorr_rowmax: bad shape nrows=%d ncol=%d", nrows, ncol);
+  const int t = atb_autocorr_length(ncol);
+  if (t < 0) return t;
+  if (fft_len != t)
+    return atb::fail(ATB_EINVAL, "atb_autocorr_rowmax: fft_len=%d, atb_autocorr_length gives %d", fft_len, t);
+  const bool half = (t & 1) == 0;
+  const int len = half ? t / 2 : t;
+  Plan pl;
+  if (!make_plan(len, static_cast<const double2 *>(twiddle), pl))
+    return atb::fail(ATB_ERANGE, "atb_autocorr_rowmax: no radix plan for length %d", len);
+  const size_t smem = (2 * (size_t)len + atb::fft::twiddle_entries(len)) * sizeof(double2);
+  const int rc = half ? atb::ensure_smem(autocorr_kernel<true>, smem, "atb_autocorr_rowmax")
+                      : atb::ensure_smem(autocorr_kernel<false>, smem, "atb_autocorr_rowmax");
+  if (rc != ATB_OK) return rc;
+  AcArgs a;
+  a.src = src; a.srs = src_row_stride; a.nrows = nrows; a.ncol = ncol;
+  a.tw = static_cast<const double2 *>(twiddle); a.out = out;
+  if (half)
+    autocorr_kernel<true><<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
+  else
+    autocorr_kernel<false><<<nrows, kThreads, smem, atb::as_stream(stream)>>>(a, pl);
+  return atb::check_launch("atb_autocorr_rowmax");
 }

@@ -175,6 +175,20 @@ def _filter_rows(x3, pad, pad_mode, spec, flen, out3):
 
 
 _AFTER_CACHE = {}
+_TW_CACHE = {}
+
+
+def _twiddle64(t, device):
+    """complex128 exp(-2 pi i m / t), m < t, on ``device`` (cached)."""
+    key = (t, str(device))
+    tw = _TW_CACHE.get(key)
+    if tw is None:
+        if len(_TW_CACHE) > 8:
+            _TW_CACHE.clear()
+        tw = _TW_CACHE[key] = torch.from_numpy(
+            np.exp(-2j * np.pi * np.arange(t) / t)).to(device,
+                                                         torch.complex128)
+    return tw
 
 
 def _after_spectrum(filter_name, width, pad, device):
@@ -198,8 +212,7 @@ def _after_spectrum(filter_name, width, pad, device):
         b = np.zeros(t)
         b[lags % t] = kappa[lags % n]
     spec = torch.from_numpy(np.fft.fft(b) / t).to(device, torch.complex128)
-    tw = torch.from_numpy(np.exp(-2j * np.pi * np.arange(t) / t)).to(
-        device, torch.complex128)
+    tw = _twiddle64(t, device)
     if len(_AFTER_CACHE) > 8:
         _AFTER_CACHE.clear()
     hit = _AFTER_CACHE[key] = (spec, tw, t)
@@ -765,10 +778,26 @@ _SEARCH_BYTES = 4 << 30  # FP64 slices reconstructed per pass over the data
 
 def _autocorrelation(imgs):
     """``mean(max(|ifft(|fft(row)|^2)|, axis=1))`` of every float32 image
-    of [n, rows, cols] (``vertrec.py:1255-1261``; library FFT)."""
-    f = torch.fft.fft(imgs, dim=-1)
-    ac = torch.fft.ifft(f.abs() ** 2, dim=-1).abs()
-    return ac.amax(dim=-1).to(torch.float64).mean(dim=-1).cpu().numpy()
+    of [n, rows, cols] (``vertrec.py:1255-1261``): the row maxima by
+    ``atb_autocorr_rowmax`` (FP64 transforms), their mean per image in
+    NumPy as the reference takes it.  Widths with no transform length up to
+    7168 (a prime factor above 13 and more than 3584 columns) take the
+    library FFT."""
+    n, rows, cols = imgs.shape
+    t = nat.load().atb_autocorr_length(int(cols))
+    if t < 0:
+        f = torch.fft.fft(imgs, dim=-1)
+        ac = torch.fft.ifft(f.abs() ** 2, dim=-1).abs()
+        return ac.amax(dim=-1).to(torch.float64).mean(dim=-1).cpu().numpy()
+    x = imgs.reshape(n * rows, cols)
+    if x.stride(-1) != 1:
+        x = x.contiguous()
+    tw = _twiddle64(t, imgs.device)
+    out = torch.empty(n * rows, dtype=torch.float64, device=imgs.device)
+    nat.call("atb_autocorr_rowmax", x.data_ptr(), x.stride(0), n * rows,
+             cols, tw.data_ptr(), t, out.data_ptr(),
+             R._stream_ptr(imgs.device))
+    return out.cpu().numpy().reshape(n, rows).mean(axis=1)
 
 
 def _entropy(imgs, nmin, nmax):
@@ -855,8 +884,8 @@ def find_center_vertical_slice(projections, slice_index, start, stop,
     sets the entropy's normalisation -- is a line of the same vertical
     back-projection launch, so the data are read once for all of them
     (in passes of about 4 GB of FP64 slices when there are many).  Metrics:
-    ``"entropy"``, ``"sharpness"`` (device kernels), ``"autocorrelation"``
-    (library FFT) or ``metric_function(recon, **kwargs)`` on each slice as a
+    ``"entropy"``, ``"sharpness"``, ``"autocorrelation"`` (device
+    kernels) or ``metric_function(recon, **kwargs)`` on each slice as a
     NumPy array.  Returns the centre of the smallest metric, or
     ``(list_center, list_metric)`` with ``return_metric``.
     """

@@ -760,6 +760,24 @@ int atb_filter_rows64(const double *src, int64_t src_row_stride, int nrows,
                       const void *twiddle, int fft_len, double *dst,
                       int64_t dst_row_stride, void *stream);
 
+/*
+ * Row maxima of the "autocorrelation" metric of the vertical centre search
+ * (__calculate_autocorrelation_coefficient, algotom/rec/vertrec.py:
+ * 1255-1261, mean(max(|ifft(|fft(row)|^2)|, axis=1))): out[r] = the largest
+ * |circular autocorrelation| of float32 row r over all lags, in FP64; the
+ * caller takes the mean of the rows of each image.
+ *
+ *   twiddle  complex128 [fft_len]: exp(-2 pi i t / fft_len)
+ *   fft_len  atb_autocorr_length(ncol): ncol when it has no prime factor
+ *            above 13, else a 7-smooth length of at least 2 ncol - 1 (the
+ *            linear autocorrelation, folded onto the circle); at most 7168
+ *   out      device float64 [nrows]
+ */
+int atb_autocorr_length(int ncol);
+int atb_autocorr_rowmax(const float *src, int64_t src_row_stride, int nrows,
+                        int ncol, const void *twiddle, int fft_len,
+                        double *out, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Total variation of the sparse-view model-based reconstruction          */
 /* ---------------------------------------------------------------------- */

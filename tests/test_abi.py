@@ -46,6 +46,33 @@ def test_filter_length():
                                                      240, 243, 250, 252, 256)
     rc = nat.load().atb_filter_length(20000, 150)
     assert rc == -3 and "16384" in nat.last_error()
+
+
+def test_fp64_row_lengths_and_argument_errors():
+    """Transform lengths of the FP64 after filter and of the autocorrelation
+    metric, and their argument checks (no device work)."""
+    lib = nat.load()
+    assert nat.call("atb_filter_rows64_length", 2560, 150) == 2860
+    assert nat.call("atb_filter_rows64_length", 61, 9) == 140  # 79 is prime
+    assert nat.call("atb_autocorr_length", 2560) == 2560
+    assert nat.call("atb_autocorr_length", 75) == 75
+    assert nat.call("atb_autocorr_length", 61) == 125  # >= 2 x 61 - 1
+    assert nat.call("atb_autocorr_length", 71) == 144
+    assert lib.atb_autocorr_length(3601) == -3  # 13 x 277, 7201 > 7168
+    assert lib.atb_autocorr_length(0) == -1
+    one = 1
+    assert lib.atb_autocorr_rowmax(None, 8, 2, 8, one, 8, one, None) == -1
+    assert lib.atb_autocorr_rowmax(one, 4, 2, 8, one, 8, one, None) == -1
+    rc = lib.atb_autocorr_rowmax(one, 61, 2, 61, one, 61, one, None)
+    assert rc == -1 and "125" in nat.last_error()
+    assert lib.atb_filter_rows64(one, 8, 2, 8, 2, 0, None, one, one, 12,
+                                 None, 8, None) == -1
+    rc = lib.atb_filter_rows64(one, 8, 2, 8, 2, 8, None, one, one, 12, one,
+                               8, None)
+    assert rc == -1 and "statistic" in nat.last_error()
+    rc = lib.atb_filter_rows64(one, 8, 2, 8, 2, 0, None, one, one, 13, one,
+                               8, None)
+    assert rc == -1 and "12" in nat.last_error()
     assert nat.load().atb_filter_length(0, 1) == -1
 
 

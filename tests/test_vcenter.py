@@ -351,3 +351,21 @@ def test_search_log_warning_and_repair(cuda, golden):
     assert texts == list(g["vc_log_warnings"])
     assert np.array_equal(bad, g["vc_log_mutated"])
     _check("sharpness", ms, g["vc_log_metrics"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cols", [2560, 75, 61, 71])
+def test_autocorrelation_matches_numpy(cuda, cols):
+    """The autocorrelation metric (atb_autocorr_rowmax + the row mean)
+    against vertrec.py:1255-1261 in FP64 at a 13-smooth even width (2560:
+    real transform of half length), a 13-smooth odd one (75: complex
+    transform), and widths embedded in 7-smooth lengths of at least
+    2 cols - 1 and folded (61 -> 125, odd; 71 -> 144, even)."""
+    import torch
+    from algotom_b200.rec import vertrec as VR
+    rng = np.random.default_rng(cols)
+    imgs = rng.standard_normal((3, 5, cols)).astype(np.float32)
+    imgs[1] += 4.0  # a large mean: the maximum at lag 0
+    got = VR._autocorrelation(torch.as_tensor(imgs, device=cuda))
+    ref = np.array([V.autocorrelation(im) for im in imgs])
+    assert np.max(np.abs(got - ref) / np.abs(ref)) < 1e-12

@@ -340,13 +340,14 @@ def test_device_pinned_and_uint16_inputs(cuda, golden):
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", ["edge", "reflect", "constant", "wrap",
                                   "linear_ramp", "mean", "median"])
-@pytest.mark.parametrize("width,pad", [(96, 14), (130, 10)])
+@pytest.mark.parametrize("width,pad", [(96, 14), (130, 10), (63, 6)])
 def test_after_filter64_matches_numpy(cuda, mode, width, pad):
     """The FP64 after filter (atb_filter_rows64) against the reference's
     numpy expression (vertrec.py:677-684) at an embedded transform length
-    (96 + 28 = 124 = 4 x 31 is not 13-smooth) and at the padded width
-    itself (130 + 20 = 150), for index, ramp and statistic pad modes; two
-    slices of an odd row count."""
+    (96 + 28 = 124 = 4 x 31 is not 13-smooth: 224), at the padded width
+    itself (130 + 20 = 150), both even (real transforms of half length), and
+    at an odd one (63 + 12 = 75: one complex transform per row), for index,
+    ramp and statistic pad modes; two slices of an odd row count."""
     import torch
     from algotom_b200.rec import vertrec as VR
     from algotom_b200.rec import windows as W
