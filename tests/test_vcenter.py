@@ -354,13 +354,14 @@ def test_search_log_warning_and_repair(cuda, golden):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cols", [2560, 75, 61, 71])
+@pytest.mark.parametrize("cols", [2560, 75, 61, 71, 1, 2, 3])
 def test_autocorrelation_matches_numpy(cuda, cols):
     """The autocorrelation metric (atb_autocorr_rowmax + the row mean)
     against vertrec.py:1255-1261 in FP64 at a 13-smooth even width (2560:
     real transform of half length), a 13-smooth odd one (75: complex
     transform), and widths embedded in 7-smooth lengths of at least
-    2 cols - 1 and folded (61 -> 125, odd; 71 -> 144, even)."""
+    2 cols - 1 and folded (61 -> 125, odd; 71 -> 144, even), and the
+    smallest widths (plans of zero or one stage)."""
     import torch
     from algotom_b200.rec import vertrec as VR
     rng = np.random.default_rng(cols)
