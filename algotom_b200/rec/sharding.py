@@ -8,6 +8,11 @@ of uneven sinograms the items are dealt out by longest-processing-time
 updates).  The only collective is the optional gather of results to one
 rank (``gather_to_root``), through whichever ``torch.distributed`` backend
 the process group uses (NCCL between GPUs, gloo in CPU tests).
+
+One slice too large for one GPU's time budget can instead have its angles
+split (``fbp_angle_split``): every rank filters and back-projects its
+contiguous share of the sinogram's rows, and one in-place ``all_reduce``
+sums the partial images -- the only exchange, after all the compute.
 """
 import heapq
 
@@ -61,3 +66,63 @@ def gather_to_root(obj, group=None, root=0):
     objs = [None] * world if dist.get_rank(group) == root else None
     dist.gather_object(obj, objs, dst=root, group=group)
     return objs
+
+
+def _device_partial(rows, angles, center, mask_r2, scale, ramp_win,
+                    filter_name, pad, pad_mode, apply_log, ncol):
+    """A rank's partial image for ``fbp_angle_split``: the device ramp
+    filter of its rows and their back-projection with the full
+    reconstruction's mask and scale; float32 [ncol, ncol] on the device."""
+    import torch
+    from . import reconstruction as R
+    if len(rows) == 0:
+        return torch.zeros((ncol, ncol), dtype=torch.float32,
+                           device=R._device())
+    if apply_log:
+        R._check_log_input(rows)
+    t, _ = R._to_device(rows)
+    f = R.filter_sinograms(R._as3(t), pad, pad_mode, apply_log, ramp_win,
+                           filter_name)
+    rec = R.backproject(f, angles, center, edge_pad=False, mask_r2=mask_r2,
+                        scale=scale)
+    return rec[:, 0, :].contiguous()
+
+
+def fbp_angle_split(sinogram, center, angles=None, ratio=1.0, ramp_win=None,
+                    filter_name="hann", pad=None, pad_mode="edge",
+                    apply_log=True, group=None, partial=None):
+    """FBP of one [nrow, ncol] sinogram with its angles split across the
+    ranks of ``group``; the arguments are ``fbp_reconstruction``'s
+    (``reconstruction.py:362-493``).
+
+    Rank r takes the rows ``slab_bounds(nrow, world, r)`` (with their angles
+    and, for a 2-D ``ramp_win`` of nrow rows, its rows), filters them and
+    back-projects them with the whole reconstruction's circle mask and
+    scale pi/(nrow-1) -- both linear, so they commute with the sum -- and
+    one in-place ``all_reduce`` (sum) over the group adds the partial
+    images.  Ranks without rows (more ranks than angles) add zeros.  Every
+    rank returns the float32 [ncol, ncol] image on its device.
+    ``partial(rows, angles, center, mask_r2, scale, ramp_win, filter_name,
+    pad, pad_mode, apply_log, ncol)`` makes a rank's partial image as a
+    tensor the group's backend can reduce; the default is the device filter
+    and back-projection.
+    """
+    import torch.distributed as dist
+    from . import reconstruction as R
+    if len(getattr(sinogram, "shape", ())) != 2:
+        raise ValueError("fbp_angle_split takes one 2-D [nrow, ncol] "
+                         "sinogram")
+    nrow, _, ncol, angles = R._validate(sinogram, center, angles)
+    if pad is None:
+        pad = min(int(0.15 * ncol), 150)
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    start, stop = slab_bounds(nrow, world, rank)
+    win = ramp_win
+    if win is not None and np.ndim(win) == 2 and np.shape(win)[0] == nrow:
+        win = win[start:stop]
+    fn = _device_partial if partial is None else partial
+    part = fn(sinogram[start:stop], angles[start:stop], center,
+              R._mask_r2(ratio, center, ncol), R._scale(nrow), win,
+              filter_name, pad, pad_mode, apply_log, ncol)
+    dist.all_reduce(part, group=group)
+    return part

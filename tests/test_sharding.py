@@ -118,3 +118,96 @@ def test_device_slabs_match_whole_stack(cuda):
     assert sharded.shape == whole.shape == ref.shape
     assert O.rel_l2(sharded, whole) < 1e-6
     assert O.rel_l2(sharded, ref) < 1e-5
+
+
+def _oracle_partial(ratio):
+    """fbp_angle_split's partial image from the FP64 oracle: ramp filter of
+    the rank's rows, back-projection of its angles, the whole slice's mask
+    and scale (a CPU tensor, for gloo)."""
+    def fn(rows, angles, center, mask_r2, scale, ramp_win, filter_name, pad,
+           pad_mode, apply_log, ncol):
+        import torch
+        from oracle import fbp_oracle as O
+        if len(rows) == 0:
+            return torch.zeros((ncol, ncol), dtype=torch.float64)
+        sino = np.array(rows, dtype=np.float64)
+        if apply_log:
+            sino[sino <= 0.0] = 1.0
+            sino = -np.log(sino)
+        f = O.apply_ramp_filter(sino, None, filter_name, pad, pad_mode)
+        r = O.back_projection(f, angles, center)
+        mask = O._mask(ncol, center, ratio)
+        return torch.from_numpy((r if mask is None else r * mask) * scale)
+    return fn
+
+
+def _angle_worker(rank, world, port, result_path):
+    import torch.distributed as dist
+    from algotom_b200 import phantom
+    from oracle import fbp_oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        nrow, ncol, cen = 37, 40, 19.5
+        sino = np.exp(-phantom.ellipse_sinogram(9, nrow, ncol, cen)[0])
+        ang = np.linspace(0, np.pi, nrow, endpoint=False)
+        got = SH.fbp_angle_split(sino, cen, angles=ang, ratio=0.9,
+                                 partial=_oracle_partial(0.9)).numpy()
+        ref = O.fbp_reconstruction(sino, cen, angles=ang, ratio=0.9)
+        # the scale is the product's float32(pi) / float32(nrow - 1), the
+        # oracle's pi / (nrow - 1) in FP64: 1e-7 apart
+        ok = np.allclose(got, ref, rtol=0, atol=2e-7 * np.abs(ref).max())
+        np.save(result_path + ".%d.npy" % rank, np.array([ok]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_angle_split_gloo(tmp_path, world):
+    """fbp_angle_split on 2 and 3 gloo ranks (37 angles: uneven shares): the
+    all-reduced partial images equal the whole-slice FP64 FBP on every
+    rank."""
+    result = str(tmp_path / "ok")
+    mp.start_processes(_angle_worker, args=(world, _free_port(), result),
+                       nprocs=world, join=True, start_method="spawn")
+    for r in range(world):
+        assert np.load(result + ".%d.npy" % r).all()
+
+
+@pytest.mark.gpu
+def test_angle_split_on_device(cuda):
+    """The device partial images of 3 angle shares (60 + 60 + 60 of 180
+    angles) summed on one GPU, and fbp_angle_split over a one-rank NCCL
+    group, against the device fbp_reconstruction of the whole slice and
+    the FP64 oracle.  (Three NCCL ranks on one GPU would be kernels waiting
+    on one another; the collective with more ranks is the gloo test.)"""
+    import torch
+    import torch.distributed as dist
+    from algotom_b200 import phantom
+    from algotom_b200.rec import reconstruction as REC
+    from oracle import fbp_oracle as O
+    nrow, ncol, cen = 180, 320, 158.6
+    sino = np.exp(-phantom.ellipse_sinogram(21, nrow, ncol, cen)[0]).astype(
+        np.float32)
+    ang = np.linspace(0, np.pi, nrow, endpoint=False)
+    whole = REC.fbp_reconstruction(sino, cen, angles=ang)
+    ref = O.fbp_reconstruction(sino, cen, angles=ang)
+    r2, scale = REC._mask_r2(1.0, cen, ncol), REC._scale(nrow)
+    acc = torch.zeros((ncol, ncol), dtype=torch.float32, device=cuda)
+    for r in range(3):
+        a, b = SH.slab_bounds(nrow, 3, r)
+        acc += SH._device_partial(sino[a:b], ang[a:b], cen, r2, scale, None,
+                                  "hann", min(int(0.15 * ncol), 150), "edge",
+                                  True, ncol)
+    summed = acc.cpu().numpy()
+    assert O.rel_l2(summed, whole) < 1e-6
+    assert O.rel_l2(summed, ref) < 1e-5
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=cuda)
+    try:
+        one = SH.fbp_angle_split(sino, cen, angles=ang).cpu().numpy()
+    finally:
+        dist.destroy_process_group()
+    assert O.rel_l2(one, whole) < 1e-6
